@@ -1,0 +1,183 @@
+/*
+ * moao_b200 — C ABI of the B200-native MOAO tomographic-reconstructor path.
+ *
+ * Plain pointers and sizes only. Every matrix is column-major with an explicit
+ * leading dimension, exactly like the reference's host buffers. Entry points
+ * whose name ends in `_host` take HOST buffers and reproduce the reference's
+ * in-place semantics (they copy to the device, compute there, and copy the
+ * results back); every other matrix argument is a DEVICE pointer and the call
+ * is asynchronous on the context's stream.
+ *
+ * Nothing here prints or exits; every call returns a moao_status.
+ */
+#ifndef MOAO_B200_H
+#define MOAO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MOAO_OK = 0,
+  MOAO_ERR_BAD_ARG = 1,     /* invalid size, type or pointer                  */
+  MOAO_ERR_NOT_SPD = 2,     /* Cholesky met a non-positive pivot (see report) */
+  MOAO_ERR_OOM = 3,         /* device allocation or admission failed          */
+  MOAO_ERR_CUDA = 4,        /* a CUDA runtime / cuFFT call failed             */
+  MOAO_ERR_IO = 5,          /* parameter / input file could not be read       */
+  MOAO_ERR_TIMEOUT = 6,     /* a bounded device or host wait ran out          */
+  MOAO_ERR_UNSUPPORTED = 7, /* option not available in this build            */
+  MOAO_ERR_BUSY = 8,        /* request queue full / request not finished      */
+  MOAO_ERR_CANCELLED = 9    /* request cancelled before it ran                */
+} moao_status;
+
+typedef enum {
+  MOAO_PREC_FP64 = 0,  /* every stage in FP64 (parity path)                    */
+  MOAO_PREC_MIXED = 1  /* tensor-core trailing updates + FP64 refinement of R  */
+} moao_prec;
+
+/* Human-readable name of a status code (static string). */
+const char* moao_status_string(moao_status s);
+/* Last error detail recorded on this thread (static buffer, never NULL). */
+const char* moao_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* System model (host side).                                                */
+/* Replaces Tomo_struct<T>(sys, atm)  common/tomo_struct/tomo_struct.cpp:11  */
+/* ------------------------------------------------------------------------ */
+typedef struct moao_tomo moao_tomo;
+
+typedef struct {
+  int nW, nLgs, nNgs, nTarget, nLayer, Nx;
+  long nmeas;   /* getNMeas   common/tomo_struct/tomo_struct.cpp:570 */
+  long nmeasts; /* getNMeasTS common/tomo_struct/tomo_struct.cpp:577 */
+  double diam, obs, lgsCst;
+  int nssp_ts;  /* Nssp of the truth sensor (intersample np = nssp_ts + 1) */
+} moao_tomo_info;
+
+/* Reads sys-params.txt and an atmosphere profile (reference positional format). */
+moao_status moao_tomo_create(const char* sys_file, const char* atm_file, moao_tomo** out);
+/* Tomo_struct::updateAtm  common/tomo_struct/tomo_struct.cpp:213 */
+moao_status moao_tomo_update_atm(moao_tomo* t, const char* atm_file);
+/* Replace the profile from arrays (serving path, no file). L0 per layer. */
+moao_status moao_tomo_set_profile(moao_tomo* t, int nLayer, const double* cn2,
+                                  const double* h, const double* L0);
+/* Tomo_struct::setTarget  common/tomo_struct/tomo_struct.cpp:278 */
+moao_status moao_tomo_set_target(moao_tomo* t, int target);
+moao_status moao_tomo_get_info(const moao_tomo* t, moao_tomo_info* out);
+/* Copies a named geometry table (u, v, X, Y, sspSizeL, L0diff, cn2, h, Nsubap,
+ * Nssp, noiseNGS, noiseLGSxx, noiseLGSyy, noiseLGSxy, alphaX, alphaY, lgsExt,
+ * lgsTheta, mr) into out (capacity cap doubles). Returns the table length, or
+ * -1 for an unknown name. out may be NULL to query the length. */
+long moao_tomo_table(const moao_tomo* t, const char* name, double* out, long cap);
+void moao_tomo_destroy(moao_tomo* t);
+
+/* ------------------------------------------------------------------------ */
+/* Device context: one per GPU. Owns a stream, cached device geometry and the */
+/* factorisation workspace.                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct moao_ctx moao_ctx;
+
+moao_status moao_ctx_create(int device, moao_ctx** out);
+void moao_ctx_destroy(moao_ctx* ctx);
+/* Use an external cudaStream_t (NULL = the context's own stream). */
+moao_status moao_ctx_set_stream(moao_ctx* ctx, void* stream);
+void* moao_ctx_stream(moao_ctx* ctx);
+moao_status moao_ctx_synchronize(moao_ctx* ctx);
+/* Number of kernels this library launched on the context since creation. */
+long long moao_ctx_launch_count(const moao_ctx* ctx);
+/* Panel width of the blocked factorisation (default 256; multiple of 64). */
+moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
+
+/* ------------------------------------------------------------------------ */
+/* Covariance generation.                                                    */
+/* Replaces MOAO_COMMON::matcov_tile  common/compute/matcov.cpp:17           */
+/*   type_mat 1: Cmm (lower triangle only, like uplo='l')                   */
+/*   type_mat 3: Ctm (full)    type_mat 4: Ctt (full)                        */
+/*   type_mat 5: Cmm with both triangles written (symmetric fill, no         */
+/*               counterpart in the reference; used by the fused pipeline)  */
+/* ------------------------------------------------------------------------ */
+moao_status moao_matcov_tile(moao_ctx* ctx, const moao_tomo* t, double* d_data,
+                             int nrows, int ncols, int xoffset, int yoffset,
+                             int lda, int type_mat);
+moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_data,
+                                  int nrows, int ncols, int xoffset, int yoffset,
+                                  int lda, int type_mat);
+
+/* ------------------------------------------------------------------------ */
+/* Reconstructor R = Ctm . Cmm^-1.                                           */
+/* Replaces MOAO_LAPACK::reconstructor  lapack/compute/reconstructor.cpp:32  */
+/*   potrf('L', Cmm); per target g: trsm(R,L,T,N) then trsm(R,L,N,N).       */
+/* Cmm is overwritten by its lower Cholesky factor (upper triangle left       */
+/* untouched) and Ctm by R, ngal targets of nmeasts x nmeas each, stored      */
+/* nmeas*nmeasts apart.                                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int info;              /* 0, or the 1-based column of a non-positive pivot */
+  int refine_steps;      /* mixed path: FP64 refinement steps taken           */
+  double refine_resid;   /* mixed path: ||Ctm - R Cmm||_F / ||Ctm||_F at exit  */
+  double ms_factor;      /* device time of the Cholesky factorisation         */
+  double ms_solve;       /* device time of the two triangular solves           */
+  double ms_refine;      /* device time of the refinement                      */
+} moao_solve_report;
+
+moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* d_Cmm,
+                               long ldCmm, double* d_Ctm, long ldCtm, long ngal,
+                               moao_prec prec, moao_solve_report* rep);
+moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, double* Cmm,
+                                    long ldCmm, double* Ctm, long ldCtm, long ngal,
+                                    moao_solve_report* rep);
+
+/* ------------------------------------------------------------------------ */
+/* Error covariances.                                                        */
+/* Replaces MOAO_LAPACK::Cee_Cvv  lapack/compute/cee_cvv.cpp:50-125          */
+/*   Cee = Ctt - Ctm R^T - R Ctm^T + R Cmm R^T ;  Cvv = Dx Cee Dx^T           */
+/* Same in-place contract: Cpp (Ctt) and Cpm (Ctm) are destroyed, Tmp is     */
+/* scratch, Cmm is read as a symmetric matrix from its lower triangle.       */
+/* ------------------------------------------------------------------------ */
+moao_status moao_cee_cvv(moao_ctx* ctx, long nmeas, long nmeasts, long nact,
+                         double* Cmm, long ldCmm, double* Cpp, long ldCpp,
+                         double* Cpm, long ldCpm, double* R, long ldR,
+                         double* Dx, long ldDx, double* Cee, long ldCee,
+                         double* Cvv, long ldCvv, double* Tmp, long ldTmp);
+moao_status moao_cee_cvv_host(moao_ctx* ctx, long nmeas, long nmeasts, long nact,
+                              double* Cmm, long ldCmm, double* Cpp, long ldCpp,
+                              double* Cpm, long ldCpm, double* R, long ldR,
+                              double* Dx, long ldDx, double* Cee, long ldCee,
+                              double* Cvv, long ldCvv, double* Tmp, long ldTmp);
+
+/* ------------------------------------------------------------------------ */
+/* Intersample PSF.                                                          */
+/* Replaces intersample_prepare / intersample_init / intersample_process /   */
+/* intersample_free  common/tomo_struct/intersample.cpp:74-333               */
+/* ------------------------------------------------------------------------ */
+typedef struct moao_isample moao_isample;
+
+typedef struct {
+  long N;          /* FFT support (max(512, 8*2^floor(ln(np)+0.5)))   */
+  long np;         /* Nssp of the truth sensor + 1                    */
+  long nidx;       /* nact*nact                                       */
+  double lambda;   /* 1.65e-6 m                                       */
+  double dactupix; /* N/(3(np-1)) + 1                                 */
+} moao_isample_info;
+
+/* intersample_prepare + intersample_init with caller-provided tables instead of
+ * idx.fits / abs2fi.fits / otftel.fits (host arrays; idx is 1-based, nidx long;
+ * abs2fi and otf_tel are N*N doubles). */
+moao_status moao_intersample_create(moao_ctx* ctx, long nidx, long np, double Dtel,
+                                    const long* idx, const double* abs2fi,
+                                    const double* otf_tel, moao_isample** out);
+moao_status moao_intersample_get_info(const moao_isample* is, moao_isample_info* out);
+/* PSF (N x N, FFTW-unnormalised like the reference) from a DEVICE Cvv (nact^2,
+ * column-major) into a DEVICE buffer d_psf of N*N doubles. */
+moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, double* d_psf);
+/* Same with host Cvv in and host PSF out. */
+moao_status moao_intersample_process_host(moao_isample* is, const double* Cvv, double* psf);
+void moao_intersample_destroy(moao_isample* is);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOAO_B200_H */

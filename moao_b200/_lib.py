@@ -1,0 +1,114 @@
+"""ctypes bindings of ``include/moao_b200.h`` (the C ABI of libmoao_b200.so).
+
+The library is loaded from the package directory only; a missing or unloadable
+library raises immediately, so no code path can silently run without the CUDA
+implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmoao_b200.so")
+
+MOAO_OK = 0
+STATUS = {0: "MOAO_OK", 1: "MOAO_ERR_BAD_ARG", 2: "MOAO_ERR_NOT_SPD", 3: "MOAO_ERR_OOM",
+          4: "MOAO_ERR_CUDA", 5: "MOAO_ERR_IO", 6: "MOAO_ERR_TIMEOUT", 7: "MOAO_ERR_UNSUPPORTED",
+          8: "MOAO_ERR_BUSY", 9: "MOAO_ERR_CANCELLED"}
+PREC = {"fp64": 0, "mixed": 1}
+
+vp = C.c_void_p
+dp = C.c_void_p  # double* (device or host address as an integer)
+i32 = C.c_int
+i64 = C.c_long
+
+
+class TomoInfo(C.Structure):
+    _fields_ = [("nW", i32), ("nLgs", i32), ("nNgs", i32), ("nTarget", i32), ("nLayer", i32),
+                ("Nx", i32), ("nmeas", i64), ("nmeasts", i64), ("diam", C.c_double),
+                ("obs", C.c_double), ("lgsCst", C.c_double), ("nssp_ts", i32)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("info", i32), ("refine_steps", i32), ("refine_resid", C.c_double),
+                ("ms_factor", C.c_double), ("ms_solve", C.c_double), ("ms_refine", C.c_double)]
+
+
+class IsampleInfo(C.Structure):
+    _fields_ = [("N", i64), ("np", i64), ("nidx", i64), ("lambda_", C.c_double),
+                ("dactupix", C.c_double)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "moao_status_string": (C.c_char_p, [i32]),
+    "moao_last_error": (C.c_char_p, []),
+    "moao_tomo_create": (i32, [C.c_char_p, C.c_char_p, C.POINTER(vp)]),
+    "moao_tomo_update_atm": (i32, [vp, C.c_char_p]),
+    "moao_tomo_set_profile": (i32, [vp, i32, dp, dp, dp]),
+    "moao_tomo_set_target": (i32, [vp, i32]),
+    "moao_tomo_get_info": (i32, [vp, C.POINTER(TomoInfo)]),
+    "moao_tomo_table": (i64, [vp, C.c_char_p, dp, i64]),
+    "moao_tomo_destroy": (None, [vp]),
+    "moao_ctx_create": (i32, [i32, C.POINTER(vp)]),
+    "moao_ctx_destroy": (None, [vp]),
+    "moao_ctx_set_stream": (i32, [vp, vp]),
+    "moao_ctx_stream": (vp, [vp]),
+    "moao_ctx_synchronize": (i32, [vp]),
+    "moao_ctx_launch_count": (C.c_longlong, [vp]),
+    "moao_ctx_set_block": (i32, [vp, i32]),
+    "moao_matcov_tile": (i32, [vp, vp, dp, i32, i32, i32, i32, i32, i32]),
+    "moao_matcov_tile_host": (i32, [vp, vp, dp, i32, i32, i32, i32, i32, i32]),
+    "moao_reconstructor": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, i32, C.POINTER(SolveReport)]),
+    "moao_reconstructor_host": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, C.POINTER(SolveReport)]),
+    "moao_cee_cvv": (i32, [vp, i64, i64, i64] + [dp, i64] * 9),
+    "moao_cee_cvv_host": (i32, [vp, i64, i64, i64] + [dp, i64] * 9),
+    "moao_intersample_create": (i32, [vp, i64, i64, C.c_double, dp, dp, dp, C.POINTER(vp)]),
+    "moao_intersample_get_info": (i32, [vp, C.POINTER(IsampleInfo)]),
+    "moao_intersample_process": (i32, [vp, dp, dp]),
+    "moao_intersample_process_host": (i32, [vp, dp, dp]),
+    "moao_intersample_destroy": (None, [vp]),
+}
+
+
+class MoaoError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{where}: {self.name}" + (f" ({detail})" if detail else ""))
+
+
+class NotSPDError(MoaoError):
+    """Cholesky met a non-positive pivot; ``column`` is the 1-based column."""
+
+    def __init__(self, status, where, detail="", column=0):
+        super().__init__(status, where, detail)
+        self.column = column
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"moao_b200: {LIB_PATH} is missing; build it with `python -m moao_b200.build` "
+                "(the CUDA implementation is the only implementation)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str, **kw):
+    if status != MOAO_OK:
+        detail = lib().moao_last_error().decode(errors="replace")
+        if status == 2:
+            raise NotSPDError(status, where, detail, **kw)
+        raise MoaoError(status, where, detail)

@@ -1,0 +1,294 @@
+"""Host-side mirror of the reference's operator interface for the reconstructor path.
+
+Names, argument order and meaning follow the reference so code written against
+it reads the same:
+
+=======================  ==================================================
+this module              reference
+=======================  ==================================================
+``Tomo``                 ``Tomo_struct<T>`` (common/tomo_struct/tomo_struct.hpp:9)
+``matcov_tile``          ``MOAO_COMMON::matcov_tile`` (common/compute/matcov.cpp:17)
+``reconstructor``        ``MOAO_LAPACK::reconstructor`` (lapack/compute/reconstructor.cpp:32)
+``Cee_Cvv``              ``MOAO_LAPACK::Cee_Cvv`` (lapack/compute/cee_cvv.cpp:50)
+``Intersample``          ``intersample_prepare/_init/_process/_free``
+                         (common/tomo_struct/intersample.cpp:74-333)
+=======================  ==================================================
+
+Matrices are column-major with an explicit leading dimension, as in the
+reference. A matrix argument is either a CUDA ``torch.Tensor`` of float64
+(device path, asynchronous on the context stream) or a writable float64
+``numpy.ndarray`` (host path: copied to the GPU, computed there, copied back,
+keeping the reference's in-place contracts). Every computation runs in the
+CUDA library; there is no CPU implementation in this package.
+
+Error behaviour: an unknown ``type_mat`` (the reference exits) raises
+``MoaoError``; a non-positive Cholesky pivot (the reference prints and returns
+without solving) raises ``NotSPDError`` carrying the 1-based column, after Cmm
+has been partially overwritten and Ctm left untouched, as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from typing import Optional
+
+import numpy as np
+
+from ._lib import (IsampleInfo, MoaoError, NotSPDError, PREC, SolveReport, TomoInfo, check,
+                   lib)
+
+__all__ = ["Context", "Tomo", "matcov_tile", "reconstructor", "Cee_Cvv", "Intersample",
+           "default_context", "MoaoError", "NotSPDError"]
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x, what: str) -> int:
+    """Address of a float64 matrix argument plus a flag telling host or device."""
+    if _is_torch(x):
+        import torch
+        if x.dtype != torch.float64:
+            raise TypeError(f"{what}: expected float64, got {x.dtype}")
+        if not x.is_cuda:
+            raise TypeError(f"{what}: CPU torch tensors are not accepted; pass a CUDA tensor or a numpy array")
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        if x.dtype != np.float64:
+            raise TypeError(f"{what}: expected float64, got {x.dtype}")
+        if not (x.flags.c_contiguous or x.flags.f_contiguous):
+            raise ValueError(f"{what}: array must be contiguous")
+        return x.ctypes.data
+    raise TypeError(f"{what}: expected a CUDA torch.Tensor or a numpy.ndarray, got {type(x)}")
+
+
+def _on_device(*xs) -> bool:
+    kinds = {_is_torch(x) for x in xs if x is not None}
+    if len(kinds) > 1:
+        raise TypeError("mixing device tensors and host arrays in one call is not supported")
+    return kinds == {True}
+
+
+class Context:
+    """One device context: stream, cached device geometry, workspaces."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        h = C.c_void_p()
+        check(lib().moao_ctx_create(device, C.byref(h)), "moao_ctx_create")
+        self._h = h
+        self.device = device
+        if stream is not None:
+            self.set_stream(stream)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream: Optional[int]):
+        """Use an external cudaStream_t (an int handle, e.g. torch's
+        ``torch.cuda.current_stream().cuda_stream``); None = own stream."""
+        check(lib().moao_ctx_set_stream(self._h, C.c_void_p(stream) if stream else None),
+              "moao_ctx_set_stream")
+
+    @property
+    def stream(self) -> int:
+        return lib().moao_ctx_stream(self._h) or 0
+
+    def synchronize(self):
+        check(lib().moao_ctx_synchronize(self._h), "moao_ctx_synchronize")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().moao_ctx_launch_count(self._h))
+
+    def set_block(self, nb: int):
+        check(lib().moao_ctx_set_block(self._h, nb), "moao_ctx_set_block")
+
+    def close(self):
+        if self._h:
+            lib().moao_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx_lock = threading.Lock()
+_default: dict = {}
+
+
+def default_context(device: Optional[int] = None) -> Context:
+    if device is None:
+        try:
+            import torch
+            device = torch.cuda.current_device() if torch.cuda.is_available() else 0
+        except Exception:
+            device = 0
+    with _ctx_lock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+class Tomo:
+    """The system model (``Tomo_struct``): parameter files, valid subapertures,
+    LGS elongation, projected subapertures per layer and WFS noise."""
+
+    def __init__(self, sys_file: str, atm_file: str):
+        h = C.c_void_p()
+        check(lib().moao_tomo_create(os.fsencode(sys_file), os.fsencode(atm_file), C.byref(h)),
+              "moao_tomo_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def updateAtm(self, atm_file: str):
+        check(lib().moao_tomo_update_atm(self._h, os.fsencode(atm_file)), "moao_tomo_update_atm")
+
+    def set_profile(self, cn2, h, L0):
+        cn2 = np.ascontiguousarray(cn2, dtype=np.float64)
+        hh = np.ascontiguousarray(h, dtype=np.float64)
+        L0 = np.ascontiguousarray(np.broadcast_to(L0, cn2.shape), dtype=np.float64)
+        check(lib().moao_tomo_set_profile(self._h, len(cn2), cn2.ctypes.data, hh.ctypes.data,
+                                          L0.ctypes.data), "moao_tomo_set_profile")
+
+    def setTarget(self, idx: int):
+        check(lib().moao_tomo_set_target(self._h, idx), "moao_tomo_set_target")
+
+    @property
+    def info(self) -> TomoInfo:
+        i = TomoInfo()
+        check(lib().moao_tomo_get_info(self._h, C.byref(i)), "moao_tomo_get_info")
+        return i
+
+    def getNMeas(self) -> int:
+        return int(self.info.nmeas)
+
+    def getNMeasTS(self) -> int:
+        return int(self.info.nmeasts)
+
+    def table(self, name: str) -> np.ndarray:
+        n = lib().moao_tomo_table(self._h, name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        lib().moao_tomo_table(self._h, name.encode(), out.ctypes.data, n)
+        return out
+
+    def close(self):
+        if self._h:
+            lib().moao_tomo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def matcov_tile(data, nrows: int, ncols: int, xoffset: int, yoffset: int, lda: int, tomo: Tomo,
+                type_mat: int, ctx: Optional[Context] = None):
+    """Fill a tile of a covariance matrix (column-major, leading dimension lda).
+
+    type_mat 1: Cmm, lower triangle only (uplo='l'); 3: Ctm (truth sensor rows);
+    4: Ctt; 2: Cmt (truth sensor columns); 5: Cmm with both triangles."""
+    ctx = ctx or default_context()
+    p = _ptr(data, "matcov_tile data")
+    if _on_device(data):
+        check(lib().moao_matcov_tile(ctx.handle, tomo.handle, p, nrows, ncols, xoffset, yoffset,
+                                     lda, type_mat), "moao_matcov_tile")
+    else:
+        check(lib().moao_matcov_tile_host(ctx.handle, tomo.handle, p, nrows, ncols, xoffset,
+                                          yoffset, lda, type_mat), "moao_matcov_tile_host")
+
+
+def reconstructor(nmeas: int, nmeasts: int, Cmm, ldCmm: int, Ctm, ldCtm: int, ngal: int = 1,
+                  prec: str = "fp64", ctx: Optional[Context] = None) -> dict:
+    """R = Ctm Cmm^-1 in place in Ctm; Cmm is overwritten by its lower Cholesky
+    factor. Returns the solve report as a dict."""
+    ctx = ctx or default_context()
+    rep = SolveReport()
+    pc, pt = _ptr(Cmm, "Cmm"), _ptr(Ctm, "Ctm")
+    if _on_device(Cmm, Ctm):
+        st = lib().moao_reconstructor(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
+                                      PREC[prec], C.byref(rep))
+    else:
+        if prec != "fp64":
+            raise ValueError("the host-buffer reconstructor runs the FP64 path")
+        st = lib().moao_reconstructor_host(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
+                                           C.byref(rep))
+    check(st, "reconstructor", column=rep.info) if st == 2 else check(st, "reconstructor")
+    return {k: getattr(rep, k) for k, _ in SolveReport._fields_}
+
+
+def Cee_Cvv(nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx, ldDx, Cee,
+            ldCee, Cvv, ldCvv, Tmp, ldTmp, ctx: Optional[Context] = None):
+    """Cee = Ctt - Ctm R^T - R Ctm^T + R Cmm R^T ; Cvv = Dx Cee Dx^T (Cpp and Cpm
+    are destroyed, Tmp is scratch), exactly the reference's in-place contract."""
+    ctx = ctx or default_context()
+    mats = [Cmm, Cpp, Cpm, R, Dx, Cee, Cvv, Tmp]
+    names = ["Cmm", "Cpp", "Cpm", "R", "Dx", "Cee", "Cvv", "Tmp"]
+    lds = [ldCmm, ldCpp, ldCpm, ldR, ldDx, ldCee, ldCvv, ldTmp]
+    args = []
+    for m, n, ld in zip(mats, names, lds):
+        args += [_ptr(m, n), ld]
+    f = lib().moao_cee_cvv if _on_device(*mats) else lib().moao_cee_cvv_host
+    check(f(ctx.handle, nmeas, nmeasts, nact, *args), "Cee_Cvv")
+
+
+class Intersample:
+    """PSF from Cvv; the three input tables (idx, abs2fi, otf_tel) are given as
+    arrays instead of the reference's idx.fits / abs2fi.fits / otftel.fits."""
+
+    def __init__(self, nidx: int, np_: int, Dtel: float, idx, abs2fi, otf_tel,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        abs2fi = np.ascontiguousarray(abs2fi, dtype=np.float64)
+        otf_tel = np.ascontiguousarray(otf_tel, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().moao_intersample_create(self.ctx.handle, nidx, np_, Dtel, idx.ctypes.data,
+                                            abs2fi.ctypes.data, otf_tel.ctypes.data, C.byref(h)),
+              "moao_intersample_create")
+        self._h = h
+        info = IsampleInfo()
+        check(lib().moao_intersample_get_info(h, C.byref(info)), "moao_intersample_get_info")
+        self.N, self.np, self.nidx = int(info.N), int(info.np), int(info.nidx)
+        self.dactupix = float(info.dactupix)
+        self.lam = float(info.lambda_)
+
+    def process(self, Cvv, out=None):
+        """PSF (N x N, FFTW-unnormalised) of a Cvv given as a CUDA tensor (result
+        is a CUDA tensor) or a numpy array (result is a numpy array)."""
+        if _is_torch(Cvv):
+            import torch
+            if out is None:
+                out = torch.empty((self.N, self.N), dtype=torch.float64, device=Cvv.device)
+            check(lib().moao_intersample_process(self._h, _ptr(Cvv, "Cvv"), _ptr(out, "psf")),
+                  "moao_intersample_process")
+            return out
+        cvv = np.ascontiguousarray(Cvv, dtype=np.float64)
+        if out is None:
+            out = np.empty((self.N, self.N), dtype=np.float64)
+        check(lib().moao_intersample_process_host(self._h, cvv.ctypes.data, _ptr(out, "psf")),
+              "moao_intersample_process_host")
+        return out
+
+    def close(self):
+        if self._h:
+            lib().moao_intersample_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

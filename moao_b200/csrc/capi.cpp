@@ -1,0 +1,415 @@
+// C ABI: status strings, system model, device context, covariance entry points
+// and the host-buffer variants that keep the reference's in-place contracts.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "context.h"
+#include "dense.h"
+
+namespace moao {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+moao_status set_error(moao_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+moao_status DevBuf::ensure(size_t n) {
+  if (n <= bytes) return MOAO_OK;
+  release();
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    bytes = 0;
+    return set_error(MOAO_ERR_OOM, "cudaMalloc of " + std::to_string(n) + " bytes failed: " +
+                                       cudaGetErrorString(e));
+  }
+  bytes = n;
+  return MOAO_OK;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometry** out) {
+  const Tomo_struct<double>& t = tp->t;
+  GeomEntry& e = ctx->geom[tp];
+  if (e.version == t.version && e.g.nLayer == t.atm.nLayer) {
+    *out = &e.g;
+    return MOAO_OK;
+  }
+  const int nW = t.sys.nW, nL = t.atm.nLayer, Nx = t.Nx;
+  if (nW > kMaxWfs) return set_error(MOAO_ERR_UNSUPPORTED, "more than 16 WFS");
+  if (nL > kMaxLayers) return set_error(MOAO_ERR_UNSUPPORTED, "more than 128 layers");
+  DevGeometry g;
+  g.nW = nW; g.nLgs = t.sys.nLgs; g.nLayer = nL; g.Nx = Nx;
+  g.diam = t.sys.diam; g.lgsCst = t.sys.lgsCst;
+  int off = 0;
+  for (int w = 0; w < nW; ++w) {
+    g.Nsubap[w] = (int)t.Nsubap[w];
+    g.off[w] = off;
+    g.Nssp[w] = (int)t.Nssp[w];
+    off += (int)t.Nsubap[w];
+  }
+  // One host staging block, one copy.
+  const size_t nu = (size_t)nL * Nx;
+  const size_t nngs = (size_t)(nW - t.sys.nLgs);
+  const size_t nlay = 3 * (size_t)nL + (size_t)nW * nL;
+  const size_t total = 2 * nu + 2 * Nx + 3 * (size_t)Nx + nngs + nlay;
+  std::vector<double> h(total);
+  size_t p = 0;
+  auto put = [&](const double* src, size_t n) {
+    std::memcpy(h.data() + p, src, n * sizeof(double));
+    size_t at = p;
+    p += n;
+    return at;
+  };
+  const size_t ou = put(t.u.data(), nu), ov = put(t.v.data(), nu);
+  const size_t oX = put(t.X.data(), Nx), oY = put(t.Y.data(), Nx);
+  const size_t oxx = put(t.noiseLGSxx.data(), Nx), oyy = put(t.noiseLGSyy.data(), Nx);
+  const size_t oxy = put(t.noiseLGSxy.data(), Nx);
+  const size_t ongs = put(t.noiseNGS.data(), nngs);
+  const size_t olay = p;
+  const double pi = 3.1415926535897932384626433;
+  const double k1 = 0.1716613621245709486;
+  for (int l = 0; l < nL; ++l) {
+    const double L0 = t.L0diff[l];
+    h[olay + l] = 2 * pi / L0;                         // rodconan :107
+    h[olay + nL + l] = k1 * std::pow(L0, 5. / 3.0);    // rodconan :114
+    h[olay + 2 * nL + l] = t.atm.cn2[l];
+  }
+  for (int k = 0; k < nW * nL; ++k) h[olay + 3 * nL + k] = t.sspSizeL[k];
+  MOAO_TRY(e.buf.ensure(total * sizeof(double)));
+  double* d = e.buf.as<double>();
+  MOAO_CUDA_TRY(cudaMemcpyAsync(d, h.data(), total * sizeof(double), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  // h is pageable, so the copy has completed on return from the call above
+  // only for small sizes; synchronise before h goes out of scope.
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  g.u = d + ou; g.v = d + ov; g.X = d + oX; g.Y = d + oY;
+  g.noiseLGSxx = d + oxx; g.noiseLGSyy = d + oyy; g.noiseLGSxy = d + oxy;
+  g.noiseNGS = d + ongs; g.layer = d + olay;
+  e.g = g;
+  e.version = t.version;
+  *out = &e.g;
+  return MOAO_OK;
+}
+
+}  // namespace moao
+
+using namespace moao;
+
+extern "C" {
+
+const char* moao_status_string(moao_status s) {
+  switch (s) {
+    case MOAO_OK: return "MOAO_OK";
+    case MOAO_ERR_BAD_ARG: return "MOAO_ERR_BAD_ARG";
+    case MOAO_ERR_NOT_SPD: return "MOAO_ERR_NOT_SPD";
+    case MOAO_ERR_OOM: return "MOAO_ERR_OOM";
+    case MOAO_ERR_CUDA: return "MOAO_ERR_CUDA";
+    case MOAO_ERR_IO: return "MOAO_ERR_IO";
+    case MOAO_ERR_TIMEOUT: return "MOAO_ERR_TIMEOUT";
+    case MOAO_ERR_UNSUPPORTED: return "MOAO_ERR_UNSUPPORTED";
+    case MOAO_ERR_BUSY: return "MOAO_ERR_BUSY";
+    case MOAO_ERR_CANCELLED: return "MOAO_ERR_CANCELLED";
+  }
+  return "MOAO_ERR_UNKNOWN";
+}
+
+const char* moao_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------- system model
+moao_status moao_tomo_create(const char* sys_file, const char* atm_file, moao_tomo** out) {
+  if (!sys_file || !atm_file || !out) return set_error(MOAO_ERR_BAD_ARG, "tomo_create: null");
+  try {
+    std::unique_ptr<moao_tomo> t(new moao_tomo);
+    t->t = Tomo_struct<double>(sys_file, atm_file);
+    if (t->t.Nx <= 0) return set_error(MOAO_ERR_IO, "tomo_create: no valid subaperture");
+    *out = t.release();
+  } catch (const std::exception& ex) {
+    return set_error(MOAO_ERR_IO, ex.what());
+  }
+  return MOAO_OK;
+}
+
+moao_status moao_tomo_update_atm(moao_tomo* t, const char* atm_file) {
+  if (!t || !atm_file) return set_error(MOAO_ERR_BAD_ARG, "tomo_update_atm: null");
+  try {
+    t->t.updateAtm(atm_file);
+  } catch (const std::exception& ex) {
+    return set_error(MOAO_ERR_IO, ex.what());
+  }
+  return MOAO_OK;
+}
+
+moao_status moao_tomo_set_profile(moao_tomo* t, int nLayer, const double* cn2, const double* h,
+                                  const double* L0) {
+  if (!t || !cn2 || !h || !L0 || nLayer < 1)
+    return set_error(MOAO_ERR_BAD_ARG, "tomo_set_profile: bad arguments");
+  for (int l = 0; l < nLayer; ++l)
+    if (!(L0[l] > 0) || !std::isfinite(cn2[l]) || !std::isfinite(h[l]))
+      return set_error(MOAO_ERR_BAD_ARG, "tomo_set_profile: non-finite layer or L0 <= 0");
+  try {
+    t->t.setProfile(nLayer, cn2, h, L0);
+  } catch (const std::exception& ex) {
+    return set_error(MOAO_ERR_BAD_ARG, ex.what());
+  }
+  return MOAO_OK;
+}
+
+moao_status moao_tomo_set_target(moao_tomo* t, int target) {
+  if (!t) return set_error(MOAO_ERR_BAD_ARG, "tomo_set_target: null");
+  try {
+    t->t.setTarget(target);
+  } catch (const std::exception& ex) {
+    return set_error(MOAO_ERR_BAD_ARG, ex.what());
+  }
+  return MOAO_OK;
+}
+
+moao_status moao_tomo_get_info(const moao_tomo* tp, moao_tomo_info* o) {
+  if (!tp || !o) return set_error(MOAO_ERR_BAD_ARG, "tomo_get_info: null");
+  const Tomo_struct<double>& t = tp->t;
+  o->nW = t.sys.nW;
+  o->nLgs = t.sys.nLgs;
+  o->nNgs = t.sys.nNgs;
+  o->nTarget = t.sys.nTarget;
+  o->nLayer = t.atm.nLayer;
+  o->Nx = t.Nx;
+  o->nmeas = t.getNMeas();
+  o->nmeasts = t.getNMeasTS();
+  o->diam = t.sys.diam;
+  o->obs = t.sys.obs;
+  o->lgsCst = t.sys.lgsCst;
+  o->nssp_ts = (int)t.Nssp[t.sys.nW - 1];
+  return MOAO_OK;
+}
+
+long moao_tomo_table(const moao_tomo* tp, const char* name, double* out, long cap) {
+  if (!tp || !name) return -1;
+  const Tomo_struct<double>& t = tp->t;
+  const std::string n(name);
+  auto cp = [&](const auto& v) -> long {
+    const long len = (long)v.size();
+    if (out)
+      for (long i = 0; i < len && i < cap; ++i) out[i] = (double)v[i];
+    return len;
+  };
+  if (n == "u") return cp(t.u);
+  if (n == "v") return cp(t.v);
+  if (n == "X") return cp(t.X);
+  if (n == "Y") return cp(t.Y);
+  if (n == "sspSizeL") return cp(t.sspSizeL);
+  if (n == "L0diff")  // only the first nLayer entries are meaningful
+    return cp(std::vector<double>(t.L0diff.begin(), t.L0diff.begin() + t.atm.nLayer));
+  if (n == "cn2") return cp(t.atm.cn2);
+  if (n == "h") return cp(t.atm.h);
+  if (n == "Nsubap") return cp(t.Nsubap);
+  if (n == "Nssp") return cp(t.Nssp);
+  if (n == "noiseNGS") return cp(t.noiseNGS);
+  if (n == "noiseLGSxx") return cp(t.noiseLGSxx);
+  if (n == "noiseLGSyy") return cp(t.noiseLGSyy);
+  if (n == "noiseLGSxy") return cp(t.noiseLGSxy);
+  if (n == "alphaX") return cp(t.alphaX);
+  if (n == "alphaY") return cp(t.alphaY);
+  if (n == "lgsExt") return cp(t.lgsExt);
+  if (n == "lgsTheta") return cp(t.lgsTheta);
+  if (n == "mr") return cp(t.mr);
+  return -1;
+}
+
+void moao_tomo_destroy(moao_tomo* t) { delete t; }
+
+// ---------------------------------------------------------------- context
+moao_status moao_ctx_create(int device, moao_ctx** out) {
+  if (!out) return set_error(MOAO_ERR_BAD_ARG, "ctx_create: null");
+  int n = 0;
+  MOAO_CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return set_error(MOAO_ERR_BAD_ARG, "ctx_create: no such device");
+  MOAO_CUDA_TRY(cudaSetDevice(device));
+  std::unique_ptr<moao_ctx> c(new moao_ctx);
+  c->device = device;
+  MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+  c->stream = c->own_stream;
+  for (auto& e : c->ev) MOAO_CUDA_TRY(cudaEventCreate(&e));
+  *out = c.release();
+  return MOAO_OK;
+}
+
+void moao_ctx_destroy(moao_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->geom) kv.second.buf.release();
+  c->ws_w.release();
+  c->ws_dinv.release();
+  c->ws_info.release();
+  c->ws_tmp.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+moao_status moao_ctx_set_stream(moao_ctx* c, void* stream) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_stream: null");
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return MOAO_OK;
+}
+
+void* moao_ctx_stream(moao_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+moao_status moao_ctx_synchronize(moao_ctx* c) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_synchronize: null");
+  MOAO_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return MOAO_OK;
+}
+
+long long moao_ctx_launch_count(const moao_ctx* c) { return c ? c->launches : 0; }
+
+moao_status moao_ctx_set_block(moao_ctx* c, int nb) {
+  if (!c || nb < 64 || nb % 64 != 0 || nb > 2048)
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_block: nb must be a multiple of 64 in [64, 2048]");
+  c->nb = nb;
+  return MOAO_OK;
+}
+
+// ---------------------------------------------------------------- matcov
+moao_status moao_matcov_tile(moao_ctx* ctx, const moao_tomo* t, double* d_data, int nrows,
+                             int ncols, int xoffset, int yoffset, int lda, int type_mat) {
+  if (!ctx || !t) return set_error(MOAO_ERR_BAD_ARG, "matcov_tile: null");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  const DevGeometry* g = nullptr;
+  MOAO_TRY(device_geometry(ctx, t, &g));
+  return launch_matcov(*g, d_data, nrows, ncols, xoffset, yoffset, lda, type_mat, ctx->stream,
+                       &ctx->launches);
+}
+
+moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_data, int nrows,
+                                  int ncols, int xoffset, int yoffset, int lda, int type_mat) {
+  if (!ctx || !t || !h_data) return set_error(MOAO_ERR_BAD_ARG, "matcov_tile_host: null");
+  if (nrows <= 0 || ncols <= 0) return MOAO_OK;
+  if (lda < nrows) return set_error(MOAO_ERR_BAD_ARG, "matcov_tile_host: lda < nrows");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  const DevGeometry* g = nullptr;
+  MOAO_TRY(device_geometry(ctx, t, &g));
+  const size_t bytes = sizeof(double) * (size_t)nrows * ncols;
+  MOAO_TRY(ctx->ws_tmp.ensure(bytes));
+  double* d = ctx->ws_tmp.as<double>();
+  // Elements the reference leaves untouched (upper triangle of Cmm) must keep
+  // the caller's values, so the tile goes down and comes back.
+  MOAO_CUDA_TRY(cudaMemcpy2DAsync(d, sizeof(double) * nrows, h_data, sizeof(double) * lda,
+                                  sizeof(double) * nrows, ncols, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, ctx->stream,
+                         &ctx->launches));
+  MOAO_CUDA_TRY(cudaMemcpy2DAsync(h_data, sizeof(double) * lda, d, sizeof(double) * nrows,
+                                  sizeof(double) * nrows, ncols, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return MOAO_OK;
+}
+
+// ---------------------------------------------------------------- host variants
+moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, double* Cmm,
+                                    long ldCmm, double* Ctm, long ldCtm, long ngal,
+                                    moao_solve_report* rep) {
+  if (!ctx || !Cmm || !Ctm) return set_error(MOAO_ERR_BAD_ARG, "reconstructor_host: null");
+  if (nmeas <= 0 || nmeasts <= 0 || ngal <= 0 || ldCmm < nmeas || ldCtm < nmeasts)
+    return set_error(MOAO_ERR_BAD_ARG, "reconstructor_host: bad sizes");
+  double *dC = nullptr, *dT = nullptr;
+  const size_t cb = sizeof(double) * (size_t)nmeas * nmeas;
+  const size_t tspan = (size_t)nmeas * nmeasts * (ngal - 1) + (size_t)ldCtm * (nmeas - 1) + nmeasts;
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  if (cudaMalloc(&dC, cb) != cudaSuccess) return set_error(MOAO_ERR_OOM, "reconstructor_host: Cmm");
+  if (cudaMalloc(&dT, sizeof(double) * tspan) != cudaSuccess) {
+    cudaFree(dC);
+    return set_error(MOAO_ERR_OOM, "reconstructor_host: Ctm");
+  }
+  moao_status st = MOAO_OK;
+  cudaStream_t s = ctx->stream;
+  auto fail = [&](cudaError_t e) {
+    if (e != cudaSuccess) st = set_error(MOAO_ERR_CUDA, cudaGetErrorString(e));
+    return e != cudaSuccess;
+  };
+  if (!fail(cudaMemcpy2DAsync(dC, sizeof(double) * nmeas, Cmm, sizeof(double) * ldCmm,
+                              sizeof(double) * nmeas, nmeas, cudaMemcpyHostToDevice, s)) &&
+      !fail(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice, s))) {
+    st = moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, MOAO_PREC_FP64, rep);
+    // On a failed factorisation the reference has already overwritten Cmm
+    // (partially) and leaves Ctm alone; mirror that.
+    if (!fail(cudaMemcpy2DAsync(Cmm, sizeof(double) * ldCmm, dC, sizeof(double) * nmeas,
+                                sizeof(double) * nmeas, nmeas, cudaMemcpyDeviceToHost, s)) &&
+        st == MOAO_OK)
+      fail(cudaMemcpyAsync(Ctm, dT, sizeof(double) * tspan, cudaMemcpyDeviceToHost, s));
+    cudaStreamSynchronize(s);
+  }
+  cudaFree(dC);
+  cudaFree(dT);
+  return st;
+}
+
+moao_status moao_cee_cvv_host(moao_ctx* ctx, long nmeas, long nmeasts, long nact, double* Cmm,
+                              long ldCmm, double* Cpp, long ldCpp, double* Cpm, long ldCpm,
+                              double* R, long ldR, double* Dx, long ldDx, double* Cee,
+                              long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp) {
+  if (!ctx) return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv_host: null");
+  struct Mat { double* h; long ld, m, n; double* d; bool in, out; };
+  Mat mats[] = {{Cmm, ldCmm, nmeas, nmeas, nullptr, true, false},
+                {Cpp, ldCpp, nmeasts, nmeasts, nullptr, true, true},
+                {Cpm, ldCpm, nmeasts, nmeas, nullptr, true, true},
+                {R, ldR, nmeasts, nmeas, nullptr, true, false},
+                {Dx, ldDx, nact, nmeasts, nullptr, true, false},
+                {Cee, ldCee, nmeasts, nmeasts, nullptr, false, true},
+                {Cvv, ldCvv, nact, nact, nullptr, false, true},
+                {Tmp, ldTmp, nact, nmeasts, nullptr, false, true}};
+  for (auto& m : mats)
+    if (!m.h || m.ld < std::max(1L, m.m) || m.m < 0 || m.n < 0)
+      return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv_host: bad matrix argument");
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  moao_status st = MOAO_OK;
+  for (auto& m : mats) {
+    if (cudaMalloc(&m.d, sizeof(double) * std::max(1L, m.m * m.n)) != cudaSuccess) {
+      st = set_error(MOAO_ERR_OOM, "Cee_Cvv_host: device allocation");
+      break;
+    }
+    if (m.in && m.m * m.n > 0 &&
+        cudaMemcpy2DAsync(m.d, sizeof(double) * m.m, m.h, sizeof(double) * m.ld,
+                          sizeof(double) * m.m, m.n, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+      st = set_error(MOAO_ERR_CUDA, "Cee_Cvv_host: H2D");
+      break;
+    }
+  }
+  if (st == MOAO_OK)
+    st = moao_cee_cvv(ctx, nmeas, nmeasts, nact, mats[0].d, std::max(1L, nmeas), mats[1].d,
+                      std::max(1L, nmeasts), mats[2].d, std::max(1L, nmeasts), mats[3].d,
+                      std::max(1L, nmeasts), mats[4].d, std::max(1L, nact), mats[5].d,
+                      std::max(1L, nmeasts), mats[6].d, std::max(1L, nact), mats[7].d,
+                      std::max(1L, nact));
+  if (st == MOAO_OK)
+    for (auto& m : mats)
+      if (m.out && m.m * m.n > 0 &&
+          cudaMemcpy2DAsync(m.h, sizeof(double) * m.ld, m.d, sizeof(double) * m.m,
+                            sizeof(double) * m.m, m.n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        st = set_error(MOAO_ERR_CUDA, "Cee_Cvv_host: D2H");
+  cudaStreamSynchronize(s);
+  for (auto& m : mats)
+    if (m.d) cudaFree(m.d);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Per-device context: stream, cached device geometry, factorisation workspace.
+#ifndef MOAO_CONTEXT_H
+#define MOAO_CONTEXT_H
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+
+#include "moao_b200_tomo.hpp"
+#include "moao_internal.h"
+
+struct moao_tomo {
+  Tomo_struct<double> t;
+};
+
+namespace moao {
+
+// A device buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  moao_status ensure(size_t n);
+  void release();
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+struct GeomEntry {
+  unsigned long long version = ~0ull;
+  DevGeometry g;
+  DevBuf buf;  // backing store of every array in g
+};
+
+}  // namespace moao
+
+struct moao_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  int nb = 256;  // outer panel width of the blocked factorisation
+  std::mutex mu;
+  std::map<const moao_tomo*, moao::GeomEntry> geom;
+  moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
+  cudaEvent_t ev[8] = {};
+};
+
+namespace moao {
+
+// Uploads (or reuses) the device copy of a tomo's geometry tables.
+moao_status device_geometry(moao_ctx* ctx, const moao_tomo* t, const DevGeometry** out);
+
+// FP64 blocked Cholesky (lower, in place) of the n x n matrix A; fills dinv
+// (n x nb, ld n) with the inverse of every diagonal block. info receives the
+// first failing column (1-based) or 0.
+moao_status potrf_f64(moao_ctx* ctx, double* A, long lda, long n, double* dinv, int* d_info);
+// R = B * L^-T * L^-1 in place on B (m x n, ldb) using the factor and dinv.
+moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, const double* dinv,
+                            double* B, long ldb, long m);
+
+}  // namespace moao
+
+#endif  // MOAO_CONTEXT_H

@@ -1,0 +1,406 @@
+// FP64 dense kernels for the plain-FP64 reconstructor path.
+//
+// Blackwell has no FP64 kind for tcgen05.mma, so FP64 contractions run on the
+// FP64 DMMA path (mma.sync m8n8k4 .f64), fed by a 4-stage cp.async pipeline of
+// 128x128x16 tiles in shared memory (bank-conflict-free padded layouts). One
+// kernel template serves every contraction of the path:
+//   trailing SYRK of the tiled Cholesky   (transB, lowerC)
+//   panel TRSM as a product with the inverse diagonal block
+//   the two triangular solves of R        (NN / NT)
+//   SYR2K / SYMM / GEMM of the Cee/Cvv chain (triB masks a lower-stored
+//   symmetric operand; no symmetric copy is ever materialised)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "dense.h"
+
+namespace moao {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int STAGES = 4;
+constexpr int NTHREADS = 256;
+constexpr int PAD_MN = 4;  // doubles of padding on m/n-contiguous rows
+constexpr int PAD_K = 4;   // doubles of padding on k-contiguous rows
+constexpr int LDA_S = BM + PAD_MN;  // As[k][m]
+constexpr int LDB_S = BN + PAD_MN;  // Bs[k][n]   (transB)
+constexpr int LDBT_S = BK + PAD_K;  // Bs[n][k]   (!transB)
+constexpr int A_STAGE = BK * LDA_S;
+constexpr int B_STAGE = (BK * LDB_S > BN * LDBT_S) ? BK * LDB_S : BN * LDBT_S;
+constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+
+__device__ __forceinline__ void cp_async(double* smem, const double* gmem, int vec, int valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = valid * 8;
+  if (vec == 2) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(bytes));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(bytes));
+  }
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+struct KParams {
+  long M, N, K;
+  double alpha, beta;
+  const double* A;
+  long lda;
+  const double* B;
+  long ldb;
+  double* C;
+  long ldc;
+  int triB;
+};
+
+// Load one BK-slice of an MN-contiguous operand (A, or B when transB): the tile
+// rows r0..r0+127 of columns k0..k0+15 of a column-major rows x K matrix.
+template <int VEC>
+__device__ __forceinline__ void load_mn_tile(double* s, const double* g, long ld, long rows,
+                                             long K, long r0, long k0) {
+  constexpr int CH = BM / VEC;           // chunks per k column
+  constexpr int TOTAL = CH * BK;
+  for (int c = threadIdx.x; c < TOTAL; c += NTHREADS) {
+    const int kk = c / CH, rr = (c % CH) * VEC;
+    const long gr = r0 + rr, gk = k0 + kk;
+    int valid = 0;
+    if (gk < K && gr < rows) valid = (int)min((long)VEC, rows - gr);
+    const double* src = valid ? g + gk * ld + gr : g;
+    cp_async(s + kk * LDA_S + rr, src, VEC, valid);
+  }
+}
+
+// Load one BK-slice of a K-contiguous operand (B when !transB): rows k0..k0+15
+// of columns n0..n0+127 of a column-major K x N matrix, stored Bs[n][k].
+template <int VEC>
+__device__ __forceinline__ void load_k_tile(double* s, const double* g, long ld, long N,
+                                            long K, long n0, long k0) {
+  constexpr int CH = BK / VEC;
+  constexpr int TOTAL = CH * BN;
+  for (int c = threadIdx.x; c < TOTAL; c += NTHREADS) {
+    const int nn = c / CH, kk = (c % CH) * VEC;
+    const long gn = n0 + nn, gk = k0 + kk;
+    int valid = 0;
+    if (gn < N && gk < K) valid = (int)min((long)VEC, K - gk);
+    const double* src = valid ? g + gn * ld + gk : g;
+    cp_async(s + nn * LDBT_S + kk, src, VEC, valid);
+  }
+}
+
+template <bool TRANSB, bool LOWERC, int VEC>
+__global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) {
+  extern __shared__ __align__(16) double smem[];
+  double* As = smem;
+  double* Bs = smem + STAGES * A_STAGE;
+
+  const long m0 = (long)blockIdx.x * BM, n0 = (long)blockIdx.y * BN;
+  if (LOWERC && m0 + BM <= n0) return;  // tile strictly above the diagonal
+
+  // K range (tile aligned); a triangular B limits it.
+  long kb = 0, ke = p.K;
+  if (p.triB != 0) {
+    if (!TRANSB) kb = n0;                      // B(k, n) with k >= n
+    else ke = min(p.K, n0 + BN);               // B(n, k) with n >= k
+  }
+  kb = (kb / BK) * BK;
+  const int ntiles = (ke > kb) ? (int)((ke - kb + BK - 1) / BK) : 0;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int gid = lane >> 2, tig = lane & 3;
+
+  double acc[8][4][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  auto issue = [&](int stage, int t) {
+    const long k0 = kb + (long)t * BK;
+    load_mn_tile<VEC>(As + stage * A_STAGE, p.A, p.lda, p.M, p.K, m0, k0);
+    if (TRANSB) load_mn_tile<VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
+    else load_k_tile<VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
+  };
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ntiles) issue(s, s);
+    cp_commit();
+  }
+
+  for (int t = 0; t < ntiles; ++t) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const int stage = t % STAGES;
+    double* as = As + stage * A_STAGE;
+    double* bs = Bs + stage * B_STAGE;
+    if (p.triB != 0) {
+      // Zero the entries of the stored B outside its lower (or strictly lower)
+      // triangle when this slice crosses the diagonal.
+      const long k0 = kb + (long)t * BK;
+      const bool crosses = TRANSB ? (k0 + BK - 1 >= n0) : (k0 <= n0 + BN - 1);
+      if (crosses) {
+        for (int e = threadIdx.x; e < BK * BN; e += NTHREADS) {
+          const int kk = e / BN, nn = e % BN;
+          const long gk = k0 + kk, gn = n0 + nn;
+          // stored row / column of this element
+          const long row = TRANSB ? gn : gk, col = TRANSB ? gk : gn;
+          const bool keep = (p.triB == 1) ? (row >= col) : (row > col);
+          if (!keep) {
+            if (TRANSB) bs[kk * LDB_S + nn] = 0.0;
+            else bs[nn * LDBT_S + kk] = 0.0;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    {
+      const int nt = t + STAGES - 1;
+      if (nt < ntiles) issue(nt % STAGES, nt);
+      cp_commit();
+    }
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = as[(k4 + tig) * LDA_S + wm + i * 8 + gid];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (TRANSB) b[j] = bs[(k4 + tig) * LDB_S + wn + j * 8 + gid];
+        else b[j] = bs[(wn + j * 8 + gid) * LDBT_S + k4 + tig];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  cp_wait<0>();
+
+  // Epilogue: C = alpha * acc + beta * C (C is not read when beta == 0).
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long r = m0 + wm + i * 8 + gid;
+    if (r >= p.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long c = n0 + wn + j * 8 + 2 * tig + h;
+        if (c >= p.N) continue;
+        if (LOWERC && r < c) continue;
+        double* dst = p.C + c * p.ldc + r;
+        double v = p.alpha * acc[i][j][h];
+        if (p.beta != 0.0) v += p.beta * *dst;
+        *dst = v;
+      }
+    }
+  }
+}
+
+template <bool TRANSB, bool LOWERC, int VEC>
+moao_status launch_gemm(const KParams& p, cudaStream_t s) {
+  static bool configured = false;
+  auto kern = gemm_f64_kernel<TRANSB, LOWERC, VEC>;
+  if (!configured) {
+    MOAO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SMEM_BYTES));
+    configured = true;
+  }
+  dim3 grid((unsigned)((p.M + BM - 1) / BM), (unsigned)((p.N + BN - 1) / BN));
+  kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(p);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// ---------------------------------------------------------------------------
+// Leaf factorisation of a diagonal block (n <= 64) in shared memory, fused with
+// the inversion of the resulting triangular factor.
+// ---------------------------------------------------------------------------
+constexpr int LEAF = 64;
+constexpr int LEAF_LD = LEAF + 1;
+
+__global__ void __launch_bounds__(256) potrf_inv_leaf_kernel(double* A, long lda, double* Linv,
+                                                             long ldi, int n, long col0,
+                                                             int* info) {
+  extern __shared__ __align__(16) double leaf_smem[];
+  double* L = leaf_smem;                 // L[i + j*LEAF_LD]
+  double* W = leaf_smem + LEAF * LEAF_LD;  // inverse
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < LEAF * LEAF; e += blockDim.x) {
+    const int i = e % LEAF, j = e / LEAF;
+    L[i + j * LEAF_LD] = (i < n && j < n && i >= j) ? A[(long)j * lda + i] : 0.0;
+    W[i + j * LEAF_LD] = 0.0;
+  }
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  // Right-looking column Cholesky.
+  for (int j = 0; j < n; ++j) {
+    if (tid == 0) {
+      const double d = L[j + j * LEAF_LD];
+      if (!(d > 0.0)) {
+        if (!s_bad) {
+          s_bad = 1;
+          atomicCAS(info, 0, (int)(col0 + j + 1));
+        }
+        L[j + j * LEAF_LD] = 1.0;  // keep going without NaNs; info reports it
+      } else {
+        L[j + j * LEAF_LD] = sqrt(d);
+      }
+    }
+    __syncthreads();
+    const double piv = L[j + j * LEAF_LD];
+    for (int i = j + 1 + tid; i < n; i += blockDim.x) L[i + j * LEAF_LD] /= piv;
+    __syncthreads();
+    const int rem = n - j - 1;
+    for (int e = tid; e < rem * rem; e += blockDim.x) {
+      const int i = j + 1 + e % rem, k = j + 1 + e / rem;
+      if (i >= k) L[i + k * LEAF_LD] -= L[i + j * LEAF_LD] * L[k + j * LEAF_LD];
+    }
+    __syncthreads();
+  }
+  // Inverse of the lower factor, one column per thread (forward substitution).
+  if (tid < n) {
+    const int j = tid;
+    W[j + j * LEAF_LD] = 1.0 / L[j + j * LEAF_LD];
+    for (int i = j + 1; i < n; ++i) {
+      double sum = 0.0;
+      for (int k = j; k < i; ++k) sum += L[i + k * LEAF_LD] * W[k + j * LEAF_LD];
+      W[i + j * LEAF_LD] = -sum / L[i + i * LEAF_LD];
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    if (i >= j) A[(long)j * lda + i] = L[i + j * LEAF_LD];
+    Linv[(long)j * ldi + i] = W[i + j * LEAF_LD];
+  }
+}
+
+__global__ void copy_kernel(const double* __restrict__ src, long lds, double* __restrict__ dst,
+                            long ldd, long m, long n) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    dst[j * ldd + i] = src[j * lds + i];
+  }
+}
+
+__global__ void fill_kernel(double* A, long lda, long m, long n, double v) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    A[j * lda + i] = v;
+  }
+}
+
+// Cee(i, j) = Cpp(max(i,j), min(i,j)); the diagonal goes through 2d * 0.5
+// exactly like the reference's geadd + scal sequence.
+__global__ void sym_from_lower_kernel(const double* __restrict__ P, long ldp,
+                                      double* __restrict__ E, long lde, long n) {
+  const long total = n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, j = e / n;
+    double v;
+    if (i > j) v = P[j * ldp + i];
+    else if (i < j) v = P[i * ldp + j];
+    else v = (P[j * ldp + i] + P[j * ldp + i]) * 0.5;
+    E[j * lde + i] = v;
+  }
+}
+
+unsigned grid_for(long total) {
+  long b = (total + 255) / 256;
+  return (unsigned)std::max(1L, std::min(b, 148L * 16));
+}
+
+}  // namespace
+
+moao_status gemm_f64(const GemmArgs& g, cudaStream_t s, long long* launches) {
+  if (g.M < 0 || g.N < 0 || g.K < 0) return set_error(MOAO_ERR_BAD_ARG, "gemm: negative size");
+  if (g.M == 0 || g.N == 0) return MOAO_OK;
+  if (g.lowerC && g.triB != TRI_FULL)
+    return set_error(MOAO_ERR_UNSUPPORTED, "gemm: lowerC with a triangular B");
+  if (g.lda < std::max(1L, g.M) || g.ldc < std::max(1L, g.M) ||
+      g.ldb < std::max(1L, g.transB ? g.N : g.K))
+    return set_error(MOAO_ERR_BAD_ARG, "gemm: leading dimension too small");
+  KParams p{g.M, g.N, g.K, g.alpha, g.beta, g.A, g.lda, g.B, g.ldb, g.C, g.ldc, (int)g.triB};
+  if (g.K == 0) {  // C = beta C
+    p.alpha = 0.0;
+  }
+  const bool v2 = aligned16(g.A) && aligned16(g.B) && (g.lda % 2 == 0) && (g.ldb % 2 == 0);
+  moao_status st;
+  if (v2) {
+    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 2>(p, s) : launch_gemm<true, false, 2>(p, s);
+    else st = g.lowerC ? launch_gemm<false, true, 2>(p, s) : launch_gemm<false, false, 2>(p, s);
+  } else {
+    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 1>(p, s) : launch_gemm<true, false, 1>(p, s);
+    else st = g.lowerC ? launch_gemm<false, true, 1>(p, s) : launch_gemm<false, false, 1>(p, s);
+  }
+  if (st == MOAO_OK && launches) ++*launches;
+  return st;
+}
+
+moao_status potrf_inv_leaf(double* A, long lda, double* Linv, long ldi, int n, long col0,
+                           int* d_info, cudaStream_t s, long long* launches) {
+  if (n <= 0) return MOAO_OK;
+  if (n > LEAF) return set_error(MOAO_ERR_BAD_ARG, "potrf leaf: n > 64");
+  static bool configured = false;
+  const int smem = 2 * LEAF * LEAF_LD * (int)sizeof(double);
+  if (!configured) {
+    MOAO_CUDA_TRY(cudaFuncSetAttribute(potrf_inv_leaf_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured = true;
+  }
+  potrf_inv_leaf_kernel<<<1, 256, smem, s>>>(A, lda, Linv, ldi, n, col0, d_info);
+  if (launches) ++*launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status copy_matrix(const double* src, long lds, double* dst, long ldd, long m, long n,
+                        cudaStream_t s) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  MOAO_CUDA_TRY(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double),
+                                  m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+  return MOAO_OK;
+}
+
+moao_status fill_matrix(double* A, long lda, long m, long n, double v, cudaStream_t s,
+                        long long* launches) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  fill_kernel<<<grid_for(m * n), 256, 0, s>>>(A, lda, m, n, v);
+  if (launches) ++*launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status sym_from_lower(const double* Cpp, long ldp, double* Cee, long lde, long n,
+                           cudaStream_t s, long long* launches) {
+  if (n <= 0) return MOAO_OK;
+  sym_from_lower_kernel<<<grid_for(n * n), 256, 0, s>>>(Cpp, ldp, Cee, lde, n);
+  if (launches) ++*launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+}  // namespace moao

@@ -1,0 +1,388 @@
+// Covariance generation on sm_100a: Cmm, Ctm, Ctt tiles from the von Karman
+// phase structure function.
+//
+// Model (restated from the reference, common/kernels/matcov_kernels.cpp):
+//   DPHI(r) = k1 L0^(5/3) f(2 pi r / L0)                          rodconan :92
+//   f(x) = -x^(5/6) K_5/6(x) series (x <= Xlim)                   macdo_x56 :38
+//   f(x) = k2 - k3 e^-x x^(1/3) (1 + a1/x + a2/x^2 + a3/x^3)      asymp_macdo :65
+//   slope covariances are 4-point DPHI stencils                    cov_XX_gb.. :147-193
+//   element = sum over layers of 0.5 cov kk cn2 (+ WFS noise)      compute_element_tiled_4 :206
+//   Ctt uses the unprojected truth-sensor positions                compute_element_ts_tile :423
+//
+// Work decomposition (B200): one thread owns one subaperture pair (i, j) and
+// produces the 2x2 slope block {x_i, y_i} x {x_j, y_j} of that pair, so the
+// geometry decode, the per-layer loads and the separation are shared by the
+// four covariances. When the two WFS have the same subaperture size on a layer
+// (every NGS/NGS and equal-altitude LGS/LGS pair) the 16 stencil points of the
+// block collapse to 9 distinct DPHI evaluations. Per-layer constants
+// (2 pi / L0, k1 L0^(5/3), 0.5 kk cn2) are hoisted to shared memory. The
+// kernel is bound by FP64 pipe throughput (cbrt / exp / an 11-term polynomial
+// per DPHI), not by HBM: each 8-byte store costs ~10^3 FP64 operations.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "moao_internal.h"
+
+namespace moao {
+namespace {
+
+// Constants of the reference model (common/moao_defs.h:15-38).
+__constant__ double c_Ga[11] = {0,
+                                12.067619015983075,
+                                5.17183672113560444,
+                                0.795667187867016068,
+                                0.0628158306210802181,
+                                0.00301515986981185091,
+                                9.72632216068338833e-05,
+                                2.25320204494595251e-06,
+                                3.93000356676612095e-08,
+                                5.34694362825451923e-10,
+                                5.83302941264329804e-12};
+__constant__ double c_Gma[11] = {-3.74878707653729304,   -2.04479295083852408,
+                                 -0.360845814853857083,  -0.0313778969438136685,
+                                 -0.001622994669507603,  -5.56455315259749673e-05,
+                                 -1.35720808599938951e-06, -2.47515152461894642e-08,
+                                 -3.50257291219662472e-10, -3.95770950530691961e-12,
+                                 -3.65327031259100284e-14};
+constexpr double kPi = 3.1415926535897932384626433;
+constexpr double kK1 = 0.1716613621245709486;
+constexpr double kK2 = 1.00563491799858928388289314170833;
+constexpr double kK3 = 1.25331413731550012081;
+constexpr double kA1 = 0.22222222222222222222;
+constexpr double kA2 = -0.08641975308641974829;
+constexpr double kA3 = 0.08001828989483310284;
+constexpr double kXlim = 0.75 * 2 * kPi;
+constexpr double kLambda2 = 0.00026942094446267851;  // (lambda/(2 pi) rasc)^2
+
+// f(x) / (k1 L0^(5/3)) for x = 2 pi r / L0 >= 0 (so that DPHI = amp * f).
+__device__ __forceinline__ double dphi_unit(double x) {
+  if (x > kXlim) {
+    const double xi = 1.0 / x;
+    return kK2 - kK3 * exp(-x) * cbrt(x) * (1.0 + xi * (kA1 + xi * (kA2 + xi * kA3)));
+  }
+  const double c = cbrt(x);
+  const double x2a = x * c * c;  // x^(5/3)
+  const double z = 0.25 * x * x;  // (x/2)^2
+  double pg = c_Gma[10];
+#pragma unroll
+  for (int n = 9; n >= 0; --n) pg = fma(pg, z, c_Gma[n]);
+  double pa = c_Ga[10];
+#pragma unroll
+  for (int n = 9; n >= 1; --n) pa = fma(pa, z, c_Ga[n]);
+  return -0.5 * (x2a * pg + z * pa);
+}
+
+__device__ __forceinline__ double D(double x, double y, double tpl) {
+  return dphi_unit(tpl * sqrt(x * x + y * y));
+}
+
+constexpr int kMaxJobs = 160;
+constexpr int kTileI = 32;
+constexpr int kTileJ = 8;
+
+struct Job {
+  int m, n;        // row WFS, column WFS
+  int i0, ni;      // subaperture range of the row WFS
+  int j0, nj;      // subaperture range of the column WFS
+  int rb, cb;      // global row / column of the first slope of each WFS
+  int tiles_i, tile_base;
+};
+
+struct LaunchDesc {
+  int njobs, total_tiles, type;
+  int r0, c0, nrows, ncols;
+  long long ld;
+  Job jobs[kMaxJobs];
+};
+
+// Element bits: 1 = (x_i, x_j), 2 = (x_i, y_j), 4 = (y_i, x_j), 8 = (y_i, y_j).
+template <typename OutT>
+__global__ void __launch_bounds__(kTileI* kTileJ)
+    matcov_block_kernel(const __grid_constant__ LaunchDesc d, const DevGeometry g,
+                        OutT* __restrict__ out) {
+  __shared__ double s_tpl[kMaxLayers], s_amp[kMaxLayers], s_w[kMaxLayers];
+  __shared__ double s_sm[kMaxLayers], s_sn[kMaxLayers];
+  __shared__ int s_job;
+
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    int k = 0;
+    while (k + 1 < d.njobs && d.jobs[k + 1].tile_base <= (int)blockIdx.x) ++k;
+    s_job = k;
+  }
+  __syncthreads();
+  const Job& jb = d.jobs[s_job];
+  const int nL = g.nLayer;
+  const int m = jb.m, n = jb.n;
+  const double sspm = g.diam / g.Nssp[m], sspn = g.diam / g.Nssp[n];
+  const double kk = kLambda2 / (sspm * sspn);
+  for (int l = threadIdx.y * kTileI + threadIdx.x; l < nL; l += kTileI * kTileJ) {
+    s_tpl[l] = g.layer[l];
+    s_amp[l] = g.layer[nL + l];
+    s_w[l] = 0.5 * kk * g.layer[2 * nL + l];
+    s_sm[l] = g.layer[3 * nL + m * nL + l];
+    s_sn[l] = g.layer[3 * nL + n * nL + l];
+  }
+  __syncthreads();
+
+  const int t = blockIdx.x - jb.tile_base;
+  const int ti = t % jb.tiles_i, tj = t / jb.tiles_i;
+  const int i = jb.i0 + ti * kTileI + threadIdx.x;
+  const int j = jb.j0 + tj * kTileJ + threadIdx.y;
+  if (i >= jb.i0 + jb.ni || j >= jb.j0 + jb.nj) return;
+
+  const int Nm = g.Nsubap[m], Nn = g.Nsubap[n];
+  const int rx = jb.rb + i, ry = jb.rb + Nm + i;
+  const int cx = jb.cb + j, cy = jb.cb + Nn + j;
+  const int r1 = d.r0 + d.nrows, c1 = d.c0 + d.ncols;
+  const bool lower = (d.type == 1 || d.type == 5);
+  auto want = [&](int r, int c) {
+    return r >= d.r0 && r < r1 && c >= d.c0 && c < c1 && (!lower || r >= c);
+  };
+  unsigned mask = (want(rx, cx) ? 1u : 0u) | (want(rx, cy) ? 2u : 0u) |
+                  (want(ry, cx) ? 4u : 0u) | (want(ry, cy) ? 8u : 0u);
+  if (!mask) return;
+
+  const int pi = g.off[m] + i, pj = g.off[n] + j;
+  double cxx = 0, cxy = 0, cyx = 0, cyy = 0;
+  for (int l = 0; l < nL; ++l) {
+    const double sml = s_sm[l], snl = s_sn[l];
+    if (!(sml > 0 && snl > 0)) continue;
+    const double* ul = g.u + (size_t)l * g.Nx;
+    const double* vl = g.v + (size_t)l * g.Nx;
+    const double du = __ldg(ul + pi) - __ldg(ul + pj);
+    const double dv = __ldg(vl + pi) - __ldg(vl + pj);
+    const double s1 = sml * 0.5, s2 = snl * 0.5;
+    const double tpl = s_tpl[l];
+    const double w = s_w[l] * s_amp[l];
+    if (s1 == s2) {
+      // Equal subaperture sizes: ac = 0, ad = 2 s; XY and YX share 4 points.
+      const double ad = s1 + s2;
+      const double d0 = (mask & 9u) ? D(du, dv, tpl) : 0.0;
+      if (mask & 1u) {
+        const double xx = -d0 + D(du + ad, dv, tpl) + D(du - ad, dv, tpl) - d0;
+        cxx += xx * w;
+      }
+      if (mask & 8u) {
+        const double yy = -d0 + D(du, dv + ad, tpl) + D(du, dv - ad, tpl) - d0;
+        cyy += yy * w;
+      }
+      if (mask & 6u) {
+        const double pp = D(du + s1, dv + s2, tpl), pm = D(du + s1, dv - s2, tpl);
+        const double mp = D(du - s1, dv + s2, tpl), mm = D(du - s1, dv - s2, tpl);
+        cxy += (-pm + pp + mm - mp) * w;
+        cyx += (-mp + pp + mm - pm) * w;
+      }
+    } else {
+      const double ac = s1 - s2, ad = s1 + s2, bc = -ad, bd = -ac;
+      if (mask & 1u)
+        cxx += (-D(du + ac, dv, tpl) + D(du + ad, dv, tpl) + D(du + bc, dv, tpl) -
+                D(du + bd, dv, tpl)) * w;
+      if (mask & 8u)
+        cyy += (-D(du, dv + ac, tpl) + D(du, dv + ad, tpl) + D(du, dv + bc, tpl) -
+                D(du, dv + bd, tpl)) * w;
+      if (mask & 2u)
+        cxy += (-D(du + s1, dv - s2, tpl) + D(du + s1, dv + s2, tpl) +
+                D(du - s1, dv - s2, tpl) - D(du - s1, dv + s2, tpl)) * w;
+      if (mask & 4u)
+        cyx += (-D(du - s2, dv + s1, tpl) + D(du + s2, dv + s1, tpl) +
+                D(du - s2, dv - s1, tpl) - D(du + s2, dv - s1, tpl)) * w;
+    }
+  }
+
+  // WFS noise on same-WFS blocks (compute_element_tiled_4 :310-330).
+  if (m == n && d.type != 3) {
+    if (m < g.nLgs) {
+      if (i == j) {
+        const int p = g.off[m] + i;
+        cxx += g.noiseLGSxx[p];
+        cyy += g.noiseLGSyy[p];
+        cxy += g.noiseLGSxy[p];
+        cyx += g.noiseLGSxy[p];
+      }
+      cxx += g.lgsCst;
+      cyy += g.lgsCst;
+    } else if (i == j) {
+      cxx += g.noiseNGS[m - g.nLgs];
+      cyy += g.noiseNGS[m - g.nLgs];
+    }
+  }
+
+  const long long ld = d.ld;
+  auto store = [&](int r, int c, double val) {
+    out[(size_t)(c - d.c0) * ld + (r - d.r0)] = (OutT)val;
+    if (d.type == 5 && r != c) out[(size_t)(r - d.c0) * ld + (c - d.r0)] = (OutT)val;
+  };
+  if (mask & 1u) store(rx, cx, cxx);
+  if (mask & 2u) store(rx, cy, cxy);
+  if (mask & 4u) store(ry, cx, cyx);
+  if (mask & 8u) store(ry, cy, cyy);
+}
+
+// Ctt (type 4): truth-sensor auto-covariance from the unprojected positions,
+// compute_element_ts_tile (common/kernels/matcov_kernels.cpp:423-483). The
+// reference indexes the truth sensor at Nsubap_ts * (nW - 1), which assumes
+// every WFS has the same number of valid subapertures; kept as is.
+template <typename OutT>
+__global__ void __launch_bounds__(kTileI* kTileJ)
+    matcov_ts_kernel(const DevGeometry g, int r0, int c0, int nrows, int ncols,
+                     long long ld, OutT* __restrict__ out) {
+  __shared__ double s_tpl[kMaxLayers], s_w[kMaxLayers];
+  const int nL = g.nLayer;
+  const int ts = g.nW - 1;
+  const int Nt = g.Nsubap[ts];
+  const double ssp = g.diam / g.Nssp[ts];
+  const double kk = kLambda2 / (ssp * ssp);
+  for (int l = threadIdx.y * kTileI + threadIdx.x; l < nL; l += kTileI * kTileJ) {
+    s_tpl[l] = g.layer[l];
+    s_w[l] = 0.5 * kk * g.layer[2 * nL + l] * g.layer[nL + l];
+  }
+  __syncthreads();
+  // Pair grid covers the subaperture bounding range of the window.
+  const int i = blockIdx.x * kTileI + threadIdx.x;
+  const int j = blockIdx.y * kTileJ + threadIdx.y;
+  if (i >= Nt || j >= Nt) return;
+  const int r1 = r0 + nrows, c1 = c0 + ncols;
+  auto want = [&](int r, int c) { return r >= r0 && r < r1 && c >= c0 && c < c1; };
+  const unsigned mask = (want(i, j) ? 1u : 0u) | (want(i, Nt + j) ? 2u : 0u) |
+                        (want(Nt + i, j) ? 4u : 0u) | (want(Nt + i, Nt + j) ? 8u : 0u);
+  if (!mask) return;
+  const int base = Nt * (g.nW - 1);
+  const double du = g.X[base + i] - g.X[base + j];
+  const double dv = g.Y[base + i] - g.Y[base + j];
+  const double s = ssp * 0.5, ad = 2.0 * s;
+  double cxx = 0, cxy = 0, cyx = 0, cyy = 0;
+  for (int l = 0; l < nL; ++l) {
+    const double tpl = s_tpl[l], w = s_w[l];
+    const double d0 = (mask & 9u) ? D(du, dv, tpl) : 0.0;
+    if (mask & 1u) cxx += (-d0 + D(du + ad, dv, tpl) + D(du - ad, dv, tpl) - d0) * w;
+    if (mask & 8u) cyy += (-d0 + D(du, dv + ad, tpl) + D(du, dv - ad, tpl) - d0) * w;
+    if (mask & 6u) {
+      const double pp = D(du + s, dv + s, tpl), pm = D(du + s, dv - s, tpl);
+      const double mp = D(du - s, dv + s, tpl), mm = D(du - s, dv - s, tpl);
+      cxy += (-pm + pp + mm - mp) * w;
+      cyx += (-mp + pp + mm - pm) * w;
+    }
+  }
+  auto store = [&](int r, int c, double val) {
+    out[(size_t)(c - c0) * ld + (r - r0)] = (OutT)val;
+  };
+  if (mask & 1u) store(i, j, cxx);
+  if (mask & 2u) store(i, Nt + j, cxy);
+  if (mask & 4u) store(Nt + i, j, cyx);
+  if (mask & 8u) store(Nt + i, Nt + j, cyy);
+}
+
+// Bounding subaperture range [lo, hi) of a WFS whose x slopes start at global
+// index base and y slopes at base + N, intersected with the window [w0, w1).
+void subap_range(int base, int N, int w0, int w1, int* lo, int* hi) {
+  int a = std::max(w0 - base, 0), b = std::min(w1 - base, N);          // x part
+  int c = std::max(w0 - base - N, 0), e = std::min(w1 - base - N, N);  // y part
+  int l = N, h = 0;
+  if (a < b) { l = std::min(l, a); h = std::max(h, b); }
+  if (c < e) { l = std::min(l, c); h = std::max(h, e); }
+  *lo = l;
+  *hi = h;
+}
+
+template <typename OutT>
+moao_status launch_impl(const DevGeometry& g, OutT* data, int nrows, int ncols, int xoffset,
+                        int yoffset, int lda, int type_mat, cudaStream_t s,
+                        long long* launches) {
+  if (nrows < 0 || ncols < 0 || xoffset < 0 || yoffset < 0)
+    return set_error(MOAO_ERR_BAD_ARG, "matcov: negative size or offset");
+  if (nrows == 0 || ncols == 0) return MOAO_OK;
+  if (lda < nrows) return set_error(MOAO_ERR_BAD_ARG, "matcov: lda < nrows");
+  if (!data) return set_error(MOAO_ERR_BAD_ARG, "matcov: null data");
+  if (g.nLayer > kMaxLayers || g.nW > kMaxWfs)
+    return set_error(MOAO_ERR_UNSUPPORTED, "matcov: too many layers or WFS");
+  const int ts = g.nW - 1;
+  long nmeas = 0;
+  for (int w = 0; w < ts; ++w) nmeas += 2L * g.Nsubap[w];
+  const long nts = 2L * g.Nsubap[ts];
+
+  if (type_mat == 4) {
+    if (xoffset + (long)nrows > nts || yoffset + (long)ncols > nts)
+      return set_error(MOAO_ERR_BAD_ARG, "matcov: Ctt tile outside nmeasts x nmeasts");
+    const int Nt = g.Nsubap[ts];
+    if ((long)Nt * g.nW > g.Nx)  // the reference's uniform-Nsubap indexing would overrun X, Y
+      return set_error(MOAO_ERR_UNSUPPORTED, "matcov: Ctt needs equal subaperture counts per WFS");
+    dim3 grid((Nt + kTileI - 1) / kTileI, (Nt + kTileJ - 1) / kTileJ);
+    matcov_ts_kernel<OutT><<<grid, dim3(kTileI, kTileJ), 0, s>>>(g, xoffset, yoffset, nrows,
+                                                                 ncols, lda, data);
+    if (launches) ++*launches;
+    MOAO_CUDA_TRY(cudaGetLastError());
+    return MOAO_OK;
+  }
+  if (type_mat != 1 && type_mat != 2 && type_mat != 3 && type_mat != 5)
+    return set_error(MOAO_ERR_BAD_ARG, "matcov: unrecognized type_mat " + std::to_string(type_mat));
+  const long rows_total = (type_mat == 3) ? nts : nmeas;
+  const long cols_total = (type_mat == 2) ? nts : nmeas;
+  if (xoffset + (long)nrows > rows_total || yoffset + (long)ncols > cols_total)
+    return set_error(MOAO_ERR_BAD_ARG, "matcov: tile outside the matrix");
+  if (type_mat == 5 && (xoffset != yoffset || nrows != ncols))
+    return set_error(MOAO_ERR_BAD_ARG, "matcov: type 5 needs a square diagonal tile");
+
+  // Row / column WFS lists and their slope bases.
+  std::vector<int> rw, cw, rbase, cbase;
+  if (type_mat == 3) { rw.push_back(ts); rbase.push_back(0); }
+  else { int b = 0; for (int w = 0; w < ts; ++w) { rw.push_back(w); rbase.push_back(b); b += 2 * g.Nsubap[w]; } }
+  if (type_mat == 2) { cw.push_back(ts); cbase.push_back(0); }
+  else { int b = 0; for (int w = 0; w < ts; ++w) { cw.push_back(w); cbase.push_back(b); b += 2 * g.Nsubap[w]; } }
+
+  const bool lower = (type_mat == 1 || type_mat == 5);
+  std::vector<Job> jobs;
+  for (size_t a = 0; a < rw.size(); ++a) {
+    for (size_t b = 0; b < cw.size(); ++b) {
+      const int m = rw[a], n = cw[b];
+      if (lower && m < n) continue;  // entirely above the diagonal
+      Job jb{};
+      jb.m = m; jb.n = n; jb.rb = rbase[a]; jb.cb = cbase[b];
+      int ilo, ihi, jlo, jhi;
+      subap_range(jb.rb, g.Nsubap[m], xoffset, xoffset + nrows, &ilo, &ihi);
+      subap_range(jb.cb, g.Nsubap[n], yoffset, yoffset + ncols, &jlo, &jhi);
+      if (ilo >= ihi || jlo >= jhi) continue;
+      jb.i0 = ilo; jb.ni = ihi - ilo; jb.j0 = jlo; jb.nj = jhi - jlo;
+      jb.tiles_i = (jb.ni + kTileI - 1) / kTileI;
+      jobs.push_back(jb);
+    }
+  }
+  // Launch in chunks of kMaxJobs jobs.
+  for (size_t base = 0; base < jobs.size(); base += kMaxJobs) {
+    LaunchDesc d{};
+    d.type = type_mat;
+    d.r0 = xoffset; d.c0 = yoffset; d.nrows = nrows; d.ncols = ncols; d.ld = lda;
+    int tiles = 0;
+    for (size_t k = base; k < jobs.size() && k < base + kMaxJobs; ++k) {
+      Job jb = jobs[k];
+      jb.tile_base = tiles;
+      tiles += jb.tiles_i * ((jb.nj + kTileJ - 1) / kTileJ);
+      d.jobs[d.njobs++] = jb;
+    }
+    d.total_tiles = tiles;
+    if (tiles == 0) continue;
+    matcov_block_kernel<OutT><<<tiles, dim3(kTileI, kTileJ), 0, s>>>(d, g, data);
+    if (launches) ++*launches;
+    MOAO_CUDA_TRY(cudaGetLastError());
+  }
+  return MOAO_OK;
+}
+
+}  // namespace
+
+moao_status launch_matcov(const DevGeometry& g, double* data, int nrows, int ncols,
+                          int xoffset, int yoffset, int lda, int type_mat, cudaStream_t s,
+                          long long* launches) {
+  return launch_impl<double>(g, data, nrows, ncols, xoffset, yoffset, lda, type_mat, s,
+                             launches);
+}
+
+moao_status launch_matcov_f32(const DevGeometry& g, float* data, int nrows, int ncols,
+                              int xoffset, int yoffset, int lda, int type_mat, cudaStream_t s,
+                              long long* launches) {
+  return launch_impl<float>(g, data, nrows, ncols, xoffset, yoffset, lda, type_mat, s,
+                            launches);
+}
+
+}  // namespace moao

@@ -1,0 +1,71 @@
+// Internal declarations shared by the host library and the CUDA kernels.
+#ifndef MOAO_INTERNAL_H
+#define MOAO_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "moao_b200.h"
+
+namespace moao {
+
+// Records a message for moao_last_error() and returns the status.
+moao_status set_error(moao_status s, const std::string& msg);
+
+#define MOAO_CUDA_TRY(expr)                                                        \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess)                                                         \
+      return ::moao::set_error(MOAO_ERR_CUDA, std::string(#expr) + ": " +          \
+                                                  cudaGetErrorString(_e));         \
+  } while (0)
+
+#define MOAO_TRY(expr)                 \
+  do {                                 \
+    moao_status _s = (expr);           \
+    if (_s != MOAO_OK) return _s;      \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Geometry tables resident on the device (uploaded from a Tomo_struct).
+// ---------------------------------------------------------------------------
+constexpr int kMaxWfs = 16;
+constexpr int kMaxLayers = 128;
+
+struct DevGeometry {
+  int nW = 0, nLgs = 0, nLayer = 0, Nx = 0;
+  double diam = 0, lgsCst = 0;
+  int Nsubap[kMaxWfs];       // valid subapertures per WFS
+  int off[kMaxWfs];          // first subaperture of each WFS in the Nx tables
+  int Nssp[kMaxWfs];
+  // device arrays
+  double* u = nullptr;       // [nLayer*Nx]
+  double* v = nullptr;       // [nLayer*Nx]
+  double* X = nullptr;       // [Nx]
+  double* Y = nullptr;       // [Nx]
+  double* noiseLGSxx = nullptr;  // [Nx]
+  double* noiseLGSyy = nullptr;
+  double* noiseLGSxy = nullptr;
+  double* noiseNGS = nullptr;    // [nW - nLgs]
+  // per-layer tables: [0,nL) 2*pi/L0, [nL,2nL) k1*L0^(5/3), [2nL,3nL) cn2,
+  // then sspSizeL [nW*nL]
+  double* layer = nullptr;
+};
+
+// Matcov launch (device pointers). type_mat: 1 Cmm lower, 3 Ctm, 4 Ctt,
+// 5 Cmm full symmetric. The tile covers rows [xoffset, xoffset+nrows) and
+// columns [yoffset, yoffset+ncols) of the global matrix; data points at the
+// tile's first element.
+moao_status launch_matcov(const DevGeometry& g, double* data, int nrows, int ncols,
+                          int xoffset, int yoffset, int lda, int type_mat,
+                          cudaStream_t s, long long* launches);
+// FP32 output variant (mixed path); same geometry, FP64 evaluation.
+moao_status launch_matcov_f32(const DevGeometry& g, float* data, int nrows, int ncols,
+                              int xoffset, int yoffset, int lda, int type_mat,
+                              cudaStream_t s, long long* launches);
+
+}  // namespace moao
+
+#endif  // MOAO_INTERNAL_H
