@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Reconstructor builds per second on B200 (ELT-scale system).
+
+One step = one tomographic reconstructor build for the ELT-scale system
+(39 m, 64x64 subapertures, 6 LGS + 2 NGS + truth sensor, 35 layers;
+nmeas 47,552, nmeasts 5,944): covariance generation of Cmm and Ctm on the GPU,
+tiled Cholesky of Cmm and the two triangular solves giving R = Ctm Cmm^-1.
+
+    python bench.py [--gpus N --steps K --warmup W] [--path fp64|mixed]
+    python bench.py --impl reference ...     # the reference's CPU path
+
+Printed on rank 0: one JSON line. ``value`` is whole-job builds/s with the
+system tables resident in HBM; ``e2e`` is the same metric through the public
+API with the geometry uploaded from host memory and R read back to pinned host
+memory every step. Multi-GPU runs are independent replicas (one reconstructor
+per GPU, no collective on the data path). The CPU baseline / reference arm runs
+the reference's own covariance code (oracle/_ref, compiled from the reference
+sources) and LAPACK through scipy's OpenBLAS on a bounded sample of the same
+workload, extrapolated by element and flop counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "R builds/s (ELT-scale reconstructor: matcov Cmm+Ctm, Cholesky, 2 triangular solves)"
+UNIT = "builds/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="moao", choices=["moao", "reference"])
+    p.add_argument("--path", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--nb", type=int, default=256)
+    p.add_argument("--config", default="elt", choices=["elt", "small"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def system(config):
+    from moao_b200 import params as P
+    s, a = P.config_elt() if config == "elt" else P.config_small()
+    d = tempfile.mkdtemp(prefix="moao_bench_")
+    P.write_system(d, s, a)
+    return os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt"), s, a
+
+
+def workload_name(config, nm, nts, nl):
+    if config == "elt":
+        return (f"ELT-scale reconstructor build: 39 m, 64x64 subapertures, 6 LGS + 2 NGS + TS, "
+                f"{nl} layers (nmeas {nm}, nmeasts {nts})")
+    return f"8 m reconstructor build: 10x10, 3 LGS + 1 NGS + TS, {nl} layers (nmeas {nm}, nmeasts {nts})"
+
+
+# ----------------------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="moao_clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU
+def cpu_reference_sample(sf, af, nm, nts, budget_s=20.0):
+    """Times the reference's CPU path on a bounded sample; returns (builds/s, info)."""
+    import numpy as np
+    import scipy.linalg.blas as blas
+    import scipy.linalg.lapack as lapack
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    kind = "reference" if O.RefTomo.available() else "port"
+    # (1) covariance generation: rows of Ctm (type 3) with every core; per-element
+    # cost applies to Cmm too (same layer loop and stencils per element).
+    if kind == "reference":
+        t = O.RefTomo(sf, af)
+        t.setTarget(0)
+        run = lambda rows: t.matcov_full(rows, nm, 3, nthreads=cores, ts=max(1, rows // cores + 1))
+    else:
+        import moao_b200 as M
+        g = O.Geometry.from_tomo(M.Tomo(sf, af))
+        run = lambda rows: O.matcov(g, rows, nm, 0, 0, 3, nthreads=cores)
+    rows, el_time = 2, None
+    while True:
+        t0 = time.perf_counter()
+        run(rows)
+        dt = time.perf_counter() - t0
+        if dt > budget_s / 3 or rows >= nts:
+            el_time = dt / (rows * nm)
+            break
+        rows = min(nts, rows * 4 if dt < budget_s / 30 else rows * 2)
+    n_el = nm * (nm + 1) / 2 + nts * nm
+    t_matcov = el_time * n_el
+    # (2) LAPACK (scipy's OpenBLAS, all cores): dpotrf + two dtrsm at a reduced size
+    rng = np.random.default_rng(0)
+    n = 4096
+    while True:
+        A = rng.standard_normal((n, n))
+        C = np.asfortranarray(A @ A.T + n * np.eye(n))
+        T = np.asfortranarray(rng.standard_normal((max(n // 8, 1), n)))
+        t0 = time.perf_counter()
+        L, info = lapack.dpotrf(C, lower=1, clean=0, overwrite_a=1)
+        t1 = time.perf_counter()
+        X = blas.dtrsm(1.0, L, T, side=1, lower=1, trans_a=1)
+        blas.dtrsm(1.0, L, X, side=1, lower=1, trans_a=0)
+        t2 = time.perf_counter()
+        if t2 - t0 > budget_s / 6 or n >= 16384:
+            break
+        n *= 2
+    rate_potrf = (n ** 3 / 3) / (t1 - t0)
+    rate_trsm = (2 * T.shape[0] * n ** 2) / (t2 - t1)
+    t_lapack = (nm ** 3 / 3) / rate_potrf + (2 * nts * nm ** 2) / rate_trsm
+    total = t_matcov + t_lapack
+    info = {
+        "cores": cores, "kind": kind,
+        "sample": (f"covariance: {rows} Ctm rows x {nm} columns through the reference's matcov_tile "
+                   f"({'oracle/_ref' if kind == 'reference' else 'C port'}, {cores} threads), "
+                   f"{el_time * 1e6:.2f} us/element scaled to {n_el:.3e} elements; LAPACK: "
+                   f"dpotrf n={n} + 2 dtrsm ({T.shape[0]} rows) with scipy OpenBLAS, "
+                   f"{rate_potrf / 1e9:.1f} / {rate_trsm / 1e9:.1f} GFLOP/s scaled to nmeas {nm}; "
+                   f"extrapolated build {total:.0f} s"),
+        "seconds_per_build": total,
+    }
+    return 1.0 / total, info
+
+
+# ----------------------------------------------------------------------------- GPU
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM (torch.matmul float64, 8192^3), best of 5: the measured FP64
+    tensor-pipe ceiling the FP64 kernels are reported against."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e9
+
+
+def read_traffic_ratio(name):
+    """bytes of DRAM traffic per unit of work of a kernel, from its committed ncu
+    summary (line 'dram_bytes_per_work: X'), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_work:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    sf, af, sysp, atm = system(args.config)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        import moao_b200 as M
+        t = M.Tomo(sf, af)
+        nm, nts = t.getNMeas(), t.getNMeasTS()
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, info = cpu_reference_sample(sf, af, nm, nts, budget_s=8.0)
+            if i >= args.warmup:
+                vals.append(v)
+        value = statistics.median(vals)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded ELT-scale system)",
+            "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer),
+                       "path": "reference CPU (matcov_tile + LAPACK)", "parallelism": "host cores"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import numpy as np
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    import moao_b200 as M
+
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = M.Context(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_block(args.nb)
+    t = M.Tomo(sf, af)
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")   # column-major nm x nm
+    Ctm = torch.empty((nm, nts), dtype=torch.float64, device="cuda")  # column-major nts x nm
+
+    def step():
+        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        return M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=args.path, ctx=ctx)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ctx.reset_kernel_stats()
+    ctx.set_kernel_timing(True)
+    launches0 = ctx.launches
+    clocks = Clocks(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record()
+    reps = []
+    for k in range(args.steps):
+        reps.append(step())
+        ev[k + 1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ctx.set_kernel_timing(False)
+    launches = ctx.launches - launches0
+    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * args.steps / (total_ms / 1000.0)
+
+    stats = {f: ctx.kernel_stats(f) for f in ("gemm_f64", "matcov", "potrf_leaf")}
+    # R reference error on this rank's last build (mixed path only): vs an FP64 build
+    rel_err = None
+    if args.path == "mixed":
+        R_mixed = Ctm.clone()
+        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec="fp64", ctx=ctx)
+        torch.cuda.synchronize()
+        rel_err = float(torch.linalg.norm(R_mixed - Ctm) / torch.linalg.norm(Ctm))
+        del R_mixed
+
+    # ---- e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        R_host = torch.empty((nm, nts), dtype=torch.float64, pin_memory=True)
+        cn2 = np.array(atm.cn2, dtype=np.float64)
+        h, L0 = np.array(atm.h), np.array(atm.L0)
+        geom_bytes = 8 * (2 * atm.nLayer * (nm // 2 + nts // 2) + 5 * (nm // 2 + nts // 2) +
+                          sysp.nW * atm.nLayer + 3 * atm.nLayer + sysp.nW)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            t.set_profile(cn2, h, L0)   # host profile -> geometry recomputed and re-uploaded
+            step()
+            R_host.copy_(Ctm, non_blocking=True)
+            torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(geom_bytes), "d2h_bytes_per_step": int(nm * nts * 8)}
+
+    # ---- roofline of the dominant kernel (largest share of device time)
+    fam = max(stats, key=lambda f: stats[f]["ms"])
+    s = stats[fam]
+    roof = None
+    if fam == "gemm_f64" and s["ms"] > 0:
+        peak = fp64_peak_tflops(torch)
+        achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
+        ratio = read_traffic_ratio("gemm_f64_elt.txt")
+        roof = {"kernel": "gemm_f64_kernel (FP64 DMMA m16n8k16)", "bound": "tensor",
+                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4),
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": (ratio * s["work"] / s["launches"]) if ratio else None,
+                "launches": s["launches"], "share": round(s["ms"] / total_ms, 4)}
+    elif s["ms"] > 0:
+        roof = {"kernel": fam, "ms": s["ms"], "share": round(s["ms"] / total_ms, 4)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+        "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.path == "fp64" else "f64 (diagonal, refinement) + tensor-core trailing updates",
+        "data": "synthetic (seeded ELT-scale system; reference parameter-file format)",
+        "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "path": args.path,
+                   "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": args.nb,
+                   "l2": f"inputs larger than L2 (Cmm {nm * nm * 8 / 1e9:.1f} GB regenerated every step)",
+                   "parallelism": f"replicas x{world}"},
+        "stages_ms_per_step": {f: stats[f]["ms"] / args.steps for f in stats},
+        "rel_fro_err_R_vs_fp64": rel_err,
+        "roofline": roof,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, info = cpu_reference_sample(sf, af, nm, nts)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                                "sample": info["sample"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -81,14 +81,28 @@ typedef struct moao_ctx moao_ctx;
 
 moao_status moao_ctx_create(int device, moao_ctx** out);
 void moao_ctx_destroy(moao_ctx* ctx);
-/* Use an external cudaStream_t (NULL = the context's own stream). */
+/* Run on an external cudaStream_t (NULL = the legacy default stream). */
 moao_status moao_ctx_set_stream(moao_ctx* ctx, void* stream);
+/* Go back to the context's own (non-blocking) stream. */
+moao_status moao_ctx_use_own_stream(moao_ctx* ctx);
 void* moao_ctx_stream(moao_ctx* ctx);
 moao_status moao_ctx_synchronize(moao_ctx* ctx);
 /* Number of kernels this library launched on the context since creation. */
 long long moao_ctx_launch_count(const moao_ctx* ctx);
 /* Panel width of the blocked factorisation (default 256; multiple of 64). */
 moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
+
+/* Per-kernel-family device timing. When enabled, every launch of the library's
+ * kernels is bracketed by CUDA events on the context stream and accumulated per
+ * family together with its algorithmic work (flops for contractions, elements
+ * for covariance generation). Families: "gemm_f64", "potrf_leaf", "matcov",
+ * "intersample", "elementwise". */
+moao_status moao_ctx_set_kernel_timing(moao_ctx* ctx, int enable);
+/* Synchronises, then reports launches, total device ms and total work of one
+ * family since the last reset. */
+moao_status moao_ctx_kernel_stats(moao_ctx* ctx, const char* family, long long* launches,
+                                  double* ms, double* work);
+moao_status moao_ctx_reset_kernel_stats(moao_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
 /* Covariance generation.                                                    */

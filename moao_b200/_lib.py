@@ -54,16 +54,21 @@ SIGNATURES = {
     "moao_ctx_create": (i32, [i32, C.POINTER(vp)]),
     "moao_ctx_destroy": (None, [vp]),
     "moao_ctx_set_stream": (i32, [vp, vp]),
+    "moao_ctx_use_own_stream": (i32, [vp]),
     "moao_ctx_stream": (vp, [vp]),
     "moao_ctx_synchronize": (i32, [vp]),
     "moao_ctx_launch_count": (C.c_longlong, [vp]),
     "moao_ctx_set_block": (i32, [vp, i32]),
+    "moao_ctx_set_kernel_timing": (i32, [vp, i32]),
+    "moao_ctx_kernel_stats": (i32, [vp, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]),
+    "moao_ctx_reset_kernel_stats": (i32, [vp]),
     "moao_matcov_tile": (i32, [vp, vp, dp, i32, i32, i32, i32, i32, i32]),
     "moao_matcov_tile_host": (i32, [vp, vp, dp, i32, i32, i32, i32, i32, i32]),
     "moao_reconstructor": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, i32, C.POINTER(SolveReport)]),
     "moao_reconstructor_host": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, C.POINTER(SolveReport)]),
-    "moao_cee_cvv": (i32, [vp, i64, i64, i64] + [dp, i64] * 9),
-    "moao_cee_cvv_host": (i32, [vp, i64, i64, i64] + [dp, i64] * 9),
+    "moao_cee_cvv": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
+    "moao_cee_cvv_host": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
     "moao_intersample_create": (i32, [vp, i64, i64, C.c_double, dp, dp, dp, C.POINTER(vp)]),
     "moao_intersample_get_info": (i32, [vp, C.POINTER(IsampleInfo)]),
     "moao_intersample_process": (i32, [vp, dp, dp]),

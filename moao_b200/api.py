@@ -87,10 +87,13 @@ class Context:
         return self._h
 
     def set_stream(self, stream: Optional[int]):
-        """Use an external cudaStream_t (an int handle, e.g. torch's
-        ``torch.cuda.current_stream().cuda_stream``); None = own stream."""
-        check(lib().moao_ctx_set_stream(self._h, C.c_void_p(stream) if stream else None),
-              "moao_ctx_set_stream")
+        """Run on an external cudaStream_t given as an int handle, e.g. torch's
+        ``torch.cuda.current_stream().cuda_stream`` (0 is the legacy default
+        stream); None returns to the context's own stream."""
+        if stream is None:
+            check(lib().moao_ctx_use_own_stream(self._h), "moao_ctx_use_own_stream")
+        else:
+            check(lib().moao_ctx_set_stream(self._h, C.c_void_p(stream)), "moao_ctx_set_stream")
 
     @property
     def stream(self) -> int:
@@ -105,6 +108,18 @@ class Context:
 
     def set_block(self, nb: int):
         check(lib().moao_ctx_set_block(self._h, nb), "moao_ctx_set_block")
+
+    def set_kernel_timing(self, enable: bool):
+        check(lib().moao_ctx_set_kernel_timing(self._h, int(enable)), "moao_ctx_set_kernel_timing")
+
+    def kernel_stats(self, family: str) -> dict:
+        n, ms, work = C.c_longlong(), C.c_double(), C.c_double()
+        check(lib().moao_ctx_kernel_stats(self._h, family.encode(), C.byref(n), C.byref(ms),
+                                          C.byref(work)), "moao_ctx_kernel_stats")
+        return {"launches": n.value, "ms": ms.value, "work": work.value}
+
+    def reset_kernel_stats(self):
+        check(lib().moao_ctx_reset_kernel_stats(self._h), "moao_ctx_reset_kernel_stats")
 
     def close(self):
         if self._h:

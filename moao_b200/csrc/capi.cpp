@@ -105,6 +105,49 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometr
   return MOAO_OK;
 }
 
+namespace {
+cudaEvent_t take_event(moao_ctx* ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+KernelTimer::KernelTimer(moao_ctx* ctx, const char* family, double work)
+    : ctx_(ctx), family_(family), work_(work) {
+  if (!ctx_->timing) return;
+  a_ = take_event(ctx_);
+  cudaEventRecord(a_, ctx_->stream);
+}
+
+KernelTimer::~KernelTimer() {
+  if (!a_) return;
+  cudaEvent_t b = take_event(ctx_);
+  cudaEventRecord(b, ctx_->stream);
+  ctx_->pending.push_back({family_, a_, b, work_});
+}
+
+moao_status collect_kernel_stats(moao_ctx* ctx) {
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (auto& p : ctx->pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    FamilyStats& f = ctx->stats[p.family];
+    f.launches += 1;
+    f.ms += ms;
+    f.work += p.work;
+    ctx->event_pool.push_back(p.a);
+    ctx->event_pool.push_back(p.b);
+  }
+  ctx->pending.clear();
+  return MOAO_OK;
+}
+
 }  // namespace moao
 
 using namespace moao;
@@ -258,13 +301,24 @@ void moao_ctx_destroy(moao_ctx* c) {
   c->ws_tmp.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& p : c->pending) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (auto e : c->event_pool) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
 
 moao_status moao_ctx_set_stream(moao_ctx* c, void* stream) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_stream: null");
-  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  c->stream = static_cast<cudaStream_t>(stream);
+  return MOAO_OK;
+}
+
+moao_status moao_ctx_use_own_stream(moao_ctx* c) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_use_own_stream: null");
+  c->stream = c->own_stream;
   return MOAO_OK;
 }
 
@@ -277,6 +331,37 @@ moao_status moao_ctx_synchronize(moao_ctx* c) {
 }
 
 long long moao_ctx_launch_count(const moao_ctx* c) { return c ? c->launches : 0; }
+
+moao_status moao_ctx_set_kernel_timing(moao_ctx* c, int enable) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_kernel_timing: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->timing = enable != 0;
+  return MOAO_OK;
+}
+
+moao_status moao_ctx_kernel_stats(moao_ctx* c, const char* family, long long* launches,
+                                  double* ms, double* work) {
+  if (!c || !family) return set_error(MOAO_ERR_BAD_ARG, "ctx_kernel_stats: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(c->device));
+  MOAO_TRY(collect_kernel_stats(c));
+  FamilyStats f;
+  auto it = c->stats.find(family);
+  if (it != c->stats.end()) f = it->second;
+  if (launches) *launches = f.launches;
+  if (ms) *ms = f.ms;
+  if (work) *work = f.work;
+  return MOAO_OK;
+}
+
+moao_status moao_ctx_reset_kernel_stats(moao_ctx* c) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_reset_kernel_stats: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(c->device));
+  MOAO_TRY(collect_kernel_stats(c));
+  c->stats.clear();
+  return MOAO_OK;
+}
 
 moao_status moao_ctx_set_block(moao_ctx* c, int nb) {
   if (!c || nb < 64 || nb % 64 != 0 || nb > 2048)
@@ -293,6 +378,9 @@ moao_status moao_matcov_tile(moao_ctx* ctx, const moao_tomo* t, double* d_data, 
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   const DevGeometry* g = nullptr;
   MOAO_TRY(device_geometry(ctx, t, &g));
+  double elems = (double)nrows * ncols;
+  if (type_mat == 1 && xoffset == yoffset && nrows == ncols) elems = 0.5 * nrows * (nrows + 1.0);
+  KernelTimer kt(ctx, "matcov", elems);
   return launch_matcov(*g, d_data, nrows, ncols, xoffset, yoffset, lda, type_mat, ctx->stream,
                        &ctx->launches);
 }

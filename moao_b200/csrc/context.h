@@ -6,6 +6,8 @@
 
 #include <map>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "moao_b200_tomo.hpp"
 #include "moao_internal.h"
@@ -26,6 +28,12 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
+// Device-time accounting per kernel family (see moao_ctx_set_kernel_timing).
+struct FamilyStats {
+  long long launches = 0;
+  double ms = 0, work = 0;
+};
+
 struct GeomEntry {
   unsigned long long version = ~0ull;
   DevGeometry g;
@@ -44,9 +52,34 @@ struct moao_ctx {
   std::map<const moao_tomo*, moao::GeomEntry> geom;
   moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
   cudaEvent_t ev[8] = {};
+  // kernel timing
+  bool timing = false;
+  std::map<std::string, moao::FamilyStats> stats;
+  struct Pending {
+    std::string family;
+    cudaEvent_t a, b;
+    double work;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
 };
 
 namespace moao {
+
+// Brackets the launches issued during its lifetime with events when the
+// context's kernel timing is on.
+class KernelTimer {
+ public:
+  KernelTimer(moao_ctx* ctx, const char* family, double work);
+  ~KernelTimer();
+ private:
+  moao_ctx* ctx_;
+  const char* family_;
+  double work_;
+  cudaEvent_t a_ = nullptr;
+};
+// Folds completed event pairs into the per-family totals (synchronises).
+moao_status collect_kernel_stats(moao_ctx* ctx);
 
 // Uploads (or reuses) the device copy of a tomo's geometry tables.
 moao_status device_geometry(moao_ctx* ctx, const moao_tomo* t, const DevGeometry** out);

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "dense.h"
 
@@ -52,6 +53,19 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
+}
+
+// m16n8k16 FP64 MMA: A 16x16 (8 per thread: rows gid, gid+8; cols tig + 4r),
+// B 16x8 (4 per thread: rows tig + 4r, col gid), C 16x8 (rows gid, gid+8;
+// cols 2 tig, 2 tig + 1).
+__device__ __forceinline__ void dmma16(double& c0, double& c1, double& c2, double& c3,
+                                       const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 struct KParams {
@@ -100,7 +114,7 @@ __device__ __forceinline__ void load_k_tile(double* s, const double* g, long ld,
   }
 }
 
-template <bool TRANSB, bool LOWERC, int VEC>
+template <bool TRANSB, bool LOWERC, int VEC, bool MMA16>
 __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) {
   extern __shared__ __align__(16) double smem[];
   double* As = smem;
@@ -122,6 +136,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
   const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
   const int gid = lane >> 2, tig = lane & 3;
 
+  // acc[i][j][h]: k4 layout = 8 m-frags of 8 rows x 4 n-frags x 2;
+  // k16 layout = 4 m-frags of 16 rows x 4 n-frags x 4 (viewed through acc16).
   double acc[8][4][2];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
@@ -172,20 +188,42 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
       if (nt < ntiles) issue(nt % STAGES, nt);
       cp_commit();
     }
+    if (MMA16) {
+      double bf[4][4];
 #pragma unroll
-    for (int k4 = 0; k4 < BK; k4 += 4) {
-      double a[8], b[4];
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = as[(k4 + tig) * LDA_S + wm + i * 8 + gid];
+        for (int r = 0; r < 4; ++r) {
+          const int k = r * 4 + tig, n = wn + j * 8 + gid;
+          bf[j][r] = TRANSB ? bs[k * LDB_S + n] : bs[n * LDBT_S + k];
+        }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (TRANSB) b[j] = bs[(k4 + tig) * LDB_S + wn + j * 8 + gid];
-        else b[j] = bs[(wn + j * 8 + gid) * LDBT_S + k4 + tig];
+      for (int i = 0; i < 4; ++i) {
+        double af[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          af[r] = as[((r >> 1) * 4 + tig) * LDA_S + wm + i * 16 + gid + 8 * (r & 1)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1],
+                 af, bf[j]);
       }
+    } else {
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int k4 = 0; k4 < BK; k4 += 4) {
+        double a[8], b[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for (int i = 0; i < 8; ++i) a[i] = as[(k4 + tig) * LDA_S + wm + i * 8 + gid];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (TRANSB) b[j] = bs[(k4 + tig) * LDB_S + wn + j * 8 + gid];
+          else b[j] = bs[(wn + j * 8 + gid) * LDBT_S + k4 + tig];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
     }
   }
   cp_wait<0>();
@@ -193,7 +231,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
   // Epilogue: C = alpha * acc + beta * C (C is not read when beta == 0).
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const long r = m0 + wm + i * 8 + gid;
+    // k4: fragment i covers rows wm + 8 i; k16: acc[2q][j] and acc[2q+1][j] hold
+    // the 4 values of m16 fragment q (rows wm + 16 q + gid and + 8).
+    const long r = MMA16 ? m0 + wm + (i >> 1) * 16 + (i & 1) * 8 + gid : m0 + wm + i * 8 + gid;
     if (r >= p.M) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -211,10 +251,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
   }
 }
 
-template <bool TRANSB, bool LOWERC, int VEC>
-moao_status launch_gemm(const KParams& p, cudaStream_t s) {
+// FP64 MMA shape: m16n8k16 unless MOAO_GEMM_MMA=k4 selects m8n8k4.
+bool use_mma16() {
+  static const bool v = [] {
+    const char* e = getenv("MOAO_GEMM_MMA");
+    return !(e && e[0] == 'k' && e[1] == '4');
+  }();
+  return v;
+}
+
+template <bool TRANSB, bool LOWERC, int VEC, bool MMA16>
+moao_status launch_gemm_t(const KParams& p, cudaStream_t s) {
   static bool configured = false;
-  auto kern = gemm_f64_kernel<TRANSB, LOWERC, VEC>;
+  auto kern = gemm_f64_kernel<TRANSB, LOWERC, VEC, MMA16>;
   if (!configured) {
     MOAO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)SMEM_BYTES));
@@ -224,6 +273,12 @@ moao_status launch_gemm(const KParams& p, cudaStream_t s) {
   kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(p);
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
+}
+
+template <bool TRANSB, bool LOWERC, int VEC>
+moao_status launch_gemm(const KParams& p, cudaStream_t s) {
+  return use_mma16() ? launch_gemm_t<TRANSB, LOWERC, VEC, true>(p, s)
+                     : launch_gemm_t<TRANSB, LOWERC, VEC, false>(p, s);
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }

@@ -27,6 +27,11 @@ moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const doub
   g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
   g.A = A; g.lda = lda; g.B = B; g.ldb = ldb; g.transB = transB; g.triB = tri;
   g.C = C; g.ldc = ldc; g.lowerC = lowerC;
+  // algorithmic flops: 2MNK, halved when only a triangle of C or of B counts
+  double fl = 2.0 * M * N * K;
+  if (lowerC) fl = (double)M * N * K + (double)std::min(M, N) * K;
+  if (tri != TRI_FULL) fl *= 0.5;
+  KernelTimer kt(ctx, "gemm_f64", fl);
   return gemm_f64(g, ctx->stream, &ctx->launches);
 }
 
@@ -34,8 +39,10 @@ moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const doub
 // W is scratch of at least nb*nb/4 doubles... (nb/2 x nb/2 + margin).
 moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long ldd, long nb,
                             long col0, int* d_info, double* W) {
-  if (nb <= kLeaf)
+  if (nb <= kLeaf) {
+    KernelTimer kt(ctx, "potrf_leaf", (double)nb * nb * nb * (1.0 / 3 + 1.0 / 3));
     return potrf_inv_leaf(A, lda, D, ldd, (int)nb, col0, d_info, ctx->stream, &ctx->launches);
+  }
   const long n1 = kLeaf * ((nb + 2 * kLeaf - 1) / (2 * kLeaf));
   const long n2 = nb - n1;
   double* A11 = A;

@@ -17,10 +17,15 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <atomic>
 
 namespace {
 
 const double kRasc = 206265.0;  // arcsec per radian, as used by the reference
+
+// Process-wide geometry version: every change of any model gets a fresh value,
+// so device caches can never confuse two models.
+std::atomic<unsigned long long> g_version{0};
 
 // ---- positional text format ------------------------------------------------
 struct LineReader {
@@ -450,7 +455,7 @@ void Tomo_struct<T>::projectedSubap() {
       }
     }
   }
-  ++version;
+  version = ++g_version;
 }
 
 template <typename T>

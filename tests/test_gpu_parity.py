@@ -273,6 +273,7 @@ def test_full_pipeline_elt16_properties(ctx):
     M.matcov_tile(C, nm, nm, 0, 0, nm, t, 5, ctx=ctx)
     t.setTarget(0)
     M.matcov_tile(T, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+    ctx.synchronize()  # the library runs on the context stream, torch on its own
     Cfull = C.clone()
     Tctm = T.clone()
     M.reconstructor(nm, nts, C, nm, T, nts, 1, ctx=ctx)
