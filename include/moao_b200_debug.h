@@ -1,0 +1,31 @@
+/*
+ * moao_b200 — building blocks exposed for tests and tuning. These have no
+ * counterpart in the reference; they let the test suite check the tensor-core
+ * kernels in isolation.
+ */
+#ifndef MOAO_B200_DEBUG_H
+#define MOAO_B200_DEBUG_H
+
+#include "moao_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Tensor-core GEMM on the context stream (device pointers):
+ *   kind 0 (bf16): C[f32, M x N, col-major, ldc] = alpha * sum_p A_{pa[p]} B_{pb[p]}^T + beta * C
+ *   kind 1 (int8): C[f64] += 2^(erow[r] + ecol[c] + shift) * sum_p A_{pa[p]} B_{pb[p]}^T
+ * A holds na slices of M x K row-major (lda elements per row), slice i at
+ * A + i * M * lda; B holds nb slices of N x K row-major likewise. lower = 1
+ * writes only C(r, c) with r >= c. Synchronises and returns MOAO_ERR_TIMEOUT
+ * if a bounded device wait expired. */
+moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long N, long K, const void* A,
+                               long lda, int na, const void* B, long ldb, int nb, int npairs,
+                               const int* pa, const int* pb, void* C, long ldc, float alpha,
+                               float beta, const int* erow, const int* ecol, int shift, int lower);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOAO_B200_DEBUG_H */

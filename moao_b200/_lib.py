@@ -74,6 +74,8 @@ SIGNATURES = {
     "moao_intersample_process": (i32, [vp, dp, dp]),
     "moao_intersample_process_host": (i32, [vp, dp, dp]),
     "moao_intersample_destroy": (None, [vp]),
+    "moao_debug_tc_gemm": (i32, [vp, i32, i64, i64, i64, dp, i64, i32, dp, i64, i32, i32, dp, dp, dp,
+                                 i64, C.c_float, C.c_float, dp, dp, i32, i32]),
 }
 
 

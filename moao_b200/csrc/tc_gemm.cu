@@ -1,0 +1,444 @@
+// tcgen05 tensor-core GEMM for the mixed-precision path (sm_100a).
+//
+//   C[M x N] (+)= sum over segments s of  A_s[M x K_s] * B_s[N x K_s]^T
+//
+// Both operands are K-major (rows of K contiguous elements) and are fetched by
+// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a 3-stage
+// shared-memory ring; one thread issues tcgen05.mma (M = 128, N = 128) into a
+// TMEM accumulator; four epilogue warps drain TMEM with tcgen05.ld and update
+// C in global memory with coalesced column stores. The K dimension is a list of
+// segments, each naming its own A and B tensor (slices) and K offset, so that a
+// split-precision product (hi*hi + hi*lo + lo*hi, or the int8 slice pairs of one
+// Ozaki diagonal) accumulates in one accumulator and C is read and written once.
+//
+// Kinds:
+//   BF16 -> FP32 accumulate (kind::f16);   epilogue C32 = alpha*acc + beta*C32
+//   INT8 -> INT32 accumulate (kind::i8), exact for K*64*64*pairs < 2^31;
+//           epilogue C64 += acc * 2^(erow[r] + ecol[c] + shift)
+// Waits on mbarriers are bounded; on expiry the kernel records an error code in
+// *err and stops issuing work instead of spinning forever.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "tc_gemm.h"
+#include "context.h"
+#include "moao_b200_debug.h"
+
+namespace moao {
+namespace {
+
+constexpr int TBM = 128, TBN = 128;
+constexpr int KBYTES = 128;             // bytes of K per stage row (one 128B swizzle atom)
+constexpr int STAGES = 3;
+constexpr int A_TILE = TBM * KBYTES;    // 16 KB
+constexpr int B_TILE = TBN * KBYTES;    // 16 KB
+constexpr int STAGE_BYTES = A_TILE + B_TILE;
+constexpr int THREADS = 256;
+constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr unsigned long long kSpinLimit = 1ull << 28;
+
+struct __align__(64) TcParams {
+  CUtensorMap mapA[kTcMaxMaps];
+  CUtensorMap mapB[kTcMaxMaps];
+  TcSegment seg[kTcMaxSegs];
+  int nseg;
+  int M, N;
+  int a_row0, b_row0;      // row coordinate of C(0,0) in the A / B tensors
+  int lower;               // 1: only C(r, c) with r + diag_off >= c
+  int diag_off;
+  int kind;                // TcKind
+  int epi;                 // TcEpilogue
+  float alpha, beta;
+  void* C;
+  long long ldc;
+  const int* erow;         // INT8: per-row exponent of A (length M, indexed by r)
+  const int* ecol;         // INT8: per-column exponent of B (length N)
+  int shift;
+  int tiles_m;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; returns false (and records code) if the phase never completes.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  for (unsigned long long i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*(volatile int*)err) return false;  // another role already gave up
+  }
+  atomicCAS(err, 0, code);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor for a K-major tile written by TMA with the
+// 128-byte swizzle: 8-row core groups 1024 bytes apart (SBO), LBO unused,
+// descriptor version 1 (tcgen05), layout SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);          // start address
+  d |= (uint64_t)(16 >> 4) << 16;                    // LBO (ignored for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                  // SBO
+  d |= (uint64_t)1 << 46;                            // version
+  d |= (uint64_t)2 << 61;                            // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// Instruction descriptors (M = 128, N = 128, both operands K-major).
+//   bits 4-5 D format (1 F32, 2 S32), 7-9 A format, 10-12 B format
+//   (kind::f16: 1 BF16; kind::i8: 1 S8), 15/16 A/B major (0 = K),
+//   17-22 N >> 3, 24-28 M >> 4.
+constexpr uint32_t idesc_of(int dfmt, int abfmt) {
+  return (uint32_t)(dfmt << 4) | (uint32_t)(abfmt << 7) | (uint32_t)(abfmt << 10) |
+         (uint32_t)((TBN >> 3) << 17) | (uint32_t)((TBM >> 4) << 24);
+}
+constexpr uint32_t kIdescBf16 = idesc_of(1, 1);
+constexpr uint32_t kIdescI8 = idesc_of(2, 1);
+
+__global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty_bar = full_bar + STAGES;
+  uint64_t* acc_bar = empty_bar + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mt = blockIdx.x % p.tiles_m, nt = blockIdx.x / p.tiles_m;
+  const int m0 = mt * TBM, n0 = nt * TBN;
+  if (p.lower && m0 + TBM - 1 + p.diag_off < n0) return;  // tile entirely above the diagonal
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  // total K blocks over all segments
+  int total = 0;
+  for (int s = 0; s < p.nseg; ++s) total += p.seg[s].nk;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    int it = 0;
+    for (int s = 0; s < p.nseg && !*(volatile int*)p.err; ++s) {
+      const TcSegment sg = p.seg[s];
+      for (int kb = 0; kb < sg.nk; ++kb, ++it) {
+        const int st = it % STAGES;
+        const uint32_t round = it / STAGES;
+        if (it >= STAGES && !mbar_wait(&empty_bar[st], (round & 1) ^ 1, p.err, 1)) break;
+        uint8_t* sa = smem + st * STAGE_BYTES;
+        uint8_t* sb = sa + A_TILE;
+        mbar_expect_tx(&full_bar[st], STAGE_BYTES);
+        const int kx = sg.k0 + kb * sg.kstep;  // element coordinate along K
+        tma_load_2d(sa, &p.mapA[sg.a], kx, p.a_row0 + m0, &full_bar[st]);
+        tma_load_2d(sb, &p.mapB[sg.b], kx, p.b_row0 + n0, &full_bar[st]);
+      }
+    }
+    // Never leave the CTA with a bulk copy still writing its shared memory:
+    // wait (bounded) for the last copies issued on every stage.
+    for (int j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
+      const int st = j % STAGES;
+      for (unsigned long long i = 0; i < kSpinLimit && !mbar_try_wait(&full_bar[st], (j / STAGES) & 1); ++i) {
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    const uint32_t idesc = (p.kind == kTcBf16) ? kIdescBf16 : kIdescI8;
+    for (int it = 0; it < total; ++it) {
+      const int st = it % STAGES;
+      const uint32_t round = it / STAGES;
+      if (!mbar_wait(&full_bar[st], round & 1, p.err, 2)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t sa = smem_u32(smem + st * STAGE_BYTES);
+      const uint32_t sb = sa + A_TILE;
+      const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
+      // 4 instructions of 32 bytes of K each (K = 16 bf16 or 32 int8)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint64_t off = (uint64_t)((k * 32) >> 4);
+        if (p.kind == kTcBf16) mma_bf16(tmem, da + off, db + off, idesc, (it | k) ? 1u : 0u);
+        else mma_i8(tmem, da + off, db + off, idesc, (it | k) ? 1u : 0u);
+      }
+      mma_commit(&empty_bar[st]);
+    }
+    mma_commit(acc_bar);
+  } else if (warp >= 4) {
+    // ---------------- epilogue: warp q = warp - 4 owns TMEM lanes 32q..32q+31
+    const int q = warp - 4;
+    const int r = m0 + q * 32 + lane;  // row of C this thread updates
+    const bool ok = mbar_wait(acc_bar, 0, p.err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (ok && total > 0 && !*(volatile int*)p.err) {
+      for (int c0 = 0; c0 < TBN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+            "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+              "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+              "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (r < p.M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int c = n0 + c0 + j;
+            if (c >= p.N) break;
+            if (p.lower && r + p.diag_off < c) continue;
+            if (p.epi == kTcEpiF32) {
+              float* dst = static_cast<float*>(p.C) + (size_t)c * p.ldc + r;
+              float val = p.alpha * __uint_as_float(v[j]);
+              if (p.beta != 0.f) val += p.beta * *dst;
+              *dst = val;
+            } else {
+              double* dst = static_cast<double*>(p.C) + (size_t)c * p.ldc + r;
+              const double a = (double)(int)v[j];
+              *dst += ldexp(a, p.erow[r] + p.ecol[c] + p.shift);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  if (warp == 2) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TBN));
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+}  // namespace
+
+moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows, long long kcols,
+                        long long row_stride_elems, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return set_error(MOAO_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const int esz = (kind == kTcBf16) ? 2 : 1;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((row_stride_elems * esz) & 15))
+    return set_error(MOAO_ERR_BAD_ARG, "tc map: base or row stride not 16-byte aligned");
+  if (rows <= 0 || kcols <= 0 || box_rows <= 0 || box_rows > 256)
+    return set_error(MOAO_ERR_BAD_ARG, "tc map: bad extents");
+  cuuint64_t dims[2] = {(cuuint64_t)kcols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(row_stride_elems * esz)};
+  cuuint32_t box[2] = {(cuuint32_t)(KBYTES / esz), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(&t->map, esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                  2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(MOAO_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  t->kind = kind;
+  t->kstep = KBYTES / esz;
+  return MOAO_OK;
+}
+
+moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
+  if (g.M <= 0 || g.N <= 0) return MOAO_OK;
+  if (g.nA < 1 || g.nA > kTcMaxMaps || g.nB < 1 || g.nB > kTcMaxMaps || g.nseg < 1 ||
+      g.nseg > kTcMaxSegs || !g.err)
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: bad operand lists");
+  if (g.epi == kTcEpiF64Scaled && (g.kind != kTcI8 || !g.erow || !g.ecol))
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: scaled epilogue needs int8 and exponents");
+  if (g.epi == kTcEpiF32 && g.kind != kTcBf16)
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: fp32 epilogue needs bf16 operands");
+  TcParams p;
+  std::memset(&p, 0, sizeof(p));
+  for (int i = 0; i < g.nA; ++i) {
+    if (g.A[i]->kind != g.kind) return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: A kind mismatch");
+    p.mapA[i] = g.A[i]->map;
+  }
+  for (int i = 0; i < g.nB; ++i) {
+    if (g.B[i]->kind != g.kind) return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: B kind mismatch");
+    p.mapB[i] = g.B[i]->map;
+  }
+  const int kstep = g.A[0]->kstep;
+  for (int i = 0; i < g.nseg; ++i) {
+    TcSegment sg = g.seg[i];
+    if (sg.a < 0 || sg.a >= g.nA || sg.b < 0 || sg.b >= g.nB || sg.nk < 0 || sg.k0 < 0 ||
+        sg.k0 % kstep)
+      return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: bad segment");
+    sg.kstep = kstep;
+    p.seg[i] = sg;
+  }
+  p.nseg = g.nseg;
+  p.M = (int)g.M;
+  p.N = (int)g.N;
+  p.a_row0 = g.a_row0;
+  p.b_row0 = g.b_row0;
+  p.lower = g.lower;
+  p.diag_off = g.diag_off;
+  p.kind = g.kind;
+  p.epi = g.epi;
+  p.alpha = g.alpha;
+  p.beta = g.beta;
+  p.C = g.C;
+  p.ldc = g.ldc;
+  p.erow = g.erow;
+  p.ecol = g.ecol;
+  p.shift = g.shift;
+  p.err = g.err;
+  p.tiles_m = (int)((g.M + TBM - 1) / TBM);
+  const long tiles_n = (g.N + TBN - 1) / TBN;
+  static bool configured = false;
+  if (!configured) {
+    MOAO_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SMEM));
+    configured = true;
+  }
+  tc_gemm_kernel<<<(unsigned)(p.tiles_m * tiles_n), THREADS, SMEM, s>>>(p);
+  if (launches) ++*launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+}  // namespace moao
+
+extern "C" moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long N, long K,
+                                          const void* A, long lda, int na, const void* B, long ldb,
+                                          int nb, int npairs, const int* pa, const int* pb, void* C,
+                                          long ldc, float alpha, float beta, const int* erow,
+                                          const int* ecol, int shift, int lower) {
+  using namespace moao;
+  if (!ctx || !A || !B || !C || !pa || !pb || kind < 0 || kind > 1 || na < 1 ||
+      na > kTcMaxMaps || nb < 1 || nb > kTcMaxMaps || npairs < 1 || npairs > kTcMaxSegs ||
+      ldc < M || lda < K || ldb < K)
+    return set_error(MOAO_ERR_BAD_ARG, "debug_tc_gemm: bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  const int esz = kind == 0 ? 2 : 1;
+  TcTensor ta[kTcMaxMaps], tb[kTcMaxMaps];
+  TcGemm g;
+  g.kind = kind;
+  g.epi = kind == 0 ? kTcEpiF32 : kTcEpiF64Scaled;
+  g.M = M;
+  g.N = N;
+  for (int i = 0; i < na; ++i) {
+    MOAO_TRY(make_tc_map(&ta[i], (const char*)A + (size_t)i * M * lda * esz, kind, M, K, lda));
+    g.A[i] = &ta[i];
+  }
+  for (int i = 0; i < nb; ++i) {
+    MOAO_TRY(make_tc_map(&tb[i], (const char*)B + (size_t)i * N * ldb * esz, kind, N, K, ldb));
+    g.B[i] = &tb[i];
+  }
+  g.nA = na;
+  g.nB = nb;
+  const int kstep = ta[0].kstep;
+  for (int p = 0; p < npairs; ++p) {
+    g.seg[p].a = pa[p];
+    g.seg[p].b = pb[p];
+    g.seg[p].k0 = 0;
+    g.seg[p].nk = (int)((K + kstep - 1) / kstep);
+  }
+  g.nseg = npairs;
+  g.lower = lower;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.C = C;
+  g.ldc = ldc;
+  g.erow = erow;
+  g.ecol = ecol;
+  g.shift = shift;
+  MOAO_TRY(ctx->ws_info.ensure(2 * sizeof(int)));
+  int* err = ctx->ws_info.as<int>() + 1;
+  MOAO_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+  g.err = err;
+  MOAO_TRY(tc_gemm(g, ctx->stream, &ctx->launches));
+  int herr = 0;
+  MOAO_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (herr) return set_error(MOAO_ERR_TIMEOUT, "tc_gemm: bounded wait expired (" + std::to_string(herr) + ")");
+  return MOAO_OK;
+}

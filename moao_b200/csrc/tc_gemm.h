@@ -1,0 +1,59 @@
+// tcgen05 tensor-core GEMM (see tc_gemm.cu).
+#ifndef MOAO_TC_GEMM_H
+#define MOAO_TC_GEMM_H
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "moao_internal.h"
+
+namespace moao {
+
+constexpr int kTcMaxMaps = 3;
+constexpr int kTcMaxSegs = 8;
+enum TcKind { kTcBf16 = 0, kTcI8 = 1 };
+enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1 };
+
+// A K-major operand: rows x kcols elements, row stride in elements.
+struct TcTensor {
+  alignas(64) CUtensorMap map;
+  int kind = 0;
+  int kstep = 0;  // K elements per pipeline stage (64 bf16, 128 int8)
+};
+
+// One K segment: A tensor a and B tensor b over K elements [k0, k0 + nk*kstep).
+struct TcSegment {
+  int a, b;
+  int k0, nk;
+  int kstep;  // filled in by tc_gemm
+};
+
+struct TcGemm {
+  int kind = kTcBf16;
+  int epi = kTcEpiF32;
+  long M = 0, N = 0;
+  const TcTensor* A[kTcMaxMaps] = {};
+  int nA = 0;
+  const TcTensor* B[kTcMaxMaps] = {};
+  int nB = 0;
+  TcSegment seg[kTcMaxSegs] = {};
+  int nseg = 0;
+  int a_row0 = 0, b_row0 = 0;  // rows of A / B that map to C row / column 0
+  int lower = 0, diag_off = 0; // only C(r, c) with r + diag_off >= c
+  float alpha = 1.f, beta = 0.f;
+  void* C = nullptr;           // float (kTcEpiF32) or double (kTcEpiF64Scaled), column-major
+  long ldc = 0;
+  const int* erow = nullptr;   // kTcEpiF64Scaled: C += acc * 2^(erow[r] + ecol[c] + shift)
+  const int* ecol = nullptr;
+  int shift = 0;
+  int* err = nullptr;          // device flag: nonzero after a bounded wait expired
+};
+
+// Describes a row-major (K-contiguous) device matrix for TMA; box rows = 128.
+moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows, long long kcols,
+                        long long row_stride_elems, int box_rows = 128);
+moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches);
+
+}  // namespace moao
+
+#endif  // MOAO_TC_GEMM_H
