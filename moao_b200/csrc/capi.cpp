@@ -299,6 +299,10 @@ void moao_ctx_destroy(moao_ctx* c) {
   c->ws_dinv.release();
   c->ws_info.release();
   c->ws_tmp.release();
+  for (moao::DevBuf* b : {&c->mx_a32, &c->mx_lr, &c->mx_lc, &c->mx_t32, &c->mx_w1, &c->mx_w2,
+                          &c->mx_x, &c->mx_r64, &c->mx_e64, &c->mx_qa, &c->mx_qb, &c->mx_ea,
+                          &c->mx_fb, &c->mx_colmax, &c->mx_norm})
+    b->release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& p : c->pending) {
@@ -363,10 +367,25 @@ moao_status moao_ctx_reset_kernel_stats(moao_ctx* c) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_mixed(moao_ctx* c, int ozaki_slices, int max_refine, double tol,
+                               int final_residual) {
+  if (!c || ozaki_slices < 2 || ozaki_slices > 6 || max_refine < 0 || max_refine > 8 || tol < 0)
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_mixed: slices in [2, 6], max_refine in [0, 8]");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->ozaki_slices = ozaki_slices;
+  c->max_refine = max_refine;
+  c->refine_tol = tol;
+  c->final_residual = final_residual != 0;
+  c->mx_factored_n = -1;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_block(moao_ctx* c, int nb) {
   if (!c || nb < 64 || nb % 64 != 0 || nb > 2048)
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_block: nb must be a multiple of 64 in [64, 2048]");
+  std::lock_guard<std::mutex> lk(c->mu);
   c->nb = nb;
+  c->mx_factored_n = -1;
   return MOAO_OK;
 }
 

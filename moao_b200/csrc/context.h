@@ -11,6 +11,7 @@
 
 #include "moao_b200_tomo.hpp"
 #include "moao_internal.h"
+#include "dense.h"
 
 struct moao_tomo {
   Tomo_struct<double> t;
@@ -51,6 +52,14 @@ struct moao_ctx {
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
   moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
+  // mixed-precision workspace
+  moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
+      mx_ea, mx_fb, mx_colmax, mx_norm;
+  long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
+  int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
+  int max_refine = 2;        // refinement corrections per target
+  double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this
+  int final_residual = 0;    // evaluate the residual once more after the last correction
   cudaEvent_t ev[8] = {};
   // kernel timing
   bool timing = false;
@@ -88,6 +97,20 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* t, const DevGeometry
 // (n x nb, ld n) with the inverse of every diagonal block. info receives the
 // first failing column (1-based) or 0.
 moao_status potrf_f64(moao_ctx* ctx, double* A, long lda, long n, double* dinv, int* d_info);
+// C = alpha A op(B) + beta C in FP64, with optional lower-only C / triangular B
+// (see dense.h); accounted as kernel family gemm_f64.
+moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const double* A, long lda,
+                 const double* B, long ldb, bool transB, double beta, double* C, long ldc,
+                 bool lowerC = false, TriMode tri = TRI_FULL);
+// Factor the nb x nb diagonal block A in place (FP64) and write its inverse into D.
+moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long ldd, long nb,
+                            long col0, int* d_info, double* W);
+// Mixed-precision reconstructor for one target (see mixed.cpp); reuse = 1 keeps
+// the factorisation of the previous call.
+moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,
+                                double* Ctm, long ldCtm, bool reuse, moao_solve_report* rep);
+// Writes the mixed factorisation's (FP32) factor into the lower triangle of Cmm.
+moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm);
 // R = B * L^-T * L^-1 in place on B (m x n, ldb) using the factor and dinv.
 moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, const double* dinv,
                             double* B, long ldb, long m);

@@ -1,0 +1,315 @@
+// Mixed-precision reconstructor R = Ctm Cmm^-1 with FP64 iterative refinement.
+//
+// Factorisation (right-looking, panel nb, multiple of 64):
+//   A32 = float(Cmm) holds the trailing matrix.
+//   diagonal block: FP64 Cholesky + inverse (potrf_inv_block), kept in dinv
+//   panel: L_panel = double(A32 panel) * Dinv^T in FP64, stored FP32 in A32 and
+//          as bf16 hi/lo in two layouts: Lr (row-major, row r = L(r, :)) and
+//          Lc (row j = L(:, j)), both K-major operands of the tensor-core GEMM
+//   trailing: A32_22 -= L L^T on the lower tiles as hi*hi + hi*lo + lo*hi
+//          bf16 products accumulated in FP32 in TMEM (tc_gemm, three segments)
+// Solve (R = Ctm L^-T L^-1, right-looking forward then backward): block
+//   products with Dinv in FP64, long updates with the bf16 split factor on the
+//   tensor cores, state in FP32.
+// Refinement: E = Ctm - R sym(Cmm) with the int8 slice products of the Ozaki
+//   scheme (exact int32 accumulation, per-diagonal power-of-two scaling into
+//   FP64), dR = E (L L^T)^-1 by the same mixed solve, R += dR; repeated while
+//   ||E||/||Ctm|| is above the tolerance (at most max_refine times).
+// Cmm is read through its lower triangle and overwritten with the (FP32)
+// factor at the end, Ctm with R in FP64, like the FP64 path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "context.h"
+#include "mixed.h"
+#include "tc_gemm.h"
+
+namespace moao {
+namespace {
+
+long round_up(long x, long a) { return (x + a - 1) / a * a; }
+
+__global__ void sumsq_kernel(const double* __restrict__ A, long lda, long m, long n,
+                             double* __restrict__ out) {
+  double s = 0;
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const double v = A[(e / m) * lda + e % m];
+    s += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+moao_status sumsq(moao_ctx* ctx, const double* A, long lda, long m, long n, double* d_out,
+                  double* h_out) {
+  MOAO_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double), ctx->stream));
+  sumsq_kernel<<<148 * 4, 256, 0, ctx->stream>>>(A, lda, m, n, d_out);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  MOAO_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return MOAO_OK;
+}
+
+struct Maps {
+  TcTensor lr_hi, lr_lo, lc_hi, lc_lo, x_hi, x_lo;
+};
+
+// Tensor-core update C(f32, m x n, ldc) -= Xs * Ls^T over K = [0, nk*64) of the
+// X slices and [kb0, ...) of the L slices (rows b_row0..).
+moao_status tc_update(moao_ctx* ctx, const TcTensor* a_hi, const TcTensor* a_lo, int a_row0,
+                      int ka, const TcTensor* b_hi, const TcTensor* b_lo, int b_row0, int kb,
+                      int nk, long M, long N, float* C, long ldc, bool lower, int* err,
+                      double flops) {
+  TcGemm g;
+  g.kind = kTcBf16;
+  g.epi = kTcEpiF32;
+  g.M = M;
+  g.N = N;
+  g.A[0] = a_hi;
+  g.A[1] = a_lo;
+  g.nA = 2;
+  g.B[0] = b_hi;
+  g.B[1] = b_lo;
+  g.nB = 2;
+  const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+  for (int s = 0; s < 3; ++s) g.seg[s] = TcSegment{pa[s], pb[s], ka, kb, nk, 0};
+  g.nseg = 3;
+  g.a_row0 = a_row0;
+  g.b_row0 = b_row0;
+  g.lower = lower ? 1 : 0;
+  g.alpha = -1.f;
+  g.beta = 1.f;
+  g.C = C;
+  g.ldc = ldc;
+  g.err = err;
+  KernelTimer kt(ctx, "tc_bf16x3", flops);
+  return tc_gemm(g, ctx->stream, &ctx->launches);
+}
+
+// In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1.
+moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double* dinv, Maps& mp,
+                        double* W1, double* W2, void* x_hi, void* x_lo, long ldx, int* err) {
+  const long nb = ctx->nb;
+  cudaStream_t s = ctx->stream;
+  for (long k0 = 0; k0 < n; k0 += nb) {
+    const long kb = std::min(nb, n - k0);
+    MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
+    MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, true, 0.0, W2, m));
+    MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    const long rest = n - k0 - kb;
+    if (rest > 0) {
+      MOAO_TRY(split_bf16(W2, m, m, kb, x_hi, x_lo, ldx, nullptr, nullptr, 0, s));
+      MOAO_TRY(tc_update(ctx, &mp.x_hi, &mp.x_lo, 0, 0, &mp.lr_hi, &mp.lr_lo, (int)(k0 + kb),
+                         (int)k0, (int)((kb + 63) / 64), m, rest, T32 + (k0 + kb) * m, m, false,
+                         err, 3.0 * 2.0 * m * rest * kb));
+    }
+  }
+  const long nblk = (n + nb - 1) / nb;
+  for (long b = nblk - 1; b >= 0; --b) {
+    const long k0 = b * nb, kb = std::min(nb, n - k0);
+    MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
+    MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
+    MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    if (k0 > 0) {
+      MOAO_TRY(split_bf16(W2, m, m, kb, x_hi, x_lo, ldx, nullptr, nullptr, 0, s));
+      MOAO_TRY(tc_update(ctx, &mp.x_hi, &mp.x_lo, 0, 0, &mp.lc_hi, &mp.lc_lo, 0, (int)k0,
+                         (int)((kb + 63) / 64), m, k0, T32, m, false, err,
+                         3.0 * 2.0 * m * k0 * kb));
+    }
+  }
+  return MOAO_OK;
+}
+
+}  // namespace
+
+moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,
+                                double* Ctm, long ldCtm, bool reuse, moao_solve_report* rep) {
+  const long nb = ctx->nb;
+  cudaStream_t s = ctx->stream;
+  const long ldn = round_up(n, 64);    // bf16 row stride of the factor copies
+  const long ldq = round_up(n, 128);   // int8 row stride of the slices
+  const int ns = ctx->ozaki_slices;
+  const long ldx = nb;
+  // ---- workspace
+  MOAO_TRY(ctx->mx_a32.ensure(sizeof(float) * (size_t)n * n));
+  MOAO_TRY(ctx->mx_lr.ensure(2 * sizeof(uint16_t) * (size_t)n * ldn));
+  MOAO_TRY(ctx->mx_lc.ensure(2 * sizeof(uint16_t) * (size_t)n * ldn));
+  MOAO_TRY(ctx->mx_t32.ensure(sizeof(float) * (size_t)m * n));
+  const size_t wbytes = sizeof(double) * (size_t)std::max(n, m) * nb;
+  MOAO_TRY(ctx->mx_w1.ensure(wbytes));
+  MOAO_TRY(ctx->mx_w2.ensure(wbytes));
+  MOAO_TRY(ctx->mx_x.ensure(2 * sizeof(uint16_t) * (size_t)std::max(n, m) * ldx));
+  MOAO_TRY(ctx->mx_r64.ensure(sizeof(double) * (size_t)m * n));
+  MOAO_TRY(ctx->mx_e64.ensure(sizeof(double) * (size_t)m * n));
+  MOAO_TRY(ctx->mx_qa.ensure((size_t)ns * m * ldq));
+  MOAO_TRY(ctx->mx_qb.ensure((size_t)ns * n * ldq));
+  MOAO_TRY(ctx->mx_ea.ensure(sizeof(int) * (size_t)m));
+  MOAO_TRY(ctx->mx_fb.ensure(sizeof(int) * (size_t)n));
+  MOAO_TRY(ctx->mx_colmax.ensure(sizeof(unsigned long long) * (size_t)n));
+  MOAO_TRY(ctx->mx_norm.ensure(sizeof(double) * 2));
+  MOAO_TRY(ctx->ws_dinv.ensure(sizeof(double) * (size_t)n * nb));
+  MOAO_TRY(ctx->ws_w.ensure(sizeof(double) * (size_t)std::max(n, 1L) * nb));
+  MOAO_TRY(ctx->ws_info.ensure(2 * sizeof(int)));
+  float* A32 = ctx->mx_a32.as<float>();
+  uint16_t* lr = ctx->mx_lr.as<uint16_t>();
+  uint16_t* lc = ctx->mx_lc.as<uint16_t>();
+  uint16_t* lr_lo = lr + (size_t)n * ldn;
+  uint16_t* lc_lo = lc + (size_t)n * ldn;
+  uint16_t* xh = ctx->mx_x.as<uint16_t>();
+  uint16_t* xl = xh + (size_t)std::max(n, m) * ldx;
+  float* T32 = ctx->mx_t32.as<float>();
+  double* W1 = ctx->mx_w1.as<double>();
+  double* W2 = ctx->mx_w2.as<double>();
+  double* R64 = ctx->mx_r64.as<double>();
+  double* E64 = ctx->mx_e64.as<double>();
+  int8_t* qa = ctx->mx_qa.as<int8_t>();
+  int8_t* qb = ctx->mx_qb.as<int8_t>();
+  int* ea = ctx->mx_ea.as<int>();
+  int* fb = ctx->mx_fb.as<int>();
+  double* dinv = ctx->ws_dinv.as<double>();
+  int* d_info = ctx->ws_info.as<int>();
+  int* err = d_info + 1;
+
+  Maps mp;
+  MOAO_TRY(make_tc_map(&mp.lr_hi, lr, kTcBf16, n, n, ldn));
+  MOAO_TRY(make_tc_map(&mp.lr_lo, lr_lo, kTcBf16, n, n, ldn));
+  MOAO_TRY(make_tc_map(&mp.lc_hi, lc, kTcBf16, n, n, ldn));
+  MOAO_TRY(make_tc_map(&mp.lc_lo, lc_lo, kTcBf16, n, n, ldn));
+  MOAO_TRY(make_tc_map(&mp.x_hi, xh, kTcBf16, m, nb, ldx));
+  MOAO_TRY(make_tc_map(&mp.x_lo, xl, kTcBf16, m, nb, ldx));
+
+  cudaEvent_t* ev = ctx->ev;
+  cudaEventRecord(ev[3], s);
+  if (!reuse || ctx->mx_factored_n != n) {
+    MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 2 * sizeof(int), s));
+    MOAO_TRY(cvt_f64_to_f32(Cmm, ldCmm, A32, n, n, n, true, s));
+    for (long k0 = 0; k0 < n; k0 += nb) {
+      const long kb = std::min(nb, n - k0);
+      float* Akk = A32 + k0 + k0 * n;
+      MOAO_TRY(cvt_f32_to_f64(Akk, n, W1, kb, kb, kb, true, s));
+      MOAO_TRY(potrf_inv_block(ctx, W1, kb, dinv + k0, n, kb, k0, d_info, ctx->ws_w.as<double>()));
+      MOAO_TRY(cvt_f64_to_f32(W1, kb, Akk, n, kb, kb, true, s));
+      const long rest = n - k0 - kb;
+      if (rest <= 0) break;
+      float* P = A32 + (k0 + kb) + k0 * n;
+      MOAO_TRY(cvt_f32_to_f64(P, n, W1, rest, rest, kb, false, s));
+      MOAO_TRY(gemm(ctx, rest, kb, kb, 1.0, W1, rest, dinv + k0, n, true, 0.0, W2, rest));
+      MOAO_TRY(cvt_f64_to_f32(W2, rest, P, n, rest, kb, false, s));
+      MOAO_TRY(split_bf16(W2, rest, rest, kb, lr + (k0 + kb) * ldn + k0,
+                          lr_lo + (k0 + kb) * ldn + k0, ldn, lc + k0 * ldn + (k0 + kb),
+                          lc_lo + k0 * ldn + (k0 + kb), ldn, s));
+      MOAO_TRY(tc_update(ctx, &mp.lr_hi, &mp.lr_lo, (int)(k0 + kb), (int)k0, &mp.lr_hi,
+                         &mp.lr_lo, (int)(k0 + kb), (int)k0, (int)(kb / 64), rest, rest,
+                         A32 + (k0 + kb) + (k0 + kb) * n, n, true, err,
+                         3.0 * (double)rest * rest * kb));
+    }
+    int info[2] = {0, 0};
+    MOAO_CUDA_TRY(cudaMemcpyAsync(info, d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+    if (info[1]) return set_error(MOAO_ERR_TIMEOUT, "tensor-core update: bounded wait expired");
+    rep->info = info[0];
+    if (info[0]) {
+      ctx->mx_factored_n = -1;
+      return set_error(MOAO_ERR_NOT_SPD, "mixed Cholesky: non-positive pivot at column " +
+                                             std::to_string(info[0]));
+    }
+    // int8 slices of sym(Cmm) for the refinement residual
+    MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
+                             ldq, s));
+    ctx->mx_factored_n = n;
+  }
+  cudaEventRecord(ev[4], s);
+  // ---- solve
+  MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
+  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xh, xl, ldx, err));
+  MOAO_TRY(cvt_f32_to_f64(T32, m, R64, m, m, n, false, s));
+  cudaEventRecord(ev[5], s);
+  // ---- refinement
+  TcTensor ta[kMaxOzakiSlices], tb[kMaxOzakiSlices];
+  for (int i = 0; i < ns; ++i) {
+    MOAO_TRY(make_tc_map(&ta[i], qa + (size_t)i * m * ldq, kTcI8, m, n, ldq));
+    MOAO_TRY(make_tc_map(&tb[i], qb + (size_t)i * n * ldq, kTcI8, n, n, ldq));
+  }
+  double* dnorm = ctx->mx_norm.as<double>();
+  double ctm2 = 0, e2 = 0;
+  MOAO_TRY(sumsq(ctx, Ctm, ldCtm, m, n, dnorm, &ctm2));
+  auto residual = [&]() -> moao_status {
+    // E = Ctm - R sym(Cmm) from the int8 slice products
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
+                                    m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+    MOAO_TRY(ozaki_split_rows(R64, m, m, n, ns, ea, qa, ldq, s));
+    const long pair_cap = std::max(1L, (long)(2147483647.0 / (4096.0 * (double)n)));
+    for (int d = 2; d <= ns + 1; ++d) {
+      std::vector<std::pair<int, int>> pairs;
+      for (int p = 1; p <= ns; ++p)
+        if (d - p >= 1 && d - p <= ns) pairs.push_back({p - 1, d - p - 1});
+      for (size_t b0 = 0; b0 < pairs.size(); b0 += pair_cap) {
+        TcGemm g;
+        g.kind = kTcI8;
+        g.epi = kTcEpiF64Scaled;
+        g.M = m;
+        g.N = n;
+        for (int i = 0; i < ns; ++i) {
+          g.A[i] = &ta[i];
+          g.B[i] = &tb[i];
+        }
+        g.nA = g.nB = ns;
+        const size_t b1 = std::min(pairs.size(), b0 + (size_t)pair_cap);
+        for (size_t q = b0; q < b1; ++q)
+          g.seg[g.nseg++] = TcSegment{pairs[q].first, pairs[q].second, 0, 0,
+                                      (int)((n + 127) / 128), 0};
+        g.alpha = -1.f;
+        g.C = E64;
+        g.ldc = m;
+        g.erow = ea;
+        g.ecol = fb;
+        g.shift = -12 - 7 * (d - 2);
+        g.err = err;
+        KernelTimer kt(ctx, "tc_int8", 2.0 * m * (double)n * n * (double)(b1 - b0));
+        MOAO_TRY(tc_gemm(g, s, &ctx->launches));
+      }
+    }
+    MOAO_TRY(sumsq(ctx, E64, m, m, n, dnorm, &e2));
+    rep->refine_resid = std::sqrt(e2 / std::max(ctm2, 1e-300));
+    return MOAO_OK;
+  };
+  int steps = 0;
+  for (; steps < ctx->max_refine; ++steps) {
+    MOAO_TRY(residual());
+    if (rep->refine_resid <= ctx->refine_tol) break;
+    MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
+    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xh, xl, ldx, err));
+    MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
+  }
+  if (ctx->final_residual) MOAO_TRY(residual());
+  rep->refine_steps = steps;
+  // ---- outputs: R in FP64, the FP32 factor into the lower triangle of Cmm
+  MOAO_CUDA_TRY(cudaMemcpy2DAsync(Ctm, ldCtm * sizeof(double), R64, m * sizeof(double),
+                                  m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+  cudaEventRecord(ev[6], s);
+  int herr = 0;
+  MOAO_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) return set_error(MOAO_ERR_TIMEOUT, "tensor-core kernel: bounded wait expired");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev[3], ev[4]);
+  rep->ms_factor += ms;
+  cudaEventElapsedTime(&ms, ev[4], ev[5]);
+  rep->ms_solve += ms;
+  cudaEventElapsedTime(&ms, ev[5], ev[6]);
+  rep->ms_refine += ms;
+  return MOAO_OK;
+}
+
+moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm) {
+  MOAO_TRY(cvt_f32_to_f64(ctx->mx_a32.as<float>(), n, Cmm, ldCmm, n, n, true, ctx->stream));
+  ctx->mx_factored_n = -1;
+  return MOAO_OK;
+}
+
+}  // namespace moao

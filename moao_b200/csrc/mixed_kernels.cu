@@ -1,0 +1,270 @@
+// Conversion and slicing kernels of the mixed-precision reconstructor.
+//
+//   cvt_*            FP32 <-> FP64 copies of column-major blocks
+//   split_bf16       FP64 block -> bf16 hi + lo (hi = bf16(x), lo = bf16(x - hi)),
+//                    written row-major (K-major operand of the tensor-core GEMM,
+//                    via a shared-memory transpose) and/or column-major
+//   ozaki_*          int8 slices for the exact-accumulation residual: every row of
+//                    R (and every column of the symmetric Cmm) gets a power-of-two
+//                    exponent e with max |x| < 2^e; then
+//                      x 2^-e = sum_p q_p 2^-(6 + 7(p-1)),  q_p in [-64, 64],
+//                    each q_p the rounded remainder of the previous slice, so the
+//                    products of slices accumulate exactly in int32.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "mixed.h"
+
+namespace moao {
+namespace {
+
+unsigned blocks_for(long total, long per = 256) {
+  return (unsigned)std::max(1L, std::min((total + per - 1) / per, 148L * 16));
+}
+
+__global__ void cvt_f32_f64_kernel(const float* __restrict__ s, long lds, double* __restrict__ d,
+                                   long ldd, long m, long n, int lower) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    if (lower && i < j) continue;
+    d[j * ldd + i] = (double)s[j * lds + i];
+  }
+}
+
+__global__ void cvt_f64_f32_kernel(const double* __restrict__ s, long lds, float* __restrict__ d,
+                                   long ldd, long m, long n, int lower) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    if (lower && i < j) continue;
+    d[j * ldd + i] = (float)s[j * lds + i];
+  }
+}
+
+__global__ void add_f32_to_f64_kernel(const float* __restrict__ s, long lds, double* __restrict__ d,
+                                      long ldd, long m, long n) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    d[j * ldd + i] += (double)s[j * lds + i];
+  }
+}
+
+// 32x32 tiles, 32x8 threads.
+__global__ void split_bf16_kernel(const double* __restrict__ src, long lds, long m, long n,
+                                  __nv_bfloat16* hr, __nv_bfloat16* lr, long ldr,
+                                  __nv_bfloat16* hc, __nv_bfloat16* lc, long ldc) {
+  __shared__ __nv_bfloat16 sh[32][34], sl[32][34];
+  const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long r = r0 + tx, c = c0 + jj;
+    __nv_bfloat16 h = __float2bfloat16(0.f), l = h;
+    if (r < m && c < n) {
+      const double x = src[c * lds + r];
+      h = __double2bfloat16(x);
+      l = __double2bfloat16(x - (double)__bfloat162float(h));
+      if (hc) {
+        hc[c * ldc + r] = h;
+        lc[c * ldc + r] = l;
+      }
+    }
+    sh[tx][jj] = h;
+    sl[tx][jj] = l;
+  }
+  if (!hr) return;
+  __syncthreads();
+  for (int ii = ty; ii < 32; ii += 8) {
+    const long r = r0 + ii, c = c0 + tx;
+    if (r < m && c < n) {
+      hr[r * ldr + c] = sh[ii][tx];
+      lr[r * ldr + c] = sl[ii][tx];
+    }
+  }
+}
+
+__device__ __forceinline__ int exponent_of(double mx) {
+  // smallest e with mx < 2^e (0 for an all-zero row)
+  if (!(mx > 0)) return 0;
+  return ilogb(mx) + 1;
+}
+
+// Row maxima of a column-major m x n block: 32 rows per block, 8 column strides.
+__global__ void row_exponent_kernel(const double* __restrict__ A, long lda, long m, long n,
+                                    int* __restrict__ e) {
+  __shared__ double red[8][33];
+  const long r = (long)blockIdx.x * 32 + threadIdx.x;
+  double mx = 0;
+  if (r < m)
+    for (long c = threadIdx.y; c < n; c += 8) mx = fmax(mx, fabs(A[c * lda + r]));
+  red[threadIdx.y][threadIdx.x] = mx;
+  __syncthreads();
+  if (threadIdx.y == 0 && r < m) {
+    for (int k = 1; k < 8; ++k) mx = fmax(mx, red[k][threadIdx.x]);
+    e[r] = exponent_of(mx);
+  }
+}
+
+// Slices of the rows of a column-major m x n block into row-major int8 (ldo).
+__global__ void split_rows_i8_kernel(const double* __restrict__ A, long lda, long m, long n,
+                                     const int* __restrict__ e, int ns, int8_t* out, long ldo,
+                                     long slice_stride) {
+  __shared__ int8_t q[kMaxOzakiSlices][32][36];
+  const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long r = r0 + tx, c = c0 + jj;
+    double v = 0;
+    if (r < m && c < n) v = ldexp(A[c * lda + r], 6 - e[r]);
+    for (int s = 0; s < ns; ++s) {
+      const double qv = rint(v);
+      q[s][tx][jj] = (int8_t)qv;
+      v = (v - qv) * 128.0;
+    }
+  }
+  __syncthreads();
+  for (int ii = ty; ii < 32; ii += 8) {
+    const long r = r0 + ii, c = c0 + tx;
+    if (r < m && c < n)
+      for (int s = 0; s < ns; ++s) out[s * slice_stride + r * ldo + c] = q[s][ii][tx];
+  }
+}
+
+// Column maxima of sym(A) for a lower-stored n x n A: every stored (r >= c)
+// element feeds column c and column r.
+__global__ void sym_col_max_kernel(const double* __restrict__ A, long lda, long n,
+                                   unsigned long long* __restrict__ cm) {
+  const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
+  if (r0 + 31 < c0) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  __shared__ double t[32][33];
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long r = r0 + tx, c = c0 + jj;
+    t[tx][jj] = (r < n && c < n && r >= c) ? fabs(A[c * lda + r]) : 0.0;
+  }
+  __syncthreads();
+  if (ty == 0) {  // column c0 + tx: max over the 32 rows
+    double mx = 0;
+    for (int i = 0; i < 32; ++i) mx = fmax(mx, t[i][tx]);
+    if (c0 + tx < n) atomicMax(&cm[c0 + tx], __double_as_longlong(mx));
+  } else if (ty == 1) {  // row r0 + tx: max over the 32 columns (its mirrored column)
+    double mx = 0;
+    for (int j = 0; j < 32; ++j) mx = fmax(mx, t[tx][j]);
+    if (r0 + tx < n) atomicMax(&cm[r0 + tx], __double_as_longlong(mx));
+  }
+}
+
+__global__ void exponents_from_max_kernel(const unsigned long long* __restrict__ cm, long n,
+                                          int* __restrict__ f) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) f[i] = exponent_of(__longlong_as_double((long long)cm[i]));
+}
+
+// Slices of sym(A) by columns, written as B[j * ldo + k] = slice(S(k, j)) (the
+// K-major B operand of S), S(k, j) = A(max(k,j), min(k,j)).
+__global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long n,
+                                    const int* __restrict__ f, int ns, int8_t* out, long ldo,
+                                    long slice_stride) {
+  __shared__ double t[32][33];  // t[jj][kk] = S(k0+kk, j0+jj)
+  const long j0 = (long)blockIdx.x * 32, k0 = (long)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (k0 >= j0 + 32) {
+    // k > j everywhere: S(k, j) = A(k, j), contiguous in k
+    for (int jj = ty; jj < 32; jj += 8) {
+      const long k = k0 + tx, j = j0 + jj;
+      t[jj][tx] = (k < n && j < n) ? A[j * lda + k] : 0.0;
+    }
+  } else if (k0 + 32 <= j0) {
+    // k < j everywhere: S(k, j) = A(j, k), contiguous in j
+    for (int kk = ty; kk < 32; kk += 8) {
+      const long j = j0 + tx, k = k0 + kk;
+      t[tx][kk] = (k < n && j < n) ? A[k * lda + j] : 0.0;
+    }
+  } else {
+    for (int jj = ty; jj < 32; jj += 8) {
+      const long k = k0 + tx, j = j0 + jj;
+      double v = 0;
+      if (k < n && j < n) v = (k >= j) ? A[j * lda + k] : A[k * lda + j];
+      t[jj][tx] = v;
+    }
+  }
+  __syncthreads();
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long j = j0 + jj, k = k0 + tx;
+    if (j >= n || k >= n) continue;
+    double v = ldexp(t[jj][tx], 6 - f[j]);
+    for (int s = 0; s < ns; ++s) {
+      const double qv = rint(v);
+      out[s * slice_stride + j * ldo + k] = (int8_t)qv;
+      v = (v - qv) * 128.0;
+    }
+  }
+}
+
+}  // namespace
+
+moao_status cvt_f32_to_f64(const float* s, long lds, double* d, long ldd, long m, long n,
+                           bool lower, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  cvt_f32_f64_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n, lower);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status cvt_f64_to_f32(const double* s, long lds, float* d, long ldd, long m, long n,
+                           bool lower, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  cvt_f64_f32_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n, lower);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status add_f32_to_f64(const float* s, long lds, double* d, long ldd, long m, long n,
+                           cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  add_f32_to_f64_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status split_bf16(const double* src, long lds, long m, long n, void* hi_r, void* lo_r,
+                       long ldr, void* hi_c, void* lo_c, long ldc, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+  split_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(
+      src, lds, m, n, (__nv_bfloat16*)hi_r, (__nv_bfloat16*)lo_r, ldr, (__nv_bfloat16*)hi_c,
+      (__nv_bfloat16*)lo_c, ldc);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
+                             int8_t* out, long ldo, cudaStream_t st) {
+  if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
+  row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e);
+  dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+  split_rows_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, m, n, e, ns, out, ldo, m * ldo);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status ozaki_split_sym(const double* A, long lda, long n, int ns, int* f,
+                            unsigned long long* colmax, int8_t* out, long ldo, cudaStream_t st) {
+  if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
+  MOAO_CUDA_TRY(cudaMemsetAsync(colmax, 0, n * sizeof(unsigned long long), st));
+  dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+  sym_col_max_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, colmax);
+  exponents_from_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(colmax, n, f);
+  split_sym_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, f, ns, out, ldo, n * ldo);
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+}  // namespace moao

@@ -16,13 +16,11 @@
 
 namespace moao {
 
-namespace {
-
 constexpr int kLeaf = 64;
 
 moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const double* A, long lda,
                  const double* B, long ldb, bool transB, double beta, double* C, long ldc,
-                 bool lowerC = false, TriMode tri = TRI_FULL) {
+                 bool lowerC, TriMode tri) {
   GemmArgs g;
   g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
   g.A = A; g.lda = lda; g.B = B; g.ldb = ldb; g.transB = transB; g.triB = tri;
@@ -64,8 +62,6 @@ moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long 
   MOAO_TRY(fill_matrix(D + n1 * ldd, ldd, n1, n2, 0.0, ctx->stream, &ctx->launches));
   return MOAO_OK;
 }
-
-}  // namespace
 
 moao_status potrf_f64(moao_ctx* ctx, double* A, long lda, long n, double* dinv, int* d_info) {
   const long nb = ctx->nb;
@@ -137,9 +133,18 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
   moao_solve_report* r = rep ? rep : &local;
   std::memset(r, 0, sizeof(*r));
   if (nmeas == 0) return MOAO_OK;
-  if (prec == MOAO_PREC_MIXED)
-    return set_error(MOAO_ERR_UNSUPPORTED, "reconstructor: mixed precision not built yet");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  if (prec == MOAO_PREC_MIXED) {
+    MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+    for (long g = 0; g < ngal; ++g) {
+      // one factorisation serves every target: later targets reuse it
+      MOAO_TRY(reconstructor_mixed(ctx, nmeas, nmeasts, d_Cmm, ldCmm,
+                                   d_Ctm + nmeas * nmeasts * g, ldCtm, g > 0, r));
+    }
+    MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
+    MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return MOAO_OK;
+  }
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   MOAO_TRY(ctx->ws_dinv.ensure(sizeof(double) * (size_t)nmeas * ctx->nb));
   MOAO_TRY(ctx->ws_info.ensure(sizeof(int)));

@@ -203,9 +203,10 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
         uint8_t* sa = smem + st * STAGE_BYTES;
         uint8_t* sb = sa + A_TILE;
         mbar_expect_tx(&full_bar[st], STAGE_BYTES);
-        const int kx = sg.k0 + kb * sg.kstep;  // element coordinate along K
-        tma_load_2d(sa, &p.mapA[sg.a], kx, p.a_row0 + m0, &full_bar[st]);
-        tma_load_2d(sb, &p.mapB[sg.b], kx, p.b_row0 + n0, &full_bar[st]);
+        const int kxa = sg.ka + kb * sg.kstep;  // element coordinates along K
+        const int kxb = sg.kb + kb * sg.kstep;
+        tma_load_2d(sa, &p.mapA[sg.a], kxa, p.a_row0 + m0, &full_bar[st]);
+        tma_load_2d(sb, &p.mapB[sg.b], kxb, p.b_row0 + n0, &full_bar[st]);
       }
     }
     // Never leave the CTA with a bulk copy still writing its shared memory:
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
             } else {
               double* dst = static_cast<double*>(p.C) + (size_t)c * p.ldc + r;
               const double a = (double)(int)v[j];
-              *dst += ldexp(a, p.erow[r] + p.ecol[c] + p.shift);
+              *dst += (double)p.alpha * ldexp(a, p.erow[r] + p.ecol[c] + p.shift);
             }
           }
         }
@@ -347,8 +348,8 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   const int kstep = g.A[0]->kstep;
   for (int i = 0; i < g.nseg; ++i) {
     TcSegment sg = g.seg[i];
-    if (sg.a < 0 || sg.a >= g.nA || sg.b < 0 || sg.b >= g.nB || sg.nk < 0 || sg.k0 < 0 ||
-        sg.k0 % kstep)
+    if (sg.a < 0 || sg.a >= g.nA || sg.b < 0 || sg.b >= g.nB || sg.nk < 0 || sg.ka < 0 ||
+        sg.kb < 0 || sg.ka % kstep || sg.kb % kstep)
       return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: bad segment");
     sg.kstep = kstep;
     p.seg[i] = sg;
@@ -419,7 +420,8 @@ extern "C" moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long 
   for (int p = 0; p < npairs; ++p) {
     g.seg[p].a = pa[p];
     g.seg[p].b = pb[p];
-    g.seg[p].k0 = 0;
+    g.seg[p].ka = 0;
+    g.seg[p].kb = 0;
     g.seg[p].nk = (int)((K + kstep - 1) / kstep);
   }
   g.nseg = npairs;

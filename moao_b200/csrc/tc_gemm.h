@@ -9,7 +9,7 @@
 
 namespace moao {
 
-constexpr int kTcMaxMaps = 3;
+constexpr int kTcMaxMaps = 6;
 constexpr int kTcMaxSegs = 8;
 enum TcKind { kTcBf16 = 0, kTcI8 = 1 };
 enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1 };
@@ -21,10 +21,11 @@ struct TcTensor {
   int kstep = 0;  // K elements per pipeline stage (64 bf16, 128 int8)
 };
 
-// One K segment: A tensor a and B tensor b over K elements [k0, k0 + nk*kstep).
+// One K segment: A tensor a over K elements [ka, ka + nk*kstep) times B tensor
+// b over [kb, kb + nk*kstep).
 struct TcSegment {
   int a, b;
-  int k0, nk;
+  int ka, kb, nk;
   int kstep;  // filled in by tc_gemm
 };
 

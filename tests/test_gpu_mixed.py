@@ -1,0 +1,113 @@
+"""Mixed-precision reconstructor against the FP64 oracle, through the C ABI.
+
+Tolerance: relative Frobenius error of R <= 1e-5 against FP64 (the accuracy the
+mixed path is specified to), with the residual ||Ctm - R Cmm||_F / ||Ctm||_F
+reported by the library after the last refinement step. Defaults: bf16 hi/lo
+split products (about 16 significant bits) in the factorisation and the solves,
+two refinement steps, residual from 5 int8 slices per operand (measured: 3e-3
+before refinement, 1.6e-4 after one step, 8e-6 after two on the 39 m systems).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import systems
+import moao_b200 as M
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(A):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(A, dtype=np.float64).T)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy().T.copy(order="F")
+
+
+def case(name):
+    sf, af = systems.files(name)
+    t = M.Tomo(sf, af)
+    g = O.Geometry.from_tomo(t)
+    nm, nts = g.nmeas, g.nmeasts
+    Cmm = O.matcov(g, nm, nm, 0, 0, 1, nthreads=8)
+    Ctm = O.matcov(g, nts, nm, 0, 0, 3, nthreads=8)
+    return nm, nts, Cmm, Ctm
+
+
+def run_mixed(ctx, nm, nts, Cmm, Ctm, nb=256, slices=5, refine=2):
+    ctx.set_block(nb)
+    ctx.set_mixed(ozaki_slices=slices, max_refine=refine, final_residual=True)
+    try:
+        dC, dT = dev(Cmm), dev(Ctm)
+        rep = M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=ctx)
+        ctx.synchronize()
+    finally:
+        ctx.set_block(256)
+        ctx.set_mixed()
+    return host(dC), host(dT), rep
+
+
+@pytest.mark.parametrize("name,nb", [("small", 128), ("elt16", 256), ("elt16", 512)])
+def test_mixed_matches_fp64(ctx, name, nb):
+    nm, nts, Cmm, Ctm = case(name)
+    L_ref, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    L, R, rep = run_mixed(ctx, nm, nts, Cmm, Ctm, nb=nb)
+    err = O.rel_fro(R, R_ref)
+    assert err <= 1e-5, (err, rep)
+    assert rep["refine_steps"] == 2
+    # the factor written back is the FP32-accurate lower Cholesky factor
+    assert O.rel_fro(np.tril(L), np.tril(L_ref)) < 1e-4
+    assert np.array_equal(np.triu(L, 1), np.triu(Cmm, 1))
+
+
+def test_mixed_refinement_reduces_error(ctx):
+    nm, nts, Cmm, Ctm = case("elt16")
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    _, R0, rep0 = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=0)
+    _, R2, rep2 = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=2)
+    e0, e2 = O.rel_fro(R0, R_ref), O.rel_fro(R2, R_ref)
+    assert e2 < e0 / 100, (e0, e2)
+    # 4 int8 slices leave the residual too coarse to converge to 1e-5
+    _, R4, _ = run_mixed(ctx, nm, nts, Cmm, Ctm, slices=4, refine=2)
+    assert O.rel_fro(R4, R_ref) > 1e-4
+    assert rep2["refine_resid"] < rep0["refine_resid"]
+
+
+def test_mixed_ill_conditioned_check_system(ctx):
+    """The reference's check system with lgs_cst = 1 has kappa ~ 2e7; more
+    refinement steps are needed there, and they converge."""
+    nm, nts, Cmm, Ctm = case("check2")
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    _, R, rep = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=4)
+    assert O.rel_fro(R, R_ref) <= 1e-5, rep
+
+
+def test_mixed_multiple_targets(ctx):
+    import torch
+    nm, nts, Cmm, Ctm = case("small")
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    T2 = np.concatenate([Ctm.flatten("F"), -2.0 * Ctm.flatten("F")])
+    dT = torch.from_numpy(T2).cuda()
+    dC = dev(Cmm)
+    ctx.set_mixed(final_residual=True)
+    try:
+        M.reconstructor(nm, nts, dC, nm, dT, nts, 2, prec="mixed", ctx=ctx)
+        ctx.synchronize()
+    finally:
+        ctx.set_mixed()
+    out = dT.cpu().numpy()
+    R0 = out[: nm * nts].reshape((nts, nm), order="F")
+    R1 = out[nm * nts:].reshape((nts, nm), order="F")
+    assert O.rel_fro(R0, R_ref) <= 1e-5
+    assert O.rel_fro(R1, -2.0 * R_ref) <= 1e-5
+
+
+def test_mixed_not_spd(ctx):
+    n = 256
+    C = np.eye(n)
+    C[200, 200] = -4.0
+    with pytest.raises(M.NotSPDError) as e:
+        M.reconstructor(n, 2, dev(C), n, dev(np.ones((2, n))), 2, 1, prec="mixed", ctx=ctx)
+    assert e.value.column == 201
