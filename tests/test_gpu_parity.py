@@ -71,6 +71,7 @@ def test_matcov_symmetric_fill_and_tiles(ctx):
     full = np.tril(want) + np.tril(want, -1).T
     d = torch.zeros((nm, nm), dtype=torch.float64, device="cuda")
     M.matcov_tile(d, nm, nm, 0, 0, nm, t, 5, ctx=ctx)
+    ctx.synchronize()
     assert_close(host(d), full, 1e-11, "type 5")
     # tiles at odd offsets through the host-buffer entry point, with untouched
     # elements preserved (the reference only writes the lower triangle)
