@@ -68,6 +68,7 @@ SIGNATURES = {
     "moao_matcov_tile_host": (i32, [vp, vp, dp, i32, i32, i32, i32, i32, i32]),
     "moao_reconstructor": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, i32, C.POINTER(SolveReport)]),
     "moao_reconstructor_host": (i32, [vp, i64, i64, dp, i64, dp, i64, i64, C.POINTER(SolveReport)]),
+    "moao_reconstructor_noalloc": (i32, [i64, i64, dp, i64, dp, i64, i64, vp, C.POINTER(i32)]),
     "moao_cee_cvv": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
     "moao_cee_cvv_host": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
     "moao_intersample_create": (i32, [vp, i64, i64, C.c_double, dp, dp, dp, C.POINTER(vp)]),
