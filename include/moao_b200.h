@@ -92,19 +92,23 @@ long long moao_ctx_launch_count(const moao_ctx* ctx);
 /* Panel width of the blocked factorisation (default 256; multiple of 64). */
 moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
 
-/* Options of the mixed-precision reconstructor: int8 slices per operand of the
- * refinement residual (2..6, default 5), refinement corrections per target
- * (0..8, default 2), residual tolerance that stops refinement early (default 0)
- * and whether to evaluate the residual again after the last correction (so the
- * report's refine_resid describes the returned R; default 0). */
-moao_status moao_ctx_set_mixed(moao_ctx* ctx, int ozaki_slices, int max_refine, double tol,
-                               int final_residual);
+/* Options of the mixed-precision reconstructor: bf16 slices of the factor in
+ * the first solve (2: ~16 significant bits, 3 products; 3: ~24 bits, 6
+ * products; default 3), bf16 slices of the factor in the correction solves
+ * (2 or 3, at most bf16_slices; default 2), int8
+ * slices per operand of the refinement residual (2..6, default 5), refinement
+ * corrections per target (0..8, default 2), residual tolerance that stops
+ * refinement early (default 0) and whether to evaluate the residual again after
+ * the last correction (so the report's refine_resid describes the returned R;
+ * default 0). */
+moao_status moao_ctx_set_mixed(moao_ctx* ctx, int bf16_slices, int corr_slices, int ozaki_slices,
+                               int max_refine, double tol, int final_residual);
 
 /* Per-kernel-family device timing. When enabled, every launch of the library's
  * kernels is bracketed by CUDA events on the context stream and accumulated per
  * family together with its algorithmic work (flops for contractions, elements
  * for covariance generation). Families: "gemm_f64", "potrf_leaf", "matcov",
- * "tc_bf16x3", "tc_int8". */
+ * "tc_bf16", "tc_int8". */
 moao_status moao_ctx_set_kernel_timing(moao_ctx* ctx, int enable);
 /* Synchronises, then reports launches, total device ms and total work of one
  * family since the last reset. */

@@ -60,7 +60,7 @@ SIGNATURES = {
     "moao_ctx_launch_count": (C.c_longlong, [vp]),
     "moao_ctx_set_block": (i32, [vp, i32]),
     "moao_ctx_set_kernel_timing": (i32, [vp, i32]),
-    "moao_ctx_set_mixed": (i32, [vp, i32, i32, C.c_double, i32]),
+    "moao_ctx_set_mixed": (i32, [vp, i32, i32, i32, i32, C.c_double, i32]),
     "moao_ctx_kernel_stats": (i32, [vp, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),
     "moao_ctx_reset_kernel_stats": (i32, [vp]),

@@ -109,10 +109,11 @@ class Context:
     def set_block(self, nb: int):
         check(lib().moao_ctx_set_block(self._h, nb), "moao_ctx_set_block")
 
-    def set_mixed(self, ozaki_slices: int = 5, max_refine: int = 2, tol: float = 0.0,
-                  final_residual: bool = False):
+    def set_mixed(self, bf16_slices: int = 3, ozaki_slices: int = 5, max_refine: int = 2,
+                  tol: float = 0.0, final_residual: bool = False, corr_slices: int = 2):
         """Options of the mixed-precision reconstructor (see moao_ctx_set_mixed)."""
-        check(lib().moao_ctx_set_mixed(self._h, ozaki_slices, max_refine, tol, int(final_residual)),
+        check(lib().moao_ctx_set_mixed(self._h, bf16_slices, corr_slices, ozaki_slices,
+                                       max_refine, tol, int(final_residual)),
               "moao_ctx_set_mixed")
 
     def set_kernel_timing(self, enable: bool):

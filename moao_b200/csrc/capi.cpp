@@ -64,8 +64,36 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometr
   // One host staging block, one copy.
   const size_t nu = (size_t)nL * Nx;
   const size_t nngs = (size_t)(nW - t.sys.nLgs);
-  const size_t nlay = 3 * (size_t)nL + (size_t)nW * nL;
+  const size_t nlay = 3 * (size_t)nL + (size_t)nW * nL + nL;
+  // per-WFS projection parameters and the subaperture grid of WFS 0
+  const double rad = 3.14159265358979323846 / 180.;
+  for (int w = 0; w < nW; ++w) {
+    g.gsAlt[w] = t.sys.gsAlt[w];
+    g.G[w] = t.diamPup[w] / (double)t.Nssp[w];
+    g.cth[w] = std::cos(t.sys.thetaML[w] * rad);
+    g.sth[w] = std::sin(t.sys.thetaML[w] * rad);
+    g.XPup[w] = t.sys.XPup[w];
+    g.YPup[w] = t.sys.YPup[w];
+    g.alphaX[w] = t.alphaX[w];
+    g.alphaY[w] = t.alphaY[w];
+  }
+  g.nssp_grid = (int)t.Nssp[0];
+  g.pitch = t.sys.diam / (1. * t.Nssp[0]);
+  const int ngrid = (int)t.Nsubap[0];
+  std::vector<int> cr(2 * (size_t)ngrid);
+  const double bornemin = -t.sys.diam / 2.;
+  for (int i = 0; i < ngrid; ++i) {
+    cr[2 * i] = (int)std::lround((t.X[i] - bornemin) / g.pitch - 0.5);
+    cr[2 * i + 1] = (int)std::lround((t.Y[i] - bornemin) / g.pitch - 0.5);
+  }
+  int npairs = 0;
+  const long ntab = toeplitz_table_doubles(g, &npairs);
+  const size_t tab_doubles = npairs ? (size_t)ntab + (size_t)npairs /* pair list */ + 4 : 0;
+  const size_t grid_doubles = ((size_t)ngrid * 2 * sizeof(int) + 7) / 8;
   const size_t total = 2 * nu + 2 * Nx + 3 * (size_t)Nx + nngs + nlay;
+  // table base rounded up to 32 doubles (256 bytes): the gather reads double4
+  const size_t tab_off = (total + grid_doubles + 31) / 32 * 32;
+  const size_t total_all = tab_off + tab_doubles;
   std::vector<double> h(total);
   size_t p = 0;
   auto put = [&](const double* src, size_t n) {
@@ -89,16 +117,25 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometr
     h[olay + 2 * nL + l] = t.atm.cn2[l];
   }
   for (int k = 0; k < nW * nL; ++k) h[olay + 3 * nL + k] = t.sspSizeL[k];
-  MOAO_TRY(e.buf.ensure(total * sizeof(double)));
+  for (int l = 0; l < nL; ++l) h[olay + 3 * nL + nW * nL + l] = t.atm.h[l];
+  MOAO_TRY(e.buf.ensure(total_all * sizeof(double)));
   double* d = e.buf.as<double>();
   MOAO_CUDA_TRY(cudaMemcpyAsync(d, h.data(), total * sizeof(double), cudaMemcpyHostToDevice,
                                 ctx->stream));
+  g.grid_cr = reinterpret_cast<int*>(d + total);
+  MOAO_CUDA_TRY(cudaMemcpyAsync(g.grid_cr, cr.data(), cr.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  g.ttab = npairs ? d + tab_off : nullptr;
   // h is pageable, so the copy has completed on return from the call above
   // only for small sizes; synchronise before h goes out of scope.
   MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   g.u = d + ou; g.v = d + ov; g.X = d + oX; g.Y = d + oY;
   g.noiseLGSxx = d + oxx; g.noiseLGSyy = d + oyy; g.noiseLGSxy = d + oxy;
   g.noiseNGS = d + ongs; g.layer = d + olay;
+  {
+    KernelTimer kt(ctx, "matcov_table", (double)ntab / 4);
+    MOAO_TRY(build_toeplitz_tables(g, ctx->stream, &ctx->launches));
+  }
   e.g = g;
   e.version = t.version;
   *out = &e.g;
@@ -367,11 +404,16 @@ moao_status moao_ctx_reset_kernel_stats(moao_ctx* c) {
   return MOAO_OK;
 }
 
-moao_status moao_ctx_set_mixed(moao_ctx* c, int ozaki_slices, int max_refine, double tol,
-                               int final_residual) {
-  if (!c || ozaki_slices < 2 || ozaki_slices > 6 || max_refine < 0 || max_refine > 8 || tol < 0)
-    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_mixed: slices in [2, 6], max_refine in [0, 8]");
+moao_status moao_ctx_set_mixed(moao_ctx* c, int bf16_slices, int corr_slices, int ozaki_slices,
+                               int max_refine, double tol, int final_residual) {
+  if (!c || bf16_slices < 2 || bf16_slices > 3 || corr_slices < 2 || corr_slices > bf16_slices ||
+      ozaki_slices < 2 || ozaki_slices > 6 || max_refine < 0 || max_refine > 8 || tol < 0)
+    return set_error(MOAO_ERR_BAD_ARG,
+                     "ctx_set_mixed: bf16 slices in [2, 3], correction slices in [2, bf16 slices], "
+                     "int8 slices in [2, 6], max_refine in [0, 8]");
   std::lock_guard<std::mutex> lk(c->mu);
+  c->bf16_slices = bf16_slices;
+  c->corr_slices = corr_slices;
   c->ozaki_slices = ozaki_slices;
   c->max_refine = max_refine;
   c->refine_tol = tol;

@@ -56,6 +56,8 @@ struct moao_ctx {
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
   long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
+  int bf16_slices = 3;       // bf16 slices of the factor (3: ~24 bits, 6 products)
+  int corr_slices = 2;       // bf16 slices of the factor in the correction solves
   int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
   int max_refine = 2;        // refinement corrections per target
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this

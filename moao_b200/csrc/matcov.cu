@@ -20,6 +20,7 @@
 // per DPHI), not by HBM: each 8-byte store costs ~10^3 FP64 operations.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -146,7 +147,19 @@ __global__ void __launch_bounds__(kTileI* kTileJ)
 
   const int pi = g.off[m] + i, pj = g.off[n] + j;
   double cxx = 0, cxy = 0, cyx = 0, cyy = 0;
-  for (int l = 0; l < nL; ++l) {
+  const int tab = g.ttab ? g.tpair[m][n] : -1;
+  if (tab >= 0) {
+    const int N = g.nssp_grid, W = 2 * N - 1;
+    const int2 a = reinterpret_cast<const int2*>(g.grid_cr)[i];
+    const int2 b = reinterpret_cast<const int2*>(g.grid_cr)[j];
+    const long off = ((long)tab * W * W + (long)(a.y - b.y + N - 1) * W + (a.x - b.x + N - 1)) * 4;
+    const double4 t4 = *reinterpret_cast<const double4*>(g.ttab + off);
+    cxx = t4.x;
+    cxy = t4.y;
+    cyx = t4.z;
+    cyy = t4.w;
+  }
+  for (int l = 0; l < nL && tab < 0; ++l) {
     const double sml = s_sm[l], snl = s_sn[l];
     if (!(sml > 0 && snl > 0)) continue;
     const double* ul = g.u + (size_t)l * g.Nx;
@@ -274,6 +287,59 @@ __global__ void __launch_bounds__(kTileI* kTileJ)
   if (mask & 8u) store(Nt + i, Nt + j, cyy);
 }
 
+// Offset tables of the equal-projection WFS pairs. Two WFS with the same guide
+// star altitude, grid, magnification and rotation see every layer through the
+// same affine map up to a constant shift, so the separation of subapertures i
+// and j depends only on their grid offset (dc, dr):
+//   du = G rr (dx cos - dy sin) + rr (XPup_m - XPup_n) + (alphaX_m - alphaX_n) h
+//   dv = G rr (dx sin + dy cos) + rr (YPup_m - YPup_n) + (alphaY_m - alphaY_n) h
+// with dx = dc pitch, dy = dr pitch and rr = 1 - h gsAlt. One thread per
+// (pair, offset) evaluates the 2x2 slope block over all layers; the matrix
+// kernel then gathers from the table. The separation is formed from the grid
+// offset instead of from two projected positions, which changes it by rounding
+// only (a few ulp of a position).
+__global__ void toeplitz_table_kernel(const DevGeometry g, const int2* __restrict__ pairs,
+                                      int npairs, double* __restrict__ out) {
+  const int N = g.nssp_grid, W = 2 * N - 1;
+  const long total = (long)npairs * W * W;
+  const int nL = g.nLayer;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const int pidx = (int)(e / ((long)W * W));
+    const int off = (int)(e % ((long)W * W));
+    const int dr = off / W - (N - 1), dc = off % W - (N - 1);
+    const int m = pairs[pidx].x, n = pairs[pidx].y;
+    const double dx = dc * g.pitch, dy = dr * g.pitch;
+    const double sspm = g.diam / g.Nssp[m], sspn = g.diam / g.Nssp[n];
+    const double kk = kLambda2 / (sspm * sspn);
+    const double bx = g.G[m] * (dx * g.cth[m] - dy * g.sth[m]);
+    const double by = g.G[m] * (dx * g.sth[m] + dy * g.cth[m]);
+    double cxx = 0, cxy = 0, cyx = 0, cyy = 0;
+    for (int l = 0; l < nL; ++l) {
+      const double sml = g.layer[3 * nL + m * nL + l];
+      if (!(sml > 0)) continue;
+      const double h = g.layer[3 * nL + g.nW * nL + l];
+      const double rr = 1. - h * g.gsAlt[m];
+      const double du = (bx + (g.XPup[m] - g.XPup[n])) * rr + (g.alphaX[m] - g.alphaX[n]) * h;
+      const double dv = (by + (g.YPup[m] - g.YPup[n])) * rr + (g.alphaY[m] - g.alphaY[n]) * h;
+      const double s = sml * 0.5, ad = s + s, tpl = g.layer[l];
+      const double w = 0.5 * kk * g.layer[2 * nL + l] * g.layer[nL + l];
+      const double d0 = D(du, dv, tpl);
+      cxx += (-d0 + D(du + ad, dv, tpl) + D(du - ad, dv, tpl) - d0) * w;
+      cyy += (-d0 + D(du, dv + ad, tpl) + D(du, dv - ad, tpl) - d0) * w;
+      const double pp = D(du + s, dv + s, tpl), pm = D(du + s, dv - s, tpl);
+      const double mp = D(du - s, dv + s, tpl), mm = D(du - s, dv - s, tpl);
+      cxy += (-pm + pp + mm - mp) * w;
+      cyx += (-mp + pp + mm - pm) * w;
+    }
+    double* o = out + 4 * e;
+    o[0] = cxx;
+    o[1] = cxy;
+    o[2] = cyx;
+    o[3] = cyy;
+  }
+}
+
 // Bounding subaperture range [lo, hi) of a WFS whose x slopes start at global
 // index base and y slopes at base + N, intersected with the window [w0, w1).
 void subap_range(int base, int N, int w0, int w1, int* lo, int* hi) {
@@ -369,7 +435,54 @@ moao_status launch_impl(const DevGeometry& g, OutT* data, int nrows, int ncols, 
   return MOAO_OK;
 }
 
+// Ordered WFS pairs that get an offset table: Cmm pairs (m >= n) and the truth
+// sensor against each WFS, in both orders, when their projections match.
+void table_pairs(const DevGeometry& g, int2* pairs, int* npairs) {
+  *npairs = 0;
+  const int ts = g.nW - 1;
+  auto same = [&](int m, int n) {
+    return g.gsAlt[m] == g.gsAlt[n] && g.G[m] == g.G[n] && g.cth[m] == g.cth[n] &&
+           g.sth[m] == g.sth[n] && g.Nssp[m] == g.nssp_grid && g.Nssp[n] == g.nssp_grid &&
+           g.Nsubap[m] == g.Nsubap[0] && g.Nsubap[n] == g.Nsubap[0];
+  };
+  for (int m = 0; m < g.nW; ++m)
+    for (int n = 0; n < g.nW; ++n) {
+      const bool needed = (m < ts && n < ts && m >= n) || (m == ts && n < ts) || (n == ts && m < ts);
+      if (needed && same(m, n)) pairs[(*npairs)++] = make_int2(m, n);
+    }
+}
+
 }  // namespace
+
+long toeplitz_table_doubles(const DevGeometry& g, int* npairs) {
+  int2 pairs[kMaxWfs * kMaxWfs];
+  table_pairs(g, pairs, npairs);
+  const long W = 2L * g.nssp_grid - 1;
+  return (long)*npairs * W * W * 4;
+}
+
+moao_status build_toeplitz_tables(DevGeometry& g, cudaStream_t s, long long* launches) {
+  int2 pairs[kMaxWfs * kMaxWfs];
+  int np = 0;
+  table_pairs(g, pairs, &np);
+  for (int m = 0; m < kMaxWfs; ++m)
+    for (int n = 0; n < kMaxWfs; ++n) g.tpair[m][n] = -1;
+  if (np == 0 || !g.ttab) {
+    g.ttab = nullptr;
+    return MOAO_OK;
+  }
+  for (int k = 0; k < np; ++k) g.tpair[pairs[k].x][pairs[k].y] = k;
+  // the pair list travels in the table's tail (4 doubles per offset before it)
+  const long W = 2L * g.nssp_grid - 1;
+  int2* d_pairs = reinterpret_cast<int2*>(g.ttab + (long)np * W * W * 4);
+  MOAO_CUDA_TRY(cudaMemcpyAsync(d_pairs, pairs, np * sizeof(int2), cudaMemcpyHostToDevice, s));
+  const long total = (long)np * W * W;
+  const unsigned blocks = (unsigned)std::min<long>((total + 127) / 128, 148L * 64);
+  toeplitz_table_kernel<<<blocks, 128, 0, s>>>(g, d_pairs, np, g.ttab);
+  if (launches) ++*launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
 
 moao_status launch_matcov(const DevGeometry& g, double* data, int nrows, int ncols,
                           int xoffset, int yoffset, int lda, int type_mat, cudaStream_t s,

@@ -4,17 +4,20 @@
 //   A32 = float(Cmm) holds the trailing matrix.
 //   diagonal block: FP64 Cholesky + inverse (potrf_inv_block), kept in dinv
 //   panel: L_panel = double(A32 panel) * Dinv^T in FP64, stored FP32 in A32 and
-//          as bf16 hi/lo in two layouts: Lr (row-major, row r = L(r, :)) and
-//          Lc (row j = L(:, j)), both K-major operands of the tensor-core GEMM
-//   trailing: A32_22 -= L L^T on the lower tiles as hi*hi + hi*lo + lo*hi
-//          bf16 products accumulated in FP32 in TMEM (tc_gemm, three segments)
+//          as bf16 slices (3 by default: ~24 significant bits) in two layouts:
+//          Lr (row-major, row r = L(r, :)) and Lc (row j = L(:, j)), both K-major
+//          operands of the tensor-core GEMM
+//   trailing: A32_22 -= L L^T on the lower tiles as the slice products s_i s_j
+//          with i + j < slices (6 products for 3 slices, 3 for 2) accumulated in
+//          FP32 in TMEM (tc_gemm, one segment per product)
 // Solve (R = Ctm L^-T L^-1, right-looking forward then backward): block
 //   products with Dinv in FP64, long updates with the bf16 split factor on the
 //   tensor cores, state in FP32.
 // Refinement: E = Ctm - R sym(Cmm) with the int8 slice products of the Ozaki
 //   scheme (exact int32 accumulation, per-diagonal power-of-two scaling into
-//   FP64), dR = E (L L^T)^-1 by the same mixed solve, R += dR; repeated while
-//   ||E||/||Ctm|| is above the tolerance (at most max_refine times).
+//   FP64), dR = E (L L^T)^-1 by the mixed solve with 2 slices (a correction
+//   needs ~1e-2 relative accuracy only), R += dR; repeated while ||E||/||Ctm|| is
+//   above the tolerance (at most max_refine times).
 // Cmm is read through its lower triangle and overwritten with the (FP32)
 // factor at the end, Ctm with R in FP64, like the FP64 path.
 #include <cuda_runtime.h>
@@ -56,29 +59,46 @@ moao_status sumsq(moao_ctx* ctx, const double* A, long lda, long m, long n, doub
 }
 
 struct Maps {
-  TcTensor lr_hi, lr_lo, lc_hi, lc_lo, x_hi, x_lo;
+  TcTensor lrA[kMaxBfSlices];  // Lr slices as A operands (128-row boxes)
+  TcTensor lrB[kMaxBfSlices];  // Lr slices as B operands (256-row boxes)
+  TcTensor lcB[kMaxBfSlices];  // Lc slices as B operands
+  TcTensor xA[kMaxBfSlices];   // solve-panel slices as A operands
 };
 
-// Tensor-core update C(f32, m x n, ldc) -= Xs * Ls^T over K = [0, nk*64) of the
-// X slices and [kb0, ...) of the L slices (rows b_row0..).
-moao_status tc_update(moao_ctx* ctx, const TcTensor* a_hi, const TcTensor* a_lo, int a_row0,
-                      int ka, const TcTensor* b_hi, const TcTensor* b_lo, int b_row0, int kb,
-                      int nk, long M, long N, float* C, long ldc, bool lower, int* err,
-                      double flops) {
+// Products s_i * s_j of bf16 slices kept for a given slice count, smallest
+// first: the tensor core's FP32 accumulation truncates each addition (a bias of
+// ~2^-28 of the running sum per term, measured), so the small correction
+// products are summed before the dominant hi*hi product grows the accumulator.
+struct Products {
+  int n;
+  int a[6], b[6];
+};
+Products products_for(int slices) {
+  if (slices >= 3) return Products{6, {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}};
+  return Products{3, {1, 0, 0}, {0, 1, 0}};
+}
+
+// Tensor-core update C(f32, M x N, ldc) -= sum_p A_{a_p} B_{b_p}^T over K blocks
+// [ka, ka + nk*64) of the A slices and [kb, ...) of the B slices.
+moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, const TcTensor* B,
+                      int b_row0, int kb, int nk, const Products& pr, long M, long N, float* C,
+                      long ldc, bool lower, int* err, double flops) {
   TcGemm g;
   g.kind = kTcBf16;
   g.epi = kTcEpiF32;
   g.M = M;
   g.N = N;
-  g.A[0] = a_hi;
-  g.A[1] = a_lo;
-  g.nA = 2;
-  g.B[0] = b_hi;
-  g.B[1] = b_lo;
-  g.nB = 2;
-  const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
-  for (int s = 0; s < 3; ++s) g.seg[s] = TcSegment{pa[s], pb[s], ka, kb, nk, 0};
-  g.nseg = 3;
+  int na = 0, nbm = 0;
+  for (int p = 0; p < pr.n; ++p) {
+    na = std::max(na, pr.a[p] + 1);
+    nbm = std::max(nbm, pr.b[p] + 1);
+  }
+  for (int i = 0; i < na; ++i) g.A[i] = &A[i];
+  for (int i = 0; i < nbm; ++i) g.B[i] = &B[i];
+  g.nA = na;
+  g.nB = nbm;
+  for (int p = 0; p < pr.n; ++p) g.seg[p] = TcSegment{pr.a[p], pr.b[p], ka, kb, nk, 0};
+  g.nseg = pr.n;
   g.a_row0 = a_row0;
   g.b_row0 = b_row0;
   g.lower = lower ? 1 : 0;
@@ -87,15 +107,19 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* a_hi, const TcTensor* a_lo,
   g.C = C;
   g.ldc = ldc;
   g.err = err;
-  KernelTimer kt(ctx, "tc_bf16x3", flops);
+  KernelTimer kt(ctx, "tc_bf16", flops * pr.n);
   return tc_gemm(g, ctx->stream, &ctx->launches);
 }
 
-// In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1.
+// In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1, with the long
+// updates as the given slice products.
 moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double* dinv, Maps& mp,
-                        double* W1, double* W2, void* x_hi, void* x_lo, long ldx, int* err) {
+                        double* W1, double* W2, void* const* xs, long ldx, const Products& pr,
+                        int slices, int* err) {
   const long nb = ctx->nb;
   cudaStream_t s = ctx->stream;
+  BfSlices xr{}, none{};
+  for (int k = 0; k < slices; ++k) xr.p[k] = xs[k];
   for (long k0 = 0; k0 < n; k0 += nb) {
     const long kb = std::min(nb, n - k0);
     MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
@@ -103,10 +127,9 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
     const long rest = n - k0 - kb;
     if (rest > 0) {
-      MOAO_TRY(split_bf16(W2, m, m, kb, x_hi, x_lo, ldx, nullptr, nullptr, 0, s));
-      MOAO_TRY(tc_update(ctx, &mp.x_hi, &mp.x_lo, 0, 0, &mp.lr_hi, &mp.lr_lo, (int)(k0 + kb),
-                         (int)k0, (int)((kb + 63) / 64), m, rest, T32 + (k0 + kb) * m, m, false,
-                         err, 3.0 * 2.0 * m * rest * kb));
+      MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
+      MOAO_TRY(tc_update(ctx, mp.xA, 0, 0, mp.lrB, (int)(k0 + kb), (int)k0, (int)((kb + 63) / 64),
+                         pr, m, rest, T32 + (k0 + kb) * m, m, false, err, 2.0 * m * rest * kb));
     }
   }
   const long nblk = (n + nb - 1) / nb;
@@ -116,10 +139,9 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
     MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
     if (k0 > 0) {
-      MOAO_TRY(split_bf16(W2, m, m, kb, x_hi, x_lo, ldx, nullptr, nullptr, 0, s));
-      MOAO_TRY(tc_update(ctx, &mp.x_hi, &mp.x_lo, 0, 0, &mp.lc_hi, &mp.lc_lo, 0, (int)k0,
-                         (int)((kb + 63) / 64), m, k0, T32, m, false, err,
-                         3.0 * 2.0 * m * k0 * kb));
+      MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
+      MOAO_TRY(tc_update(ctx, mp.xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
+                         T32, m, false, err, 2.0 * m * k0 * kb));
     }
   }
   return MOAO_OK;
@@ -137,13 +159,14 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   const long ldx = nb;
   // ---- workspace
   MOAO_TRY(ctx->mx_a32.ensure(sizeof(float) * (size_t)n * n));
-  MOAO_TRY(ctx->mx_lr.ensure(2 * sizeof(uint16_t) * (size_t)n * ldn));
-  MOAO_TRY(ctx->mx_lc.ensure(2 * sizeof(uint16_t) * (size_t)n * ldn));
+  const int nsl = std::max(2, std::min(kMaxBfSlices, ctx->bf16_slices));
+  MOAO_TRY(ctx->mx_lr.ensure(nsl * sizeof(uint16_t) * (size_t)n * ldn));
+  MOAO_TRY(ctx->mx_lc.ensure(nsl * sizeof(uint16_t) * (size_t)n * ldn));
   MOAO_TRY(ctx->mx_t32.ensure(sizeof(float) * (size_t)m * n));
   const size_t wbytes = sizeof(double) * (size_t)std::max(n, m) * nb;
   MOAO_TRY(ctx->mx_w1.ensure(wbytes));
   MOAO_TRY(ctx->mx_w2.ensure(wbytes));
-  MOAO_TRY(ctx->mx_x.ensure(2 * sizeof(uint16_t) * (size_t)std::max(n, m) * ldx));
+  MOAO_TRY(ctx->mx_x.ensure(nsl * sizeof(uint16_t) * (size_t)std::max(n, m) * ldx));
   MOAO_TRY(ctx->mx_r64.ensure(sizeof(double) * (size_t)m * n));
   MOAO_TRY(ctx->mx_e64.ensure(sizeof(double) * (size_t)m * n));
   MOAO_TRY(ctx->mx_qa.ensure((size_t)ns * m * ldq));
@@ -158,10 +181,9 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   float* A32 = ctx->mx_a32.as<float>();
   uint16_t* lr = ctx->mx_lr.as<uint16_t>();
   uint16_t* lc = ctx->mx_lc.as<uint16_t>();
-  uint16_t* lr_lo = lr + (size_t)n * ldn;
-  uint16_t* lc_lo = lc + (size_t)n * ldn;
-  uint16_t* xh = ctx->mx_x.as<uint16_t>();
-  uint16_t* xl = xh + (size_t)std::max(n, m) * ldx;
+  void* xs[kMaxBfSlices] = {};
+  for (int k = 0; k < nsl; ++k)
+    xs[k] = ctx->mx_x.as<uint16_t>() + (size_t)k * std::max(n, m) * ldx;
   float* T32 = ctx->mx_t32.as<float>();
   double* W1 = ctx->mx_w1.as<double>();
   double* W2 = ctx->mx_w2.as<double>();
@@ -176,12 +198,16 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   int* err = d_info + 1;
 
   Maps mp;
-  MOAO_TRY(make_tc_map(&mp.lr_hi, lr, kTcBf16, n, n, ldn));
-  MOAO_TRY(make_tc_map(&mp.lr_lo, lr_lo, kTcBf16, n, n, ldn));
-  MOAO_TRY(make_tc_map(&mp.lc_hi, lc, kTcBf16, n, n, ldn));
-  MOAO_TRY(make_tc_map(&mp.lc_lo, lc_lo, kTcBf16, n, n, ldn));
-  MOAO_TRY(make_tc_map(&mp.x_hi, xh, kTcBf16, m, nb, ldx));
-  MOAO_TRY(make_tc_map(&mp.x_lo, xl, kTcBf16, m, nb, ldx));
+  for (int k = 0; k < nsl; ++k) {
+    uint16_t* lrk = lr + (size_t)k * n * ldn;
+    uint16_t* lck = lc + (size_t)k * n * ldn;
+    MOAO_TRY(make_tc_map(&mp.lrA[k], lrk, kTcBf16, n, n, ldn));
+    MOAO_TRY(make_tc_map(&mp.lrB[k], lrk, kTcBf16, n, n, ldn, 256));
+    MOAO_TRY(make_tc_map(&mp.lcB[k], lck, kTcBf16, n, n, ldn, 256));
+    MOAO_TRY(make_tc_map(&mp.xA[k], xs[k], kTcBf16, m, nb, ldx));
+  }
+  const int csl = std::max(2, std::min(nsl, ctx->corr_slices));
+  const Products full = products_for(nsl), corr = products_for(csl);
 
   cudaEvent_t* ev = ctx->ev;
   cudaEventRecord(ev[3], s);
@@ -200,13 +226,15 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       MOAO_TRY(cvt_f32_to_f64(P, n, W1, rest, rest, kb, false, s));
       MOAO_TRY(gemm(ctx, rest, kb, kb, 1.0, W1, rest, dinv + k0, n, true, 0.0, W2, rest));
       MOAO_TRY(cvt_f64_to_f32(W2, rest, P, n, rest, kb, false, s));
-      MOAO_TRY(split_bf16(W2, rest, rest, kb, lr + (k0 + kb) * ldn + k0,
-                          lr_lo + (k0 + kb) * ldn + k0, ldn, lc + k0 * ldn + (k0 + kb),
-                          lc_lo + k0 * ldn + (k0 + kb), ldn, s));
-      MOAO_TRY(tc_update(ctx, &mp.lr_hi, &mp.lr_lo, (int)(k0 + kb), (int)k0, &mp.lr_hi,
-                         &mp.lr_lo, (int)(k0 + kb), (int)k0, (int)(kb / 64), rest, rest,
-                         A32 + (k0 + kb) + (k0 + kb) * n, n, true, err,
-                         3.0 * (double)rest * rest * kb));
+      BfSlices rr{}, cc{};
+      for (int k = 0; k < nsl; ++k) {
+        rr.p[k] = lr + (size_t)k * n * ldn + (k0 + kb) * ldn + k0;
+        cc.p[k] = lc + (size_t)k * n * ldn + k0 * ldn + (k0 + kb);
+      }
+      MOAO_TRY(split_bf16(W2, rest, rest, kb, nsl, rr, ldn, cc, ldn, s));
+      MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k0 + kb), (int)k0, mp.lrB, (int)(k0 + kb), (int)k0,
+                         (int)(kb / 64), full, rest, rest, A32 + (k0 + kb) + (k0 + kb) * n, n,
+                         true, err, (double)rest * rest * kb));
     }
     int info[2] = {0, 0};
     MOAO_CUDA_TRY(cudaMemcpyAsync(info, d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -226,14 +254,14 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   cudaEventRecord(ev[4], s);
   // ---- solve
   MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
-  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xh, xl, ldx, err));
+  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xs, ldx, full, nsl, err));
   MOAO_TRY(cvt_f32_to_f64(T32, m, R64, m, m, n, false, s));
   cudaEventRecord(ev[5], s);
   // ---- refinement
   TcTensor ta[kMaxOzakiSlices], tb[kMaxOzakiSlices];
   for (int i = 0; i < ns; ++i) {
     MOAO_TRY(make_tc_map(&ta[i], qa + (size_t)i * m * ldq, kTcI8, m, n, ldq));
-    MOAO_TRY(make_tc_map(&tb[i], qb + (size_t)i * n * ldq, kTcI8, n, n, ldq));
+    MOAO_TRY(make_tc_map(&tb[i], qb + (size_t)i * n * ldq, kTcI8, n, n, ldq, 256));
   }
   double* dnorm = ctx->mx_norm.as<double>();
   double ctm2 = 0, e2 = 0;
@@ -283,7 +311,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(residual());
     if (rep->refine_resid <= ctx->refine_tol) break;
     MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
-    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xh, xl, ldx, err));
+    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xs, ldx, corr, csl, err));
     MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
   }
   if (ctx->final_residual) MOAO_TRY(residual());

@@ -57,36 +57,32 @@ __global__ void add_f32_to_f64_kernel(const float* __restrict__ s, long lds, dou
   }
 }
 
-// 32x32 tiles, 32x8 threads.
+// 32x32 tiles, 32x8 threads. Slice k = bf16(x - sum of the previous slices),
+// computed in FP64: two slices carry ~16 significant bits, three ~24.
 __global__ void split_bf16_kernel(const double* __restrict__ src, long lds, long m, long n,
-                                  __nv_bfloat16* hr, __nv_bfloat16* lr, long ldr,
-                                  __nv_bfloat16* hc, __nv_bfloat16* lc, long ldc) {
-  __shared__ __nv_bfloat16 sh[32][34], sl[32][34];
+                                  int ns, BfSlices rmaj, long ldr, BfSlices cmaj, long ldc) {
+  __shared__ __nv_bfloat16 t[kMaxBfSlices][32][34];
   const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int jj = ty; jj < 32; jj += 8) {
     const long r = r0 + tx, c = c0 + jj;
-    __nv_bfloat16 h = __float2bfloat16(0.f), l = h;
-    if (r < m && c < n) {
-      const double x = src[c * lds + r];
-      h = __double2bfloat16(x);
-      l = __double2bfloat16(x - (double)__bfloat162float(h));
-      if (hc) {
-        hc[c * ldc + r] = h;
-        lc[c * ldc + r] = l;
-      }
+    double rem = 0;
+    if (r < m && c < n) rem = src[c * lds + r];
+    for (int k = 0; k < ns; ++k) {
+      const __nv_bfloat16 h = __double2bfloat16(rem);
+      rem -= (double)__bfloat162float(h);
+      t[k][tx][jj] = h;
+      if (cmaj.p[0] && r < m && c < n)
+        static_cast<__nv_bfloat16*>(cmaj.p[k])[c * ldc + r] = h;
     }
-    sh[tx][jj] = h;
-    sl[tx][jj] = l;
   }
-  if (!hr) return;
+  if (!rmaj.p[0]) return;
   __syncthreads();
   for (int ii = ty; ii < 32; ii += 8) {
     const long r = r0 + ii, c = c0 + tx;
-    if (r < m && c < n) {
-      hr[r * ldr + c] = sh[ii][tx];
-      lr[r * ldr + c] = sl[ii][tx];
-    }
+    if (r < m && c < n)
+      for (int k = 0; k < ns; ++k)
+        static_cast<__nv_bfloat16*>(rmaj.p[k])[r * ldr + c] = t[k][ii][tx];
   }
 }
 
@@ -234,13 +230,12 @@ moao_status add_f32_to_f64(const float* s, long lds, double* d, long ldd, long m
   return MOAO_OK;
 }
 
-moao_status split_bf16(const double* src, long lds, long m, long n, void* hi_r, void* lo_r,
-                       long ldr, void* hi_c, void* lo_c, long ldc, cudaStream_t st) {
+moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                       long ldr, BfSlices cmaj, long ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
+  if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_bf16: slices");
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
-  split_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(
-      src, lds, m, n, (__nv_bfloat16*)hi_r, (__nv_bfloat16*)lo_r, ldr, (__nv_bfloat16*)hi_c,
-      (__nv_bfloat16*)lo_c, ldc);
+  split_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(src, lds, m, n, ns, rmaj, ldr, cmaj, ldc);
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }

@@ -50,9 +50,28 @@ struct DevGeometry {
   double* noiseLGSxy = nullptr;
   double* noiseNGS = nullptr;    // [nW - nLgs]
   // per-layer tables: [0,nL) 2*pi/L0, [nL,2nL) k1*L0^(5/3), [2nL,3nL) cn2,
-  // then sspSizeL [nW*nL]
+  // [3nL, 3nL + nW*nL) sspSizeL, then h [nL]
   double* layer = nullptr;
+
+  // Projection of each WFS onto a layer at altitude h (projectedSubap):
+  //   u = (G (X cos - Y sin) + XPup) (1 - h gsAlt) + alphaX h
+  //   v = (G (X sin + Y cos) + YPup) (1 - h gsAlt) + alphaY h
+  double gsAlt[kMaxWfs], G[kMaxWfs], cth[kMaxWfs], sth[kMaxWfs];
+  double XPup[kMaxWfs], YPup[kMaxWfs], alphaX[kMaxWfs], alphaY[kMaxWfs];
+  // Subaperture grid: pitch and the (column, row) of every valid subaperture
+  // of a WFS (all WFS share one grid when their Nssp are equal).
+  double pitch = 0;
+  int nssp_grid = 0;
+  int* grid_cr = nullptr;    // [2 * Nsubap of WFS 0]: column, row
+  // Offset tables of the equal-projection WFS pairs (see matcov.cu), or null.
+  double* ttab = nullptr;
+  int tpair[kMaxWfs][kMaxWfs];  // table index of the pair (m, n), or -1
 };
+
+// Builds the offset tables of g's equal-projection WFS pairs into g.ttab (device
+// memory provided by the caller, toeplitz_table_doubles(g) doubles).
+long toeplitz_table_doubles(const DevGeometry& g, int* npairs);
+moao_status build_toeplitz_tables(DevGeometry& g, cudaStream_t s, long long* launches);
 
 // Matcov launch (device pointers). type_mat: 1 Cmm lower, 3 Ctm, 4 Ctt,
 // 5 Cmm full symmetric. The tile covers rows [xoffset, xoffset+nrows) and

@@ -33,13 +33,16 @@
 namespace moao {
 namespace {
 
-constexpr int TBM = 128, TBN = 128;
+constexpr int TBM = 128, TBN = 256;
 constexpr int KBYTES = 128;             // bytes of K per stage row (one 128B swizzle atom)
-constexpr int STAGES = 3;
+constexpr int STAGES = 4;
 constexpr int A_TILE = TBM * KBYTES;    // 16 KB
-constexpr int B_TILE = TBN * KBYTES;    // 16 KB
+constexpr int B_TILE = TBN * KBYTES;    // 32 KB
 constexpr int STAGE_BYTES = A_TILE + B_TILE;
-constexpr int THREADS = 256;
+constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quadrant
+constexpr int THREADS = (4 + EPI_WARPS) * 32;
+constexpr int ACC_COLS = TBN;           // fp32 / int32 columns of one accumulator
+constexpr int TMEM_COLS = 2 * ACC_COLS; // double-buffered accumulator
 constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr unsigned long long kSpinLimit = 1ull << 28;
 
@@ -60,7 +63,8 @@ struct __align__(64) TcParams {
   const int* erow;         // INT8: per-row exponent of A (length M, indexed by r)
   const int* ecol;         // INT8: per-column exponent of B (length N)
   int shift;
-  int tiles_m;
+  int tiles_m, tiles_n;
+  int total_tiles;         // tiles that intersect the written part of C
   int* err;
 };
 
@@ -78,6 +82,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -93,7 +101,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
   for (unsigned long long i = 0; i < kSpinLimit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (*(volatile int*)err) return false;  // another role already gave up
+    if ((i & 1023) == 1023 && *(volatile int*)err) return false;  // another role gave up
   }
   atomicCAS(err, 0, code);
   return false;
@@ -109,15 +117,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // Shared-memory matrix descriptor for a K-major tile written by TMA with the
-// 128-byte swizzle: 8-row core groups 1024 bytes apart (SBO), LBO unused,
-// descriptor version 1 (tcgen05), layout SWIZZLE_128B (2).
+// 128-byte swizzle: 8-row core groups 1024 bytes apart (SBO), LBO = 16 bytes
+// (unused for swizzled K-major), descriptor version 1 (tcgen05), SWIZZLE_128B.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);          // start address
-  d |= (uint64_t)(16 >> 4) << 16;                    // LBO (ignored for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;                  // SBO
-  d |= (uint64_t)1 << 46;                            // version
-  d |= (uint64_t)2 << 61;                            // SWIZZLE_128B
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)(16 >> 4) << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
   return d;
 }
 
@@ -144,7 +152,7 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
       : "memory");
 }
 
-// Instruction descriptors (M = 128, N = 128, both operands K-major).
+// Instruction descriptors (M = 128, N = 256, both operands K-major).
 //   bits 4-5 D format (1 F32, 2 S32), 7-9 A format, 10-12 B format
 //   (kind::f16: 1 BF16; kind::i8: 1 S8), 15/16 A/B major (0 = K),
 //   17-22 N >> 3, 24-28 M >> 4.
@@ -155,134 +163,215 @@ constexpr uint32_t idesc_of(int dfmt, int abfmt) {
 constexpr uint32_t kIdescBf16 = idesc_of(1, 1);
 constexpr uint32_t kIdescI8 = idesc_of(2, 1);
 
+// First row tile of column tile nt that reaches the written (lower) part.
+__device__ __forceinline__ int first_mt(const TcParams& p, int nt) {
+  if (!p.lower) return 0;
+  const int num = nt * TBN - p.diag_off - (TBM - 1);
+  return num <= 0 ? 0 : (num + TBM - 1) / TBM;
+}
+
+// v-th tile (in column-major tile order over the tiles that are written).
+__device__ __forceinline__ void decode_tile(const TcParams& p, int v, int* mt, int* nt) {
+  if (!p.lower) {
+    *mt = v % p.tiles_m;
+    *nt = v / p.tiles_m;
+    return;
+  }
+  int c = 0;
+  for (;;) {
+    const int cnt = max(0, p.tiles_m - first_mt(p, c));
+    if (v < cnt || c == p.tiles_n - 1) break;
+    v -= cnt;
+    ++c;
+  }
+  *nt = c;
+  *mt = first_mt(p, c) + v;
+}
+
+// Persistent warp-specialised kernel: warp 0 TMA producer, warp 1 MMA issuer,
+// warp 2 TMEM allocator, warps 4.. epilogue. The accumulator is double-buffered
+// in TMEM so the epilogue of one tile overlaps the main loop of the next.
 __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty_bar = full_bar + STAGES;
-  uint64_t* acc_bar = empty_bar + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+  uint64_t* tfull_bar = empty_bar + STAGES;  // [2]
+  uint64_t* tempty_bar = tfull_bar + 2;      // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mt = blockIdx.x % p.tiles_m, nt = blockIdx.x / p.tiles_m;
-  const int m0 = mt * TBM, n0 = nt * TBN;
-  if (p.lower && m0 + TBM - 1 + p.diag_off < n0) return;  // tile entirely above the diagonal
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(acc_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], EPI_WARPS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(TBN));
+                 "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // total K blocks over all segments
-  int total = 0;
-  for (int s = 0; s < p.nseg; ++s) total += p.seg[s].nk;
+  int kblocks = 0;  // K blocks per tile over all segments
+  for (int s = 0; s < p.nseg; ++s) kblocks += p.seg[s].nk;
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer
     int it = 0;
-    for (int s = 0; s < p.nseg && !*(volatile int*)p.err; ++s) {
-      const TcSegment sg = p.seg[s];
-      for (int kb = 0; kb < sg.nk; ++kb, ++it) {
-        const int st = it % STAGES;
-        const uint32_t round = it / STAGES;
-        if (it >= STAGES && !mbar_wait(&empty_bar[st], (round & 1) ^ 1, p.err, 1)) break;
-        uint8_t* sa = smem + st * STAGE_BYTES;
-        uint8_t* sb = sa + A_TILE;
-        mbar_expect_tx(&full_bar[st], STAGE_BYTES);
-        const int kxa = sg.ka + kb * sg.kstep;  // element coordinates along K
-        const int kxb = sg.kb + kb * sg.kstep;
-        tma_load_2d(sa, &p.mapA[sg.a], kxa, p.a_row0 + m0, &full_bar[st]);
-        tma_load_2d(sb, &p.mapB[sg.b], kxb, p.b_row0 + n0, &full_bar[st]);
+    bool ok = true;
+    for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x) {
+      int mt, nt;
+      decode_tile(p, v, &mt, &nt);
+      const int m0 = mt * TBM, n0 = nt * TBN;
+      for (int s = 0; s < p.nseg && ok; ++s) {
+        const TcSegment sg = p.seg[s];
+        for (int kb = 0; kb < sg.nk; ++kb, ++it) {
+          const int st = it % STAGES;
+          const uint32_t use = it / STAGES;
+          if (use > 0 && !mbar_wait(&empty_bar[st], (use - 1) & 1, p.err, 1)) {
+            ok = false;
+            break;
+          }
+          uint8_t* sa = smem + st * STAGE_BYTES;
+          uint8_t* sb = sa + A_TILE;
+          mbar_expect_tx(&full_bar[st], STAGE_BYTES);
+          tma_load_2d(sa, &p.mapA[sg.a], sg.ka + kb * sg.kstep, p.a_row0 + m0, &full_bar[st]);
+          tma_load_2d(sb, &p.mapB[sg.b], sg.kb + kb * sg.kstep, p.b_row0 + n0, &full_bar[st]);
+        }
       }
     }
-    // Never leave the CTA with a bulk copy still writing its shared memory:
-    // wait (bounded) for the last copies issued on every stage.
+    // Never leave the CTA with a bulk copy still writing its shared memory.
     for (int j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
       const int st = j % STAGES;
-      for (unsigned long long i = 0; i < kSpinLimit && !mbar_try_wait(&full_bar[st], (j / STAGES) & 1); ++i) {
+      for (unsigned long long i = 0;
+           i < kSpinLimit && !mbar_try_wait(&full_bar[st], (j / STAGES) & 1); ++i) {
       }
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     const uint32_t idesc = (p.kind == kTcBf16) ? kIdescBf16 : kIdescI8;
-    for (int it = 0; it < total; ++it) {
-      const int st = it % STAGES;
-      const uint32_t round = it / STAGES;
-      if (!mbar_wait(&full_bar[st], round & 1, p.err, 2)) break;
+    int it = 0, tc = 0;
+    bool ok = true;
+    for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x, ++tc) {
+      const int buf = tc & 1;
+      const uint32_t use = tc >> 1;
+      if (use > 0 && !mbar_wait(&tempty_bar[buf], (use - 1) & 1, p.err, 4)) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t sa = smem_u32(smem + st * STAGE_BYTES);
-      const uint32_t sb = sa + A_TILE;
-      const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
-      // 4 instructions of 32 bytes of K each (K = 16 bf16 or 32 int8)
+      const uint32_t acc = tmem + (uint32_t)(buf * ACC_COLS);
+      for (int k = 0; k < kblocks; ++k, ++it) {
+        const int st = it % STAGES;
+        if (!mbar_wait(&full_bar[st], (it / STAGES) & 1, p.err, 2)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t sa = smem_u32(smem + st * STAGE_BYTES);
+        const uint64_t da = sw128_desc(sa), db = sw128_desc(sa + A_TILE);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const uint64_t off = (uint64_t)((k * 32) >> 4);
-        if (p.kind == kTcBf16) mma_bf16(tmem, da + off, db + off, idesc, (it | k) ? 1u : 0u);
-        else mma_i8(tmem, da + off, db + off, idesc, (it | k) ? 1u : 0u);
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint64_t off = (uint64_t)((kk * 32) >> 4);
+          const uint32_t accum = (k | kk) ? 1u : 0u;
+          if (p.kind == kTcBf16) mma_bf16(acc, da + off, db + off, idesc, accum);
+          else mma_i8(acc, da + off, db + off, idesc, accum);
+        }
+        mma_commit(&empty_bar[st]);
       }
-      mma_commit(&empty_bar[st]);
+      mma_commit(&tfull_bar[buf]);
     }
-    mma_commit(acc_bar);
   } else if (warp >= 4) {
-    // ---------------- epilogue: warp q = warp - 4 owns TMEM lanes 32q..32q+31
-    const int q = warp - 4;
-    const int r = m0 + q * 32 + lane;  // row of C this thread updates
-    const bool ok = mbar_wait(acc_bar, 0, p.err, 3);
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (ok && total > 0 && !*(volatile int*)p.err) {
-      for (int c0 = 0; c0 < TBN; c0 += 32) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+    // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4).. and one
+    // half of the tile's columns
+    const int q = warp & 3;
+    const int half = (warp - 4) >> 2;
+    int tc = 0;
+    for (int v = blockIdx.x; v < p.total_tiles; v += gridDim.x, ++tc) {
+      int mt, nt;
+      decode_tile(p, v, &mt, &nt);
+      const int m0 = mt * TBM, n0 = nt * TBN;
+      const int buf = tc & 1;
+      if (!mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int r = m0 + q * 32 + lane;
+      const bool live = kblocks > 0 && !*(volatile int*)p.err;
+      for (int c0 = half * (TBN / 2); c0 < (half + 1) * (TBN / 2) && live; c0 += 32) {
+        uint32_t v32[32];
+        const uint32_t taddr =
+            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * ACC_COLS + c0);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
             "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-              "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-              "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-              "=r"(v[31])
+            : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]),
+              "=r"(v32[6]), "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]),
+              "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]), "=r"(v32[14]), "=r"(v32[15]),
+              "=r"(v32[16]), "=r"(v32[17]), "=r"(v32[18]), "=r"(v32[19]), "=r"(v32[20]),
+              "=r"(v32[21]), "=r"(v32[22]), "=r"(v32[23]), "=r"(v32[24]), "=r"(v32[25]),
+              "=r"(v32[26]), "=r"(v32[27]), "=r"(v32[28]), "=r"(v32[29]), "=r"(v32[30]),
+              "=r"(v32[31])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
         if (r < p.M) {
+          // Mask of the chunk's columns that this row writes.
+          uint32_t mask = 0;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int c = n0 + c0 + j;
-            if (c >= p.N) break;
-            if (p.lower && r + p.diag_off < c) continue;
-            if (p.epi == kTcEpiF32) {
-              float* dst = static_cast<float*>(p.C) + (size_t)c * p.ldc + r;
-              float val = p.alpha * __uint_as_float(v[j]);
-              if (p.beta != 0.f) val += p.beta * *dst;
-              *dst = val;
-            } else {
-              double* dst = static_cast<double*>(p.C) + (size_t)c * p.ldc + r;
-              const double a = (double)(int)v[j];
-              *dst += (double)p.alpha * ldexp(a, p.erow[r] + p.ecol[c] + p.shift);
+            if (c < p.N && !(p.lower && r + p.diag_off < c)) mask |= 1u << j;
+          }
+          // All loads of C first (independent, in flight together), then the
+          // stores: interleaving them would serialise each load behind the
+          // previous store, since the compiler cannot rule out aliasing.
+          if (p.epi == kTcEpiF32) {
+            float* dst = static_cast<float*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
+            float old[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              old[j] = (p.beta != 0.f && (mask >> j & 1u)) ? dst[(size_t)j * p.ldc] : 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (mask >> j & 1u)
+                dst[(size_t)j * p.ldc] = p.alpha * __uint_as_float(v32[j]) + p.beta * old[j];
+          } else {
+            double* dst = static_cast<double*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
+            const int er = p.erow[r] + p.shift;
+            double old[32];
+            int ec[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const bool w = mask >> j & 1u;
+              old[j] = w ? dst[(size_t)j * p.ldc] : 0.0;
+              ec[j] = w ? p.ecol[n0 + c0 + j] : 0;
             }
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (mask >> j & 1u)
+                dst[(size_t)j * p.ldc] =
+                    old[j] + (double)p.alpha * ldexp((double)(int)v32[j], er + ec[j]);
           }
         }
       }
+      // release this accumulator buffer to the MMA issuer
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
     }
   }
   __syncthreads();
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 2) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TBN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(TMEM_COLS));
   }
 }
 
@@ -304,6 +393,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows, long long kcols,
                         long long row_stride_elems, int box_rows) {
+  if (box_rows != TBM && box_rows != TBN)
+    return set_error(MOAO_ERR_BAD_ARG, "tc map: box rows must be 128 (A) or 256 (B)");
   auto fn = encode_fn();
   if (!fn) return set_error(MOAO_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   const int esz = (kind == kTcBf16) ? 2 : 1;
@@ -323,6 +414,7 @@ moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows,
     return set_error(MOAO_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   t->kind = kind;
   t->kstep = KBYTES / esz;
+  t->box_rows = box_rows;
   return MOAO_OK;
 }
 
@@ -338,11 +430,13 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   TcParams p;
   std::memset(&p, 0, sizeof(p));
   for (int i = 0; i < g.nA; ++i) {
-    if (g.A[i]->kind != g.kind) return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: A kind mismatch");
+    if (g.A[i]->kind != g.kind || g.A[i]->box_rows != TBM)
+      return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: A operand kind or box mismatch");
     p.mapA[i] = g.A[i]->map;
   }
   for (int i = 0; i < g.nB; ++i) {
-    if (g.B[i]->kind != g.kind) return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: B kind mismatch");
+    if (g.B[i]->kind != g.kind || g.B[i]->box_rows != TBN)
+      return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: B operand kind or box mismatch");
     p.mapB[i] = g.B[i]->map;
   }
   const int kstep = g.A[0]->kstep;
@@ -372,14 +466,32 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   p.shift = g.shift;
   p.err = g.err;
   p.tiles_m = (int)((g.M + TBM - 1) / TBM);
-  const long tiles_n = (g.N + TBN - 1) / TBN;
+  p.tiles_n = (int)((g.N + TBN - 1) / TBN);
+  long total = 0;
+  for (int nt = 0; nt < p.tiles_n; ++nt) {
+    long first = 0;
+    if (g.lower) {
+      const long num = (long)nt * TBN - g.diag_off - (TBM - 1);
+      first = num <= 0 ? 0 : (num + TBM - 1) / TBM;
+    }
+    total += std::max(0L, (long)p.tiles_m - first);
+  }
+  if (total == 0) return MOAO_OK;
+  p.total_tiles = (int)total;
+  static int num_sms = 0;
+  if (!num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (num_sms <= 0) num_sms = 148;
+  }
   static bool configured = false;
   if (!configured) {
     MOAO_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)SMEM));
     configured = true;
   }
-  tc_gemm_kernel<<<(unsigned)(p.tiles_m * tiles_n), THREADS, SMEM, s>>>(p);
+  tc_gemm_kernel<<<(unsigned)std::min<long>(total, num_sms), THREADS, SMEM, s>>>(p);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
@@ -411,7 +523,7 @@ extern "C" moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long 
     g.A[i] = &ta[i];
   }
   for (int i = 0; i < nb; ++i) {
-    MOAO_TRY(make_tc_map(&tb[i], (const char*)B + (size_t)i * N * ldb * esz, kind, N, K, ldb));
+    MOAO_TRY(make_tc_map(&tb[i], (const char*)B + (size_t)i * N * ldb * esz, kind, N, K, ldb, 256));
     g.B[i] = &tb[i];
   }
   g.nA = na;

@@ -18,7 +18,8 @@ enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1 };
 struct TcTensor {
   alignas(64) CUtensorMap map;
   int kind = 0;
-  int kstep = 0;  // K elements per pipeline stage (64 bf16, 128 int8)
+  int kstep = 0;     // K elements per pipeline stage (64 bf16, 128 int8)
+  int box_rows = 0;  // rows per TMA box: 128 for an A operand, 256 for a B operand
 };
 
 // One K segment: A tensor a over K elements [ka, ka + nk*kstep) times B tensor
@@ -50,7 +51,8 @@ struct TcGemm {
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
 };
 
-// Describes a row-major (K-contiguous) device matrix for TMA; box rows = 128.
+// Describes a row-major (K-contiguous) device matrix for TMA. The output tile is
+// 128 x 256: A operands use boxes of 128 rows, B operands boxes of 256 rows.
 moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows, long long kcols,
                         long long row_stride_elems, int box_rows = 128);
 moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches);

@@ -2,10 +2,10 @@
 
 Tolerance: relative Frobenius error of R <= 1e-5 against FP64 (the accuracy the
 mixed path is specified to), with the residual ||Ctm - R Cmm||_F / ||Ctm||_F
-reported by the library after the last refinement step. Defaults: bf16 hi/lo
-split products (about 16 significant bits) in the factorisation and the solves,
-two refinement steps, residual from 5 int8 slices per operand (measured: 3e-3
-before refinement, 1.6e-4 after one step, 8e-6 after two on the 39 m systems).
+reported by the library after the last refinement step. Defaults: three bf16
+slices of the factor (about 24 significant bits, six tensor-core products) in
+the factorisation and the first solve, one refinement step whose correction
+solve uses two slices, residual from 5 int8 slices per operand.
 """
 import numpy as np
 import pytest
@@ -36,9 +36,10 @@ def case(name):
     return nm, nts, Cmm, Ctm
 
 
-def run_mixed(ctx, nm, nts, Cmm, Ctm, nb=256, slices=5, refine=2):
+def run_mixed(ctx, nm, nts, Cmm, Ctm, nb=256, slices=5, refine=1, bf16_slices=3):
     ctx.set_block(nb)
-    ctx.set_mixed(ozaki_slices=slices, max_refine=refine, final_residual=True)
+    ctx.set_mixed(bf16_slices=bf16_slices, ozaki_slices=slices, max_refine=refine,
+                  final_residual=True)
     try:
         dC, dT = dev(Cmm), dev(Ctm)
         rep = M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=ctx)
@@ -56,7 +57,7 @@ def test_mixed_matches_fp64(ctx, name, nb):
     L, R, rep = run_mixed(ctx, nm, nts, Cmm, Ctm, nb=nb)
     err = O.rel_fro(R, R_ref)
     assert err <= 1e-5, (err, rep)
-    assert rep["refine_steps"] == 2
+    assert rep["refine_steps"] == 1
     # the factor written back carries the accuracy of the bf16 split products
     assert O.rel_fro(np.tril(L), np.tril(L_ref)) < 1e-3
     assert np.array_equal(np.triu(L, 1), np.triu(Cmm, 1))
@@ -69,9 +70,10 @@ def test_mixed_refinement_reduces_error(ctx):
     _, R2, rep2 = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=2)
     e0, e2 = O.rel_fro(R0, R_ref), O.rel_fro(R2, R_ref)
     assert e2 < e0 / 100, (e0, e2)
-    # 4 int8 slices leave the residual too coarse to converge to 1e-5
-    _, R4, _ = run_mixed(ctx, nm, nts, Cmm, Ctm, slices=4, refine=2)
-    assert O.rel_fro(R4, R_ref) > 1e-4
+    # two bf16 slices (~16 bits) need more refinement than three (~24 bits)
+    _, Rb2, _ = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=1, bf16_slices=2)
+    _, Rb3, _ = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=1, bf16_slices=3)
+    assert O.rel_fro(Rb3, R_ref) < O.rel_fro(Rb2, R_ref)
     assert rep2["refine_resid"] < rep0["refine_resid"]
 
 
@@ -82,7 +84,7 @@ def test_mixed_ill_conditioned_check_system(ctx):
     nm, nts, Cmm, Ctm = case("check2")
     _, R_ref, _ = O.reconstructor(Cmm, Ctm)
     errs = []
-    for steps in (0, 2, 4):
+    for steps in (0, 1, 3):
         _, R, rep = run_mixed(ctx, nm, nts, Cmm, Ctm, refine=steps)
         errs.append(O.rel_fro(R, R_ref))
     assert errs[1] < errs[0] and errs[2] < errs[1], errs
