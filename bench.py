@@ -42,11 +42,13 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="moao", choices=["moao", "reference"])
-    p.add_argument("--path", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--path", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--nb", type=int, default=256)
     p.add_argument("--config", default="elt", choices=["elt", "small"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-compare", action="store_true",
+                   help="mixed path: skip timing the FP64 path beside it")
     return p.parse_args()
 
 
@@ -274,59 +276,82 @@ def main():
     cn2_p = np.array(atm.cn2, dtype=np.float64)
     h_p, L0_p = np.array(atm.h, dtype=np.float64), np.array(atm.L0, dtype=np.float64)
 
-    def step():
+    if args.path == "mixed":
+        # defaults of the mixed path; the LGS constant blocks of the covariance
+        # model are declared so the factorisation works on Cmm without them
+        ctx.set_mixed()
+        ctx.set_offsets_from_tomo(t)
+
+    def step(path):
         # every build starts from the turbulence profile: projected geometry,
         # offset tables and both covariance matrices are recomputed
         t.set_profile(cn2_p, h_p, L0_p)
         M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
         M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
-        return M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=args.path, ctx=ctx)
+        return M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=path, ctx=ctx)
 
-    for _ in range(max(3, args.warmup)):
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ctx.reset_kernel_stats()
-    ctx.set_kernel_timing(True)
-    launches0 = ctx.launches
-    clocks = Clocks(dev)
-    clocks.start()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    ev[0].record()
-    reps = []
-    for k in range(args.steps):
-        reps.append(step())
-        ev[k + 1].record()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ctx.set_kernel_timing(False)
-    launches = ctx.launches - launches0
-    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if dist:
-        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    def timed(path, steps, warmup, measure):
+        """Device time of `steps` builds after `warmup` untimed ones (CUDA events
+        on the launching stream, barriers on both sides)."""
+        for _ in range(warmup):
+            step(path)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        if measure:
+            ctx.reset_kernel_stats()
+            ctx.set_kernel_timing(True)
+            clocks = Clocks(dev)
+            clocks.start()
+        launches0 = ctx.launches
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record()
+        for k in range(steps):
+            step(path)
+            ev[k + 1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        out = {"launches": ctx.launches - launches0}
+        if measure:
+            out["clocks"] = clocks.stop()
+            ctx.set_kernel_timing(False)
+        out["per_step"] = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        total = ev[0].elapsed_time(ev[-1])
+        if dist:
+            tt = torch.tensor([total], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total = float(tt.item())
+        out["total_ms"] = total
+        return out
+
+    main_run = timed(args.path, args.steps, max(3, args.warmup), True)
+    total_ms, per_step, launches, clk = (main_run["total_ms"], main_run["per_step"],
+                                         main_run["launches"], main_run["clocks"])
     value = world * args.steps / (total_ms / 1000.0)
-
     stats = {f: ctx.kernel_stats(f) for f in ("gemm_f64", "matcov", "matcov_table", "potrf_leaf",
                                               "tc_bf16", "tc_int8")}
-    # R reference error on this rank's last build (mixed path only): vs an FP64 build
-    rel_err = None
+
+    # The mixed path is reported beside the FP64 path of the same build: its
+    # builds/s in this run and the relative Frobenius error of R between them.
+    rel_err, fp64_arm = None, None
     if args.path == "mixed":
         R_mixed = Ctm.clone()
-        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
-        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
-        M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec="fp64", ctx=ctx)
-        torch.cuda.synchronize()
+        if args.no_compare:
+            step("fp64")
+            torch.cuda.synchronize()
+        else:
+            arm = timed("fp64", args.steps, 1, False)
+            v64 = world * args.steps / (arm["total_ms"] / 1000.0)
+            fp64_arm = {"value": v64, "unit": UNIT, "ms_per_step": arm["total_ms"] / args.steps,
+                        "latency_ms": {"p50": float(np.percentile(arm["per_step"], 50)),
+                                       "p99": float(np.percentile(arm["per_step"], 99))},
+                        "mixed_over_fp64": value / v64}
         rel_err = float(torch.linalg.norm(R_mixed - Ctm) / torch.linalg.norm(Ctm))
         del R_mixed
 
@@ -343,7 +368,7 @@ def main():
             dist.barrier()
         t0 = time.perf_counter()
         for k in range(args.steps):
-            step()                      # host profile -> geometry recomputed and re-uploaded
+            step(args.path)             # host profile -> geometry recomputed and re-uploaded
             R_host.copy_(Ctm, non_blocking=True)
             torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
@@ -387,7 +412,8 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
         "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.path == "fp64" else "f64 (diagonal, refinement) + tensor-core trailing updates",
+        "dtype": "f64" if args.path == "fp64" else
+                 "bf16x3 split (fp32 accumulate) tensor-core updates + f64 diagonal blocks + int8 Ozaki f64 residual",
         "data": "synthetic (seeded ELT-scale system; reference parameter-file format)",
         "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "path": args.path,
                    "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": args.nb,
@@ -395,6 +421,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "stages_ms_per_step": {f: stats[f]["ms"] / args.steps for f in stats},
         "rel_fro_err_R_vs_fp64": rel_err,
+        "fp64_path": fp64_arm,
         "roofline": roof,
         "gpu_launches": int(launches),
         "clocks": clk,

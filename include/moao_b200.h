@@ -87,6 +87,21 @@ moao_status moao_ctx_set_stream(moao_ctx* ctx, void* stream);
 moao_status moao_ctx_use_own_stream(moao_ctx* ctx);
 void* moao_ctx_stream(moao_ctx* ctx);
 moao_status moao_ctx_synchronize(moao_ctx* ctx);
+/* Block-constant offsets of Cmm known to the caller, for the mixed-precision
+ * reconstructor: value[w] is part of every entry (i, j) with begin[w] <= i, j
+ * < end[w] (0..32 non-overlapping ranges, values > 0; nranges 0 clears). The
+ * mixed path then factors Cmm minus the offsets, whose entries keep their low
+ * bits in FP32, and adds the offsets back exactly (Woodbury identity; the
+ * refinement residual still uses Cmm as given). The result does not depend on
+ * whether offsets are declared, only the refinement's convergence does. No
+ * reference counterpart. */
+moao_status moao_ctx_set_offsets(moao_ctx* ctx, int nranges, const int* begin, const int* end,
+                                 const double* value);
+/* The offsets of the covariance model itself: the LGS constant (lgsCst) on the
+ * x-x and y-y blocks of every LGS (common/kernels/matcov_kernels.cpp:311-321 of
+ * the reference adds it to each such element). */
+moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* ctx, const moao_tomo* tomo);
+
 /* Number of kernels this library launched on the context since creation. */
 long long moao_ctx_launch_count(const moao_ctx* ctx);
 /* Panel width of the blocked factorisation (default 256; multiple of 64). */
@@ -97,7 +112,7 @@ moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
  * products; default 3), bf16 slices of the factor in the correction solves
  * (2 or 3, at most bf16_slices; default 2), int8
  * slices per operand of the refinement residual (2..6, default 5), refinement
- * corrections per target (0..8, default 2), residual tolerance that stops
+ * corrections per target (0..8, default 1), residual tolerance that stops
  * refinement early (default 0) and whether to evaluate the residual again after
  * the last correction (so the report's refine_resid describes the returned R;
  * default 0). */

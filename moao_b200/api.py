@@ -16,7 +16,10 @@ this module              reference
 
 Matrices are column-major with an explicit leading dimension, as in the
 reference. A matrix argument is either a CUDA ``torch.Tensor`` of float64
-(device path, asynchronous on the context stream) or a writable float64
+(device path, asynchronous on the context stream, ordered after the work
+already queued on torch's current stream and before the work queued there
+afterwards, so tensors flow between torch and this library without explicit
+synchronisation) or a writable float64
 ``numpy.ndarray`` (host path: copied to the GPU, computed there, copied back,
 keeping the reference's in-place contracts). Every computation runs in the
 CUDA library; there is no CPU implementation in this package.
@@ -64,6 +67,37 @@ def _ptr(x, what: str) -> int:
     raise TypeError(f"{what}: expected a CUDA torch.Tensor or a numpy.ndarray, got {type(x)}")
 
 
+class _TorchOrder:
+    """Stream ordering of a device call against torch's current stream.
+
+    On entry the context's stream waits for the work already queued on torch's
+    current stream (the producer of the inputs); on exit torch's current stream
+    waits for the context's work (so later torch kernels, and the caching
+    allocator's reuse of freed blocks, come after the call). No host
+    synchronisation; a no-op when both are the same stream."""
+
+    def __init__(self, ctx: "Context", active: bool):
+        self.active = active
+        self.ctx = ctx
+
+    def __enter__(self):
+        if not self.active:
+            return self
+        import torch
+        self.cur = torch.cuda.current_stream(self.ctx.device)
+        handle = self.ctx.stream
+        self.same = handle == self.cur.cuda_stream
+        if not self.same:
+            self.ext = torch.cuda.ExternalStream(handle, device=self.ctx.device)
+            self.ext.wait_stream(self.cur)
+        return self
+
+    def __exit__(self, *exc):
+        if self.active and not self.same:
+            self.cur.wait_stream(self.ext)
+        return False
+
+
 def _on_device(*xs) -> bool:
     kinds = {_is_torch(x) for x in xs if x is not None}
     if len(kinds) > 1:
@@ -109,12 +143,28 @@ class Context:
     def set_block(self, nb: int):
         check(lib().moao_ctx_set_block(self._h, nb), "moao_ctx_set_block")
 
-    def set_mixed(self, bf16_slices: int = 3, ozaki_slices: int = 5, max_refine: int = 2,
+    def set_mixed(self, bf16_slices: int = 3, ozaki_slices: int = 5, max_refine: int = 1,
                   tol: float = 0.0, final_residual: bool = False, corr_slices: int = 2):
         """Options of the mixed-precision reconstructor (see moao_ctx_set_mixed)."""
         check(lib().moao_ctx_set_mixed(self._h, bf16_slices, corr_slices, ozaki_slices,
                                        max_refine, tol, int(final_residual)),
               "moao_ctx_set_mixed")
+
+    def set_offsets(self, begin, end, value):
+        """Block-constant offsets of Cmm for the mixed path (see moao_ctx_set_offsets);
+        empty sequences clear them."""
+        b = np.ascontiguousarray(begin, dtype=np.int32)
+        e = np.ascontiguousarray(end, dtype=np.int32)
+        v = np.ascontiguousarray(value, dtype=np.float64)
+        if not (len(b) == len(e) == len(v)):
+            raise ValueError("set_offsets: begin, end and value differ in length")
+        check(lib().moao_ctx_set_offsets(self._h, len(b), b.ctypes.data, e.ctypes.data,
+                                         v.ctypes.data), "moao_ctx_set_offsets")
+
+    def set_offsets_from_tomo(self, tomo: "Tomo"):
+        """Declare the LGS constant blocks of the tomo's covariance model."""
+        check(lib().moao_ctx_set_offsets_from_tomo(self._h, tomo.handle),
+              "moao_ctx_set_offsets_from_tomo")
 
     def set_kernel_timing(self, enable: bool):
         check(lib().moao_ctx_set_kernel_timing(self._h, int(enable)), "moao_ctx_set_kernel_timing")
@@ -225,8 +275,9 @@ def matcov_tile(data, nrows: int, ncols: int, xoffset: int, yoffset: int, lda: i
     ctx = ctx or default_context()
     p = _ptr(data, "matcov_tile data")
     if _on_device(data):
-        check(lib().moao_matcov_tile(ctx.handle, tomo.handle, p, nrows, ncols, xoffset, yoffset,
-                                     lda, type_mat), "moao_matcov_tile")
+        with _TorchOrder(ctx, True):
+            check(lib().moao_matcov_tile(ctx.handle, tomo.handle, p, nrows, ncols, xoffset,
+                                         yoffset, lda, type_mat), "moao_matcov_tile")
     else:
         check(lib().moao_matcov_tile_host(ctx.handle, tomo.handle, p, nrows, ncols, xoffset,
                                           yoffset, lda, type_mat), "moao_matcov_tile_host")
@@ -240,8 +291,9 @@ def reconstructor(nmeas: int, nmeasts: int, Cmm, ldCmm: int, Ctm, ldCtm: int, ng
     rep = SolveReport()
     pc, pt = _ptr(Cmm, "Cmm"), _ptr(Ctm, "Ctm")
     if _on_device(Cmm, Ctm):
-        st = lib().moao_reconstructor(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
-                                      PREC[prec], C.byref(rep))
+        with _TorchOrder(ctx, True):
+            st = lib().moao_reconstructor(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
+                                          PREC[prec], C.byref(rep))
     else:
         if prec != "fp64":
             raise ValueError("the host-buffer reconstructor runs the FP64 path")
@@ -262,8 +314,10 @@ def Cee_Cvv(nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx
     args = []
     for m, n, ld in zip(mats, names, lds):
         args += [_ptr(m, n), ld]
-    f = lib().moao_cee_cvv if _on_device(*mats) else lib().moao_cee_cvv_host
-    check(f(ctx.handle, nmeas, nmeasts, nact, *args), "Cee_Cvv")
+    dev = _on_device(*mats)
+    f = lib().moao_cee_cvv if dev else lib().moao_cee_cvv_host
+    with _TorchOrder(ctx, dev):
+        check(f(ctx.handle, nmeas, nmeasts, nact, *args), "Cee_Cvv")
 
 
 class Intersample:
@@ -294,8 +348,9 @@ class Intersample:
             import torch
             if out is None:
                 out = torch.empty((self.N, self.N), dtype=torch.float64, device=Cvv.device)
-            check(lib().moao_intersample_process(self._h, _ptr(Cvv, "Cvv"), _ptr(out, "psf")),
-                  "moao_intersample_process")
+            with _TorchOrder(self.ctx, True):
+                check(lib().moao_intersample_process(self._h, _ptr(Cvv, "Cvv"),
+                                                     _ptr(out, "psf")), "moao_intersample_process")
             return out
         cvv = np.ascontiguousarray(Cvv, dtype=np.float64)
         if out is None:

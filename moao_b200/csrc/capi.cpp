@@ -422,6 +422,51 @@ moao_status moao_ctx_set_mixed(moao_ctx* c, int bf16_slices, int corr_slices, in
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_offsets(moao_ctx* c, int nranges, const int* begin, const int* end,
+                                 const double* value) {
+  if (!c || nranges < 0 || nranges > kMaxOffsetRanges || (nranges > 0 && (!begin || !end || !value)))
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_offsets: 0..32 ranges with begin, end and value");
+  OffsetRanges o;
+  for (int w = 0; w < nranges; ++w) {
+    if (begin[w] < 0 || end[w] <= begin[w] || !(value[w] > 0) || !std::isfinite(value[w]))
+      return set_error(MOAO_ERR_BAD_ARG, "ctx_set_offsets: range " + std::to_string(w) +
+                                             " needs 0 <= begin < end and a finite value > 0");
+    for (int v = 0; v < w; ++v)
+      if (begin[w] < end[v] && begin[v] < end[w])
+        return set_error(MOAO_ERR_BAD_ARG, "ctx_set_offsets: ranges overlap");
+    o.begin[o.n] = begin[w];
+    o.end[o.n] = end[w];
+    o.value[o.n] = value[w];
+    ++o.n;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->offsets = o;
+  c->mx_factored_n = -1;
+  return MOAO_OK;
+}
+
+moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* c, const moao_tomo* tp) {
+  if (!c || !tp) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_offsets_from_tomo: null argument");
+  const Tomo_struct<double>& t = tp->t;
+  std::vector<int> b, e;
+  std::vector<double> v;
+  const double cst = t.sys.lgsCst;
+  if (cst > 0) {
+    // Cmm rows: WFS w holds x slopes [base, base + Nsubap) then y slopes; the
+    // LGS constant sits on every xx and yy entry of an LGS's own block.
+    long base = 0;
+    for (int w = 0; w + 1 < t.sys.nW; ++w) {
+      const long ns = t.Nsubap[w];
+      if (w < t.sys.nLgs) {
+        b.push_back((int)base); e.push_back((int)(base + ns)); v.push_back(cst);
+        b.push_back((int)(base + ns)); e.push_back((int)(base + 2 * ns)); v.push_back(cst);
+      }
+      base += 2 * ns;
+    }
+  }
+  return moao_ctx_set_offsets(c, (int)b.size(), b.data(), e.data(), v.data());
+}
+
 moao_status moao_ctx_set_block(moao_ctx* c, int nb) {
   if (!c || nb < 64 || nb % 64 != 0 || nb > 2048)
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_block: nb must be a multiple of 64 in [64, 2048]");

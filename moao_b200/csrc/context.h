@@ -12,6 +12,7 @@
 #include "moao_b200_tomo.hpp"
 #include "moao_internal.h"
 #include "dense.h"
+#include "mixed.h"
 
 struct moao_tomo {
   Tomo_struct<double> t;
@@ -55,11 +56,15 @@ struct moao_ctx {
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
+  moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv;
   long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
+  // Block-constant offsets of Cmm known to the caller (moao_ctx_set_offsets):
+  // the mixed path factors Cmm minus them and adds them back exactly.
+  moao::OffsetRanges offsets;
   int bf16_slices = 3;       // bf16 slices of the factor (3: ~24 bits, 6 products)
   int corr_slices = 2;       // bf16 slices of the factor in the correction solves
   int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
-  int max_refine = 2;        // refinement corrections per target
+  int max_refine = 1;        // refinement corrections per target
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this
   int final_residual = 0;    // evaluate the residual once more after the last correction
   cudaEvent_t ev[8] = {};

@@ -18,8 +18,19 @@
 //   FP64), dR = E (L L^T)^-1 by the mixed solve with 2 slices (a correction
 //   needs ~1e-2 relative accuracy only), R += dR; repeated while ||E||/||Ctm|| is
 //   above the tolerance (at most max_refine times).
+// Offsets: when the caller declares block-constant offsets of Cmm
+// (Cmm = B + U D U^T, U the indicator columns of index ranges, D diagonal; the
+// LGS tip-tilt constant of the covariance model is one per LGS and axis), the
+// factorisation is of B, whose entries are not dominated by the constants
+// (FP32 keeps their low bits), and the solves add the offsets back by the
+// Woodbury identity:
+//   X M^-1 = Z - (Z U) S^-1 Y,  Z = X M_B^-1,  Y = U^T M_B^-1,  S = D^-1 + Y U.
+// The refinement residual takes the product with B from the int8 slices (the
+// column scales of B are not set by the constants either) and the offsets'
+// part R U D U^T from FP64 range sums of R.
 // Cmm is read through its lower triangle and overwritten with the (FP32)
-// factor at the end, Ctm with R in FP64, like the FP64 path.
+// factor at the end, Ctm with R in FP64, like the FP64 path; with offsets the
+// factor written is that of B.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,6 +63,7 @@ moao_status sumsq(moao_ctx* ctx, const double* A, long lda, long m, long n, doub
                   double* h_out) {
   MOAO_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double), ctx->stream));
   sumsq_kernel<<<148 * 4, 256, 0, ctx->stream>>>(A, lda, m, n, d_out);
+  ++ctx->launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   MOAO_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -62,8 +74,45 @@ struct Maps {
   TcTensor lrA[kMaxBfSlices];  // Lr slices as A operands (128-row boxes)
   TcTensor lrB[kMaxBfSlices];  // Lr slices as B operands (256-row boxes)
   TcTensor lcB[kMaxBfSlices];  // Lc slices as B operands
-  TcTensor xA[kMaxBfSlices];   // solve-panel slices as A operands
+  TcTensor xA[kMaxBfSlices];   // solve-panel slices as A operands (m rows)
+  TcTensor yA[kMaxBfSlices];   // the same slices for the 128-row offset solve
 };
+
+constexpr long kYRows = 128;  // rows of the offset-indicator solve (one tile)
+
+// Inverse of a small dense matrix (row-major k x k) by Gauss-Jordan elimination
+// with partial pivoting; false if singular.
+bool invert_small(std::vector<double>& a, int k) {
+  std::vector<double> inv(k * k, 0.0);
+  for (int i = 0; i < k; ++i) inv[i * k + i] = 1.0;
+  for (int c = 0; c < k; ++c) {
+    int p = c;
+    for (int r = c + 1; r < k; ++r)
+      if (std::fabs(a[r * k + c]) > std::fabs(a[p * k + c])) p = r;
+    if (!(std::fabs(a[p * k + c]) > 0)) return false;
+    if (p != c)
+      for (int j = 0; j < k; ++j) {
+        std::swap(a[p * k + j], a[c * k + j]);
+        std::swap(inv[p * k + j], inv[c * k + j]);
+      }
+    const double d = 1.0 / a[c * k + c];
+    for (int j = 0; j < k; ++j) {
+      a[c * k + j] *= d;
+      inv[c * k + j] *= d;
+    }
+    for (int r = 0; r < k; ++r) {
+      if (r == c) continue;
+      const double f = a[r * k + c];
+      if (f == 0) continue;
+      for (int j = 0; j < k; ++j) {
+        a[r * k + j] -= f * a[c * k + j];
+        inv[r * k + j] -= f * inv[c * k + j];
+      }
+    }
+  }
+  a.swap(inv);
+  return true;
+}
 
 // Products s_i * s_j of bf16 slices kept for a given slice count, smallest
 // first: the tensor core's FP32 accumulation truncates each addition (a bias of
@@ -113,9 +162,9 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
 
 // In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1, with the long
 // updates as the given slice products.
-moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double* dinv, Maps& mp,
-                        double* W1, double* W2, void* const* xs, long ldx, const Products& pr,
-                        int slices, int* err) {
+moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double* dinv,
+                        const TcTensor* xA, const Maps& mp, double* W1, double* W2,
+                        void* const* xs, long ldx, const Products& pr, int slices, int* err) {
   const long nb = ctx->nb;
   cudaStream_t s = ctx->stream;
   BfSlices xr{}, none{};
@@ -128,7 +177,7 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     const long rest = n - k0 - kb;
     if (rest > 0) {
       MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
-      MOAO_TRY(tc_update(ctx, mp.xA, 0, 0, mp.lrB, (int)(k0 + kb), (int)k0, (int)((kb + 63) / 64),
+      MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lrB, (int)(k0 + kb), (int)k0, (int)((kb + 63) / 64),
                          pr, m, rest, T32 + (k0 + kb) * m, m, false, err, 2.0 * m * rest * kb));
     }
   }
@@ -140,7 +189,7 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
     if (k0 > 0) {
       MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
-      MOAO_TRY(tc_update(ctx, mp.xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
+      MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
                          T32, m, false, err, 2.0 * m * k0 * kb));
     }
   }
@@ -149,8 +198,17 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
 
 }  // namespace
 
+// Adds the helper kernels launched during its lifetime to the context's count.
+struct HelperCount {
+  moao_ctx* ctx;
+  long long h0 = helper_launches();
+  explicit HelperCount(moao_ctx* c) : ctx(c) {}
+  ~HelperCount() { ctx->launches += helper_launches() - h0; }
+};
+
 moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,
                                 double* Ctm, long ldCtm, bool reuse, moao_solve_report* rep) {
+  HelperCount hc(ctx);
   const long nb = ctx->nb;
   cudaStream_t s = ctx->stream;
   const long ldn = round_up(n, 64);    // bf16 row stride of the factor copies
@@ -197,6 +255,28 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   int* d_info = ctx->ws_info.as<int>();
   int* err = d_info + 1;
 
+  // ---- declared offsets of Cmm (Woodbury)
+  const OffsetRanges& off = ctx->offsets;
+  const int nro = off.n;  // offset ranges
+  for (int w = 0; w < nro; ++w)
+    if (off.end[w] > n)
+      return set_error(MOAO_ERR_BAD_ARG, "mixed reconstructor: an offset range ends beyond nmeas");
+  int* rid = nullptr;
+  float* Y32 = nullptr;
+  double *Y2 = nullptr, *ZU = nullptr, *Sinv = nullptr;
+  if (nro > 0) {
+    MOAO_TRY(ctx->mx_rid.ensure(sizeof(int) * (size_t)n));
+    MOAO_TRY(ctx->mx_y.ensure(sizeof(float) * (size_t)kYRows * n));
+    MOAO_TRY(ctx->mx_y2.ensure(sizeof(double) * (size_t)nro * n));
+    MOAO_TRY(ctx->mx_zu.ensure(sizeof(double) * (size_t)std::max(m, (long)nro) * nro));
+    MOAO_TRY(ctx->mx_sinv.ensure(sizeof(double) * (size_t)nro * nro));
+    rid = ctx->mx_rid.as<int>();
+    Y32 = ctx->mx_y.as<float>();
+    Y2 = ctx->mx_y2.as<double>();
+    ZU = ctx->mx_zu.as<double>();
+    Sinv = ctx->mx_sinv.as<double>();
+  }
+
   Maps mp;
   for (int k = 0; k < nsl; ++k) {
     uint16_t* lrk = lr + (size_t)k * n * ldn;
@@ -205,6 +285,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(make_tc_map(&mp.lrB[k], lrk, kTcBf16, n, n, ldn, 256));
     MOAO_TRY(make_tc_map(&mp.lcB[k], lck, kTcBf16, n, n, ldn, 256));
     MOAO_TRY(make_tc_map(&mp.xA[k], xs[k], kTcBf16, m, nb, ldx));
+    MOAO_TRY(make_tc_map(&mp.yA[k], xs[k], kTcBf16, kYRows, nb, ldx));
   }
   const int csl = std::max(2, std::min(nsl, ctx->corr_slices));
   const Products full = products_for(nsl), corr = products_for(csl);
@@ -213,7 +294,14 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   cudaEventRecord(ev[3], s);
   if (!reuse || ctx->mx_factored_n != n) {
     MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 2 * sizeof(int), s));
-    MOAO_TRY(cvt_f64_to_f32(Cmm, ldCmm, A32, n, n, n, true, s));
+    if (nro > 0) {
+      std::vector<int> hrid(n, -1);
+      for (int w = 0; w < nro; ++w)
+        for (int j = off.begin[w]; j < off.end[w]; ++j) hrid[j] = w;
+      // pageable source: the copy is staged before the call returns
+      MOAO_CUDA_TRY(cudaMemcpyAsync(rid, hrid.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    }
+    MOAO_TRY(cvt_lower_minus_offsets(Cmm, ldCmm, A32, n, n, rid, off, s));
     for (long k0 = 0; k0 < n; k0 += nb) {
       const long kb = std::min(nb, n - k0);
       float* Akk = A32 + k0 + k0 * n;
@@ -248,14 +336,38 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     }
     // int8 slices of sym(Cmm) for the refinement residual
     MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
-                             ldq, s));
+                             ldq, rid, off, s));
+    if (nro > 0) {
+      // Y = U^T M_B^-1 (one 128-row solve), S = D^-1 + Y U, Y2 = S^-1 Y
+      MOAO_TRY(fill_range_indicators(Y32, kYRows, n, off, s));
+      MOAO_TRY(mixed_solve(ctx, n, kYRows, Y32, dinv, mp.yA, mp, W1, W2, xs, ldx, full, nsl, err));
+      MOAO_TRY(range_sums(Y32, kYRows, nro, off, ZU, s));
+      std::vector<double> yu((size_t)nro * nro), a((size_t)nro * nro), sc((size_t)nro * nro);
+      MOAO_CUDA_TRY(cudaMemcpyAsync(yu.data(), ZU, sizeof(double) * nro * nro, cudaMemcpyDeviceToHost, s));
+      MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+      for (int v = 0; v < nro; ++v)
+        for (int w = 0; w < nro; ++w)
+          a[v * nro + w] = yu[(size_t)w * nro + v] + (v == w ? 1.0 / off.value[v] : 0.0);
+      if (!invert_small(a, nro))
+        return set_error(MOAO_ERR_BAD_ARG,
+                         "mixed reconstructor: offsets give a singular capacitance matrix");
+      for (int v = 0; v < nro; ++v)
+        for (int w = 0; w < nro; ++w) sc[(size_t)w * nro + v] = a[v * nro + w];
+      MOAO_CUDA_TRY(cudaMemcpyAsync(Sinv, sc.data(), sizeof(double) * nro * nro, cudaMemcpyHostToDevice, s));
+      MOAO_TRY(mul_small_left(Sinv, nro, Y32, kYRows, n, Y2, s));
+    }
     ctx->mx_factored_n = n;
   }
   cudaEventRecord(ev[4], s);
   // ---- solve
   MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
-  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xs, ldx, full, nsl, err));
-  MOAO_TRY(cvt_f32_to_f64(T32, m, R64, m, m, n, false, s));
+  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, full, nsl, err));
+  if (nro > 0) {
+    MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
+    MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, R64, m, false, s));
+  } else {
+    MOAO_TRY(cvt_f32_to_f64(T32, m, R64, m, m, n, false, s));
+  }
   cudaEventRecord(ev[5], s);
   // ---- refinement
   TcTensor ta[kMaxOzakiSlices], tb[kMaxOzakiSlices];
@@ -302,6 +414,10 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
         MOAO_TRY(tc_gemm(g, s, &ctx->launches));
       }
     }
+    if (nro > 0) {  // the offsets' part of R Cmm
+      MOAO_TRY(range_sums(R64, m, m, off, ZU, s));
+      MOAO_TRY(subtract_offset_products(E64, m, m, n, ZU, rid, off, s));
+    }
     MOAO_TRY(sumsq(ctx, E64, m, m, n, dnorm, &e2));
     rep->refine_resid = std::sqrt(e2 / std::max(ctm2, 1e-300));
     return MOAO_OK;
@@ -311,8 +427,13 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(residual());
     if (rep->refine_resid <= ctx->refine_tol) break;
     MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
-    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp, W1, W2, xs, ldx, corr, csl, err));
-    MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
+    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, corr, csl, err));
+    if (nro > 0) {
+      MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
+      MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, R64, m, true, s));
+    } else {
+      MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
+    }
   }
   if (ctx->final_residual) MOAO_TRY(residual());
   rep->refine_steps = steps;
@@ -335,6 +456,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
 }
 
 moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm) {
+  HelperCount hc(ctx);
   MOAO_TRY(cvt_f32_to_f64(ctx->mx_a32.as<float>(), n, Cmm, ldCmm, n, n, true, ctx->stream));
   ctx->mx_factored_n = -1;
   return MOAO_OK;

@@ -11,7 +11,21 @@
 namespace moao {
 
 constexpr int kMaxOzakiSlices = 6;
+
+// Kernels launched so far on this thread by the helpers declared here.
+long long helper_launches();
 constexpr int kMaxBfSlices = 3;
+
+constexpr int kMaxOffsetRanges = 32;
+
+// Block-constant offsets of a symmetric matrix: value[w] is part of every entry
+// (i, j) with both i and j in [begin[w], end[w]). Ranges do not overlap.
+struct OffsetRanges {
+  int n = 0;
+  int begin[kMaxOffsetRanges] = {};
+  int end[kMaxOffsetRanges] = {};
+  double value[kMaxOffsetRanges] = {};
+};
 
 // Destinations of the bf16 slices of one block (null p[0] = not wanted); each
 // pointer addresses the block's first element in its slice.
@@ -34,10 +48,37 @@ moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSl
 // slice s at out + s*m*ldo, row-major with row stride ldo.
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
                              int8_t* out, long ldo, cudaStream_t st);
-// int8 slices of the columns of sym(A) for a lower-stored n x n A: per-column
-// exponents in f[n]; slice s at out + s*n*ldo with row j holding column j.
+// int8 slices of the columns of sym(A) - offsets for a lower-stored n x n A
+// (rid: range of every index or -1, null for no offsets): per-column exponents
+// in f[n]; slice s at out + s*n*ldo with row j holding column j.
 moao_status ozaki_split_sym(const double* A, long lda, long n, int ns, int* f,
-                            unsigned long long* colmax, int8_t* out, long ldo, cudaStream_t st);
+                            unsigned long long* colmax, int8_t* out, long ldo, const int* rid,
+                            const OffsetRanges& off, cudaStream_t st);
+
+// ---- offsets handled by the Woodbury identity (mixed.cpp)
+// Lower triangle of (A - offsets) in FP32.
+moao_status cvt_lower_minus_offsets(const double* s, long lds, float* d, long ldd, long n,
+                                    const int* rid, const OffsetRanges& off, cudaStream_t st);
+// Y (ldy x n, column-major, FP32) = indicator rows: Y(w, j) = 1 for j in range w,
+// 0 elsewhere (rows off.n .. ldy-1 included).
+moao_status fill_range_indicators(float* Y, long ldy, long n, const OffsetRanges& off,
+                                  cudaStream_t st);
+// out(i, w) = sum over j in range w of Z(i, j), Z m x n column-major; out m x
+// off.n column-major (ld m), accumulated in FP64.
+moao_status range_sums(const float* Z, long ldz, long m, const OffsetRanges& off, double* out,
+                       cudaStream_t st);
+moao_status range_sums(const double* Z, long ldz, long m, const OffsetRanges& off, double* out,
+                       cudaStream_t st);
+// Y2 (k x n, ld k, FP64) = S (k x k, column-major, device) * Y (rows 0..k-1 of ldy x n).
+moao_status mul_small_left(const double* S, int k, const float* Y, long ldy, long n, double* Y2,
+                           cudaStream_t st);
+// R(i, j) (+)= Z(i, j) - sum_w ZU(i, w) Y2(w, j) for an m x n Z (FP32) and R (FP64).
+moao_status woodbury_apply(const float* Z, long ldz, long m, long n, const double* ZU, int k,
+                           const double* Y2, double* R, long ldr, bool accumulate,
+                           cudaStream_t st);
+// E(i, j) -= RU(i, w) value[w] for j in range w (the offsets' part of R*A).
+moao_status subtract_offset_products(double* E, long lde, long m, long n, const double* RU,
+                                     const int* rid, const OffsetRanges& off, cudaStream_t st);
 
 }  // namespace moao
 

@@ -19,6 +19,12 @@
 #include "mixed.h"
 
 namespace moao {
+
+// Kernels launched by the helpers below on the calling thread (the driver adds
+// the difference over a call to its context's launch count).
+static thread_local long long tl_launches = 0;
+long long helper_launches() { return tl_launches; }
+
 namespace {
 
 unsigned blocks_for(long total, long per = 256) {
@@ -133,17 +139,39 @@ __global__ void split_rows_i8_kernel(const double* __restrict__ A, long lda, lon
   }
 }
 
+struct OffsetValues {
+  double v[kMaxOffsetRanges];
+};
+
+OffsetValues values_of(const OffsetRanges& off) {
+  OffsetValues o{};
+  for (int w = 0; w < off.n; ++w) o.v[w] = off.value[w];
+  return o;
+}
+
+// Stored element A(r, c) (r >= c) minus the offset of its block.
+__device__ __forceinline__ double stored_minus(const double* A, long lda, long r, long c,
+                                               const int* rid, const OffsetValues& ov) {
+  double v = A[c * lda + r];
+  if (rid) {
+    const int w = rid[r];
+    if (w >= 0 && w == rid[c]) v -= ov.v[w];
+  }
+  return v;
+}
+
 // Column maxima of sym(A) for a lower-stored n x n A: every stored (r >= c)
 // element feeds column c and column r.
 __global__ void sym_col_max_kernel(const double* __restrict__ A, long lda, long n,
-                                   unsigned long long* __restrict__ cm) {
+                                   unsigned long long* __restrict__ cm, const int* rid,
+                                   const OffsetValues ov) {
   const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
   if (r0 + 31 < c0) return;
   const int tx = threadIdx.x, ty = threadIdx.y;
   __shared__ double t[32][33];
   for (int jj = ty; jj < 32; jj += 8) {
     const long r = r0 + tx, c = c0 + jj;
-    t[tx][jj] = (r < n && c < n && r >= c) ? fabs(A[c * lda + r]) : 0.0;
+    t[tx][jj] = (r < n && c < n && r >= c) ? fabs(stored_minus(A, lda, r, c, rid, ov)) : 0.0;
   }
   __syncthreads();
   if (ty == 0) {  // column c0 + tx: max over the 32 rows
@@ -167,7 +195,7 @@ __global__ void exponents_from_max_kernel(const unsigned long long* __restrict__
 // K-major B operand of S), S(k, j) = A(max(k,j), min(k,j)).
 __global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long n,
                                     const int* __restrict__ f, int ns, int8_t* out, long ldo,
-                                    long slice_stride) {
+                                    long slice_stride, const int* rid, const OffsetValues ov) {
   __shared__ double t[32][33];  // t[jj][kk] = S(k0+kk, j0+jj)
   const long j0 = (long)blockIdx.x * 32, k0 = (long)blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -175,19 +203,20 @@ __global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long
     // k > j everywhere: S(k, j) = A(k, j), contiguous in k
     for (int jj = ty; jj < 32; jj += 8) {
       const long k = k0 + tx, j = j0 + jj;
-      t[jj][tx] = (k < n && j < n) ? A[j * lda + k] : 0.0;
+      t[jj][tx] = (k < n && j < n) ? stored_minus(A, lda, k, j, rid, ov) : 0.0;
     }
   } else if (k0 + 32 <= j0) {
     // k < j everywhere: S(k, j) = A(j, k), contiguous in j
     for (int kk = ty; kk < 32; kk += 8) {
       const long j = j0 + tx, k = k0 + kk;
-      t[tx][kk] = (k < n && j < n) ? A[k * lda + j] : 0.0;
+      t[tx][kk] = (k < n && j < n) ? stored_minus(A, lda, j, k, rid, ov) : 0.0;
     }
   } else {
     for (int jj = ty; jj < 32; jj += 8) {
       const long k = k0 + tx, j = j0 + jj;
       double v = 0;
-      if (k < n && j < n) v = (k >= j) ? A[j * lda + k] : A[k * lda + j];
+      if (k < n && j < n)
+        v = (k >= j) ? stored_minus(A, lda, k, j, rid, ov) : stored_minus(A, lda, j, k, rid, ov);
       t[jj][tx] = v;
     }
   }
@@ -204,12 +233,193 @@ __global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long
   }
 }
 
+// ---- offsets by the Woodbury identity
+
+__global__ void cvt_lower_minus_kernel(const double* __restrict__ s, long lds,
+                                       float* __restrict__ d, long ldd, long n,
+                                       const int* __restrict__ rid, const OffsetValues ov) {
+  const long total = n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, j = e / n;
+    if (i < j) continue;
+    d[j * ldd + i] = (float)stored_minus(s, lds, i, j, rid, ov);
+  }
+}
+
+struct RangeList {
+  int n;
+  int begin[kMaxOffsetRanges], end[kMaxOffsetRanges];
+};
+
+RangeList ranges_of(const OffsetRanges& off) {
+  RangeList r{};
+  r.n = off.n;
+  for (int w = 0; w < off.n; ++w) {
+    r.begin[w] = off.begin[w];
+    r.end[w] = off.end[w];
+  }
+  return r;
+}
+
+__global__ void fill_indicator_kernel(float* __restrict__ Y, long ldy, long n, const RangeList rl) {
+  const long total = ldy * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long w = e % ldy, j = e / ldy;
+    Y[e] = (w < rl.n && j >= rl.begin[w] && j < rl.end[w]) ? 1.f : 0.f;
+  }
+}
+
+// One thread per (row i, range w): rows are contiguous in memory, so a warp
+// reads 32 consecutive elements of each column of the range.
+template <typename T>
+__global__ void range_sums_kernel(const T* __restrict__ Z, long ldz, long m, const RangeList rl,
+                                  double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int w = blockIdx.y;
+  if (i >= m) return;
+  double s0 = 0, s1 = 0;
+  long j = rl.begin[w];
+  for (; j + 1 < rl.end[w]; j += 2) {
+    s0 += (double)Z[j * ldz + i];
+    s1 += (double)Z[(j + 1) * ldz + i];
+  }
+  if (j < rl.end[w]) s0 += (double)Z[j * ldz + i];
+  out[(long)w * m + i] = s0 + s1;
+}
+
+__global__ void mul_small_left_kernel(const double* __restrict__ S, int k,
+                                      const float* __restrict__ Y, long ldy, long n,
+                                      double* __restrict__ Y2) {
+  __shared__ double sS[kMaxOffsetRanges * kMaxOffsetRanges];
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) sS[t] = S[t];
+  __syncthreads();
+  const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double y[kMaxOffsetRanges];
+  for (int w = 0; w < k; ++w) y[w] = (double)Y[j * ldy + w];
+  for (int v = 0; v < k; ++v) {
+    double a = 0;
+    for (int w = 0; w < k; ++w) a = fma(sS[w * k + v], y[w], a);
+    Y2[j * k + v] = a;
+  }
+}
+
+// 256 rows per block, 64 columns per block; ZU(i, :) stays in registers.
+__global__ void woodbury_kernel(const float* __restrict__ Z, long ldz, long m, long n,
+                                const double* __restrict__ ZU, int k,
+                                const double* __restrict__ Y2, double* __restrict__ R, long ldr,
+                                int accumulate) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long j0 = (long)blockIdx.y * 64;
+  if (i >= m) return;
+  double zu[kMaxOffsetRanges];
+#pragma unroll
+  for (int w = 0; w < kMaxOffsetRanges; ++w) zu[w] = w < k ? ZU[(long)w * m + i] : 0.0;
+  const long j1 = min(n, j0 + 64);
+  for (long j = j0; j < j1; ++j) {
+    double a = (double)Z[j * ldz + i];
+    const double* y = Y2 + j * k;
+#pragma unroll
+    for (int w = 0; w < kMaxOffsetRanges; ++w)
+      if (w < k) a = fma(-zu[w], y[w], a);
+    if (accumulate) R[j * ldr + i] += a;
+    else R[j * ldr + i] = a;
+  }
+}
+
+__global__ void subtract_offset_kernel(double* __restrict__ E, long lde, long m, long n,
+                                       const double* __restrict__ RU,
+                                       const int* __restrict__ rid, const OffsetValues ov) {
+  const long total = m * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long i = e % m, j = e / m;
+    const int w = rid[j];
+    if (w >= 0) E[j * lde + i] -= RU[(long)w * m + i] * ov.v[w];
+  }
+}
+
 }  // namespace
+
+moao_status cvt_lower_minus_offsets(const double* s, long lds, float* d, long ldd, long n,
+                                    const int* rid, const OffsetRanges& off, cudaStream_t st) {
+  if (n <= 0) return MOAO_OK;
+  cvt_lower_minus_kernel<<<blocks_for(n * n), 256, 0, st>>>(s, lds, d, ldd, n,
+                                                            off.n ? rid : nullptr, values_of(off));
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status fill_range_indicators(float* Y, long ldy, long n, const OffsetRanges& off,
+                                  cudaStream_t st) {
+  if (n <= 0) return MOAO_OK;
+  fill_indicator_kernel<<<blocks_for(ldy * n), 256, 0, st>>>(Y, ldy, n, ranges_of(off));
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+template <typename T>
+static moao_status range_sums_impl(const T* Z, long ldz, long m, const OffsetRanges& off,
+                                   double* out, cudaStream_t st) {
+  if (m <= 0 || off.n <= 0) return MOAO_OK;
+  dim3 grid((unsigned)((m + 255) / 256), (unsigned)off.n);
+  range_sums_kernel<T><<<grid, 256, 0, st>>>(Z, ldz, m, ranges_of(off), out);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status range_sums(const float* Z, long ldz, long m, const OffsetRanges& off, double* out,
+                       cudaStream_t st) {
+  return range_sums_impl(Z, ldz, m, off, out, st);
+}
+
+moao_status range_sums(const double* Z, long ldz, long m, const OffsetRanges& off, double* out,
+                       cudaStream_t st) {
+  return range_sums_impl(Z, ldz, m, off, out, st);
+}
+
+moao_status mul_small_left(const double* S, int k, const float* Y, long ldy, long n, double* Y2,
+                           cudaStream_t st) {
+  if (n <= 0 || k <= 0) return MOAO_OK;
+  if (k > kMaxOffsetRanges) return set_error(MOAO_ERR_BAD_ARG, "mul_small_left: k");
+  mul_small_left_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, k, Y, ldy, n, Y2);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status woodbury_apply(const float* Z, long ldz, long m, long n, const double* ZU, int k,
+                           const double* Y2, double* R, long ldr, bool accumulate,
+                           cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  if (k < 1 || k > kMaxOffsetRanges) return set_error(MOAO_ERR_BAD_ARG, "woodbury_apply: k");
+  dim3 grid((unsigned)((m + 255) / 256), (unsigned)((n + 63) / 64));
+  woodbury_kernel<<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, accumulate ? 1 : 0);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status subtract_offset_products(double* E, long lde, long m, long n, const double* RU,
+                                     const int* rid, const OffsetRanges& off, cudaStream_t st) {
+  if (m <= 0 || n <= 0 || off.n <= 0) return MOAO_OK;
+  subtract_offset_kernel<<<blocks_for(m * n), 256, 0, st>>>(E, lde, m, n, RU, rid,
+                                                            values_of(off));
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
 
 moao_status cvt_f32_to_f64(const float* s, long lds, double* d, long ldd, long m, long n,
                            bool lower, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   cvt_f32_f64_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n, lower);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
@@ -218,6 +428,7 @@ moao_status cvt_f64_to_f32(const double* s, long lds, float* d, long ldd, long m
                            bool lower, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   cvt_f64_f32_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n, lower);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
@@ -226,6 +437,7 @@ moao_status add_f32_to_f64(const float* s, long lds, double* d, long ldd, long m
                            cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   add_f32_to_f64_kernel<<<blocks_for(m * n), 256, 0, st>>>(s, lds, d, ldd, m, n);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
@@ -236,6 +448,7 @@ moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSl
   if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_bf16: slices");
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
   split_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(src, lds, m, n, ns, rmaj, ldr, cmaj, ldc);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
@@ -244,20 +457,28 @@ moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, 
                              int8_t* out, long ldo, cudaStream_t st) {
   if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
   row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e);
+  ++tl_launches;
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
   split_rows_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, m, n, e, ns, out, ldo, m * ldo);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
 
 moao_status ozaki_split_sym(const double* A, long lda, long n, int ns, int* f,
-                            unsigned long long* colmax, int8_t* out, long ldo, cudaStream_t st) {
+                            unsigned long long* colmax, int8_t* out, long ldo, const int* rid,
+                            const OffsetRanges& off, cudaStream_t st) {
   if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
   MOAO_CUDA_TRY(cudaMemsetAsync(colmax, 0, n * sizeof(unsigned long long), st));
+  const int* r = off.n ? rid : nullptr;
+  const OffsetValues ov = values_of(off);
   dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
-  sym_col_max_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, colmax);
+  sym_col_max_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, colmax, r, ov);
+  ++tl_launches;
   exponents_from_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(colmax, n, f);
-  split_sym_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, f, ns, out, ldo, n * ldo);
+  ++tl_launches;
+  split_sym_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, f, ns, out, ldo, n * ldo, r, ov);
+  ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
