@@ -102,6 +102,10 @@ moao_status moao_ctx_set_offsets(moao_ctx* ctx, int nranges, const int* begin, c
  * the reference adds it to each such element). */
 moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* ctx, const moao_tomo* tomo);
 
+/* Precision of moao_reconstructor_host (default MOAO_PREC_FP64, the
+ * reference's behaviour). No reference counterpart. */
+moao_status moao_ctx_set_host_precision(moao_ctx* ctx, moao_prec prec);
+
 /* Number of kernels this library launched on the context since creation. */
 long long moao_ctx_launch_count(const moao_ctx* ctx);
 /* Panel width of the blocked factorisation (default 256; multiple of 64). */
@@ -236,6 +240,20 @@ moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, doub
 /* Same with host Cvv in and host PSF out. */
 moao_status moao_intersample_process_host(moao_isample* is, const double* Cvv, double* psf);
 void moao_intersample_destroy(moao_isample* is);
+
+/* ---- FITS images (primary HDU, 1-D or 2-D), the file format of the
+ * reference's inputs and check outputs (common/io/fits.cpp;
+ * common/tomo_struct/intersample.cpp:208-300 reads idx, abs2fi, otftel).
+ * Readers convert any BITPIX (8, 16, 32, 64, -32, -64) and apply BZERO/BSCALE;
+ * out may be NULL to query NAXIS1/NAXIS2 (NAXIS2 = 1 for a 1-D image). Data
+ * order is the file's: NAXIS1 fastest. Host-only: no GPU needed. */
+moao_status moao_fits_read_f64(const char* path, long* naxis1, long* naxis2, double* out,
+                               long cap);
+moao_status moao_fits_read_i64(const char* path, long* naxis1, long* naxis2, long long* out,
+                               long cap);
+moao_status moao_fits_write_f64(const char* path, long naxis1, long naxis2, const double* data);
+moao_status moao_fits_write_i64(const char* path, long naxis1, long naxis2,
+                                const long long* data);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,11 @@ SIGNATURES = {
     "moao_ctx_set_kernel_timing": (i32, [vp, i32]),
     "moao_ctx_set_mixed": (i32, [vp, i32, i32, i32, i32, C.c_double, i32]),
     "moao_ctx_set_offsets": (i32, [vp, i32, vp, vp, vp]),
+    "moao_ctx_set_host_precision": (i32, [vp, i32]),
+    "moao_fits_read_f64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
+    "moao_fits_read_i64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
+    "moao_fits_write_f64": (i32, [C.c_char_p, C.c_long, C.c_long, vp]),
+    "moao_fits_write_i64": (i32, [C.c_char_p, C.c_long, C.c_long, vp]),
     "moao_ctx_set_offsets_from_tomo": (i32, [vp, vp]),
     "moao_ctx_kernel_stats": (i32, [vp, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),

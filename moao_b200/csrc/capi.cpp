@@ -467,6 +467,13 @@ moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* c, const moao_tomo* tp) {
   return moao_ctx_set_offsets(c, (int)b.size(), b.data(), e.data(), v.data());
 }
 
+moao_status moao_ctx_set_host_precision(moao_ctx* c, moao_prec prec) {
+  if (!c || (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED))
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_precision: FP64 or MIXED");
+  c->host_prec = prec;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_block(moao_ctx* c, int nb) {
   if (!c || nb < 64 || nb % 64 != 0 || nb > 2048)
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_block: nb must be a multiple of 64 in [64, 2048]");
@@ -542,7 +549,7 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
   if (!fail(cudaMemcpy2DAsync(dC, sizeof(double) * nmeas, Cmm, sizeof(double) * ldCmm,
                               sizeof(double) * nmeas, nmeas, cudaMemcpyHostToDevice, s)) &&
       !fail(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice, s))) {
-    st = moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, MOAO_PREC_FP64, rep);
+    st = moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, ctx->host_prec, rep);
     // On a failed factorisation the reference has already overwritten Cmm
     // (partially) and leaves Ctm alone; mirror that.
     if (!fail(cudaMemcpy2DAsync(Cmm, sizeof(double) * ldCmm, dC, sizeof(double) * nmeas,

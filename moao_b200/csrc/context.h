@@ -50,6 +50,7 @@ struct moao_ctx {
   cudaStream_t stream = nullptr;
   long long launches = 0;
   int nb = 256;  // outer panel width of the blocked factorisation
+  moao_prec host_prec = MOAO_PREC_FP64;  // precision of moao_reconstructor_host
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
   moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;

@@ -1,0 +1,112 @@
+"""The reference's C++ entry points (include/moao_b200_compat.hpp): a driver
+written against that interface alone (tests/drivers/lapack_driver.cpp, the call
+sequence of the reference's lapack driver) compiles and links against the
+library; on a GPU its outputs equal the Python API's."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import moao_b200 as M
+from moao_b200 import inputs as I
+from moao_b200 import params as P
+from moao_b200.fits import read_fits, write_fits
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "moao_b200")
+
+
+def build_driver(tmp_path):
+    exe = str(tmp_path / "lapack_driver")
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "drivers", "lapack_driver.cpp"), "-L", LIBDIR,
+           "-lmoao_b200", "-Wl,-rpath," + LIBDIR, "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
+def test_driver_compiles_and_links(tmp_path, built):
+    exe = build_driver(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+
+
+def test_exports_reference_symbols(built):
+    r = subprocess.run(["nm", "-DC", os.path.join(LIBDIR, "libmoao_b200.so")],
+                       capture_output=True, text=True)
+    syms = r.stdout
+    for want in ["MOAO_COMMON::matcov_tile<double>(double*, int, int, int, int, int, Tomo_struct<double>*, int)",
+                 "MOAO_COMMON::matcov_tile<float>(float*, int, int, int, int, int, Tomo_struct<float>*, int)",
+                 "MOAO_LAPACK::reconstructor<double>(long, long, double*, long, double*, long, long)",
+                 "MOAO_LAPACK::reconstructor<float>(long, long, float*, long, float*, long, long)",
+                 "MOAO_LAPACK::Cee_Cvv<double>(",
+                 "MOAO_LAPACK::geadd<double>(char, long, long, double, double*, long, double, double*, long)",
+                 "intersample_prepare", "intersample_init", "intersample_free",
+                 "int intersample_process<double>(isample_struct*, double*)",
+                 "void readFits<double>(char const*, double*)", "getFitsDims", "fitsExists",
+                 "Tomo_struct<double>::Tomo_struct("]:
+        assert want in syms, want
+
+
+def write_inputs(d, sysp, nts):
+    x = I.intersample_inputs(sysp.nssp, sysp.diam, sysp.obs)
+    Dx = I.make_dx(x.nact, nts)
+    write_fits(os.path.join(d, "Dx.fits"), Dx.T)  # NAXIS1 = nact (column-major nact x nts)
+    write_fits(os.path.join(d, "idx.fits"), x.idx.astype(np.int64))
+    write_fits(os.path.join(d, "abs2fi.fits"), x.abs2fi)
+    write_fits(os.path.join(d, "otftel.fits"), x.otf)
+    return x, Dx
+
+
+@pytest.mark.gpu
+def test_driver_matches_python_api(tmp_path, built, ctx):
+    sysp, atm = P.config_small()
+    d = str(tmp_path / "sys")
+    out = str(tmp_path / "out")
+    os.makedirs(out)
+    sf, af = os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt")
+    os.makedirs(d)
+    P.write_system(d, sysp, atm)
+    t = M.Tomo(sf, af)
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    x, Dx = write_inputs(d, sysp, nts)
+    exe = build_driver(tmp_path)
+    r = subprocess.run([exe, d, af, out], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+    # the same sequence through the Python API (host buffers)
+    Cmm = np.zeros((nm, nm), order="F")
+    M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+    t.setTarget(0)
+    R = np.zeros((nts, nm), order="F")
+    M.matcov_tile(R, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+    M.reconstructor(nm, nts, Cmm, nm, R, nts, 1, ctx=ctx)
+    Cmm2 = np.zeros((nm, nm), order="F")
+    M.matcov_tile(Cmm2, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+    Ctm = np.zeros((nts, nm), order="F")
+    M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+    Ctt = np.zeros((nts, nts), order="F")
+    M.matcov_tile(Ctt, nts, nts, 0, 0, nts, t, 4, ctx=ctx)
+    nact = x.nact
+    Cee = np.zeros((nts, nts), order="F")
+    Cvv = np.zeros((nact, nact), order="F")
+    Tmp = np.zeros((nact, nts), order="F")
+    M.Cee_Cvv(nm, nts, nact, Cmm2, nm, Ctt, nts, Ctm, nts, R.copy(order="F"), nts, Dx, nact, Cee,
+              nts, Cvv, nact, Tmp, nact, ctx=ctx)
+    isx = M.Intersample(nact * nact, x.np_, sysp.diam, x.idx, x.abs2fi, x.otf, ctx=ctx)
+    psf = isx.process(Cvv.copy(order="F"))
+    isx.close()
+
+    def same(name, want):
+        got = read_fits(os.path.join(out, name))
+        err = np.max(np.abs(got - want)) / np.max(np.abs(want))
+        assert err <= 1e-12, f"{name}: {err:.2e}"
+
+    same("R_g0.fits", R.T)
+    same("Cee_g0.fits", Cee.T)
+    same("Cvv_g0.fits", Cvv.T)
+    same("psf_g0.fits", psf)
