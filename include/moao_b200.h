@@ -241,6 +241,75 @@ moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, doub
 moao_status moao_intersample_process_host(moao_isample* is, const double* Cvv, double* psf);
 void moao_intersample_destroy(moao_isample* is);
 
+/* ---- Serving: a persistent request loop on one GPU (no reference
+ * counterpart: the reference runs one synchronous driver loop,
+ * lapack/moao_lapack.cpp:95-190). Systems (geometry from a parameter file,
+ * optional Dx and PSF tables) are registered once; requests carry their own
+ * profile and target and arrive at any time. Each is admitted, in arrival
+ * order, when a slot (a worker with its own stream and resident workspaces)
+ * is idle and the request's device footprint fits the HBM budget beside what
+ * the other slots hold, so the device work of concurrent requests overlaps.
+ * Results go to the caller's host buffers. Thread-safe. */
+typedef struct moao_server moao_server;
+typedef struct {
+  int device;            /* CUDA device */
+  int slots;             /* concurrent requests, 1..16 */
+  double hbm_budget_gb;  /* admission budget; <= 0: 90% of the free memory at creation */
+  int queue_capacity;    /* queued requests before submit returns BUSY (<= 0: 4096) */
+  int nb;                /* panel width (<= 0: library default) */
+  int dry_run;           /* 1: host-only model (tests): a request waits dry_run_ms, no GPU */
+} moao_server_opts;
+typedef struct {
+  int system;            /* id from moao_server_add_system */
+  int nlayer;            /* profile of this request (copied at submit) */
+  const double *cn2, *h, *L0;
+  int target;            /* truth-sensor target */
+  moao_prec prec;
+  double* R;             /* host out: nmeasts x nmeas (ld nmeasts), or NULL */
+  double* Cvv;           /* host out: nact x nact, or NULL (system needs Dx) */
+  double* psf;           /* host out: N x N, or NULL (system needs the PSF tables) */
+  double dry_run_ms;     /* duration of this request in dry_run mode */
+} moao_request;
+typedef struct {
+  moao_status status;    /* MOAO_ERR_BUSY while queued or running */
+  int info;              /* Cholesky failure column when NOT_SPD */
+  int slot;              /* slot that ran it */
+  int refine_steps;
+  double refine_resid;
+  double queue_ms, run_ms, latency_ms;  /* submit->start, start->done, submit->done */
+  double start_ms, end_ms;              /* start and end, ms since server creation */
+  double footprint_gb;   /* device bytes admitted for it */
+  char message[256];     /* error text when status is an error */
+} moao_request_result;
+typedef struct {
+  long long submitted, completed, failed, cancelled, rejected;
+  int max_in_flight;       /* peak concurrent requests */
+  double peak_admitted_gb; /* peak device bytes held by slots and admitted requests */
+  double budget_gb;
+} moao_server_stats;
+
+moao_status moao_server_create(const moao_server_opts* opts, moao_server** out);
+/* nact > 0 registers Dx (nact x nmeasts, column-major) for Cvv; idx (nact^2),
+ * abs2fi and otf_tel (N x N) add the PSF step. Host-only. */
+moao_status moao_server_add_system(moao_server* s, const char* sys_file, const char* atm_file,
+                                   long nact, const double* Dx, const long* idx,
+                                   const double* abs2fi, const double* otf_tel, int* system_id);
+moao_status moao_server_system_info(moao_server* s, int system, long* nmeas, long* nmeasts,
+                                    long* nact, long* psf_n);
+/* MOAO_ERR_OOM if the request alone exceeds the budget, MOAO_ERR_BUSY if the
+ * queue is full. */
+moao_status moao_serve_submit(moao_server* s, const moao_request* r, long long* id);
+/* out->status: MOAO_ERR_BUSY (pending), MOAO_ERR_CANCELLED, or the result. */
+moao_status moao_serve_poll(moao_server* s, long long id, moao_request_result* out);
+/* Blocks until done (timeout_s < 0: no limit); MOAO_ERR_TIMEOUT otherwise. */
+moao_status moao_serve_wait(moao_server* s, long long id, double timeout_s,
+                            moao_request_result* out);
+/* Only before the request starts; MOAO_ERR_BUSY after. */
+moao_status moao_serve_cancel(moao_server* s, long long id);
+moao_status moao_server_get_stats(moao_server* s, moao_server_stats* out);
+/* Cancels queued requests, lets running ones finish, frees everything. */
+void moao_server_destroy(moao_server* s);
+
 /* ---- FITS images (primary HDU, 1-D or 2-D), the file format of the
  * reference's inputs and check outputs (common/io/fits.cpp;
  * common/tomo_struct/intersample.cpp:208-300 reads idx, abs2fi, otftel).

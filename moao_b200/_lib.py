@@ -40,6 +40,31 @@ class IsampleInfo(C.Structure):
                 ("dactupix", C.c_double)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", i32), ("slots", i32), ("hbm_budget_gb", C.c_double),
+                ("queue_capacity", i32), ("nb", i32), ("dry_run", i32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("system", i32), ("nlayer", i32), ("cn2", vp), ("h", vp), ("L0", vp),
+                ("target", i32), ("prec", i32), ("R", vp), ("Cvv", vp), ("psf", vp),
+                ("dry_run_ms", C.c_double)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", i32), ("info", i32), ("slot", i32), ("refine_steps", i32),
+                ("refine_resid", C.c_double), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("latency_ms", C.c_double), ("start_ms", C.c_double), ("end_ms", C.c_double),
+                ("footprint_gb", C.c_double),
+                ("message", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("cancelled", C.c_longlong), ("rejected", C.c_longlong), ("max_in_flight", i32),
+                ("peak_admitted_gb", C.c_double), ("budget_gb", C.c_double)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "moao_status_string": (C.c_char_p, [i32]),
@@ -63,6 +88,17 @@ SIGNATURES = {
     "moao_ctx_set_mixed": (i32, [vp, i32, i32, i32, i32, C.c_double, i32]),
     "moao_ctx_set_offsets": (i32, [vp, i32, vp, vp, vp]),
     "moao_ctx_set_host_precision": (i32, [vp, i32]),
+    "moao_server_create": (i32, [C.POINTER(ServerOpts), C.POINTER(vp)]),
+    "moao_server_add_system": (i32, [vp, C.c_char_p, C.c_char_p, C.c_long, vp, vp, vp, vp,
+                                     C.POINTER(i32)]),
+    "moao_server_system_info": (i32, [vp, i32, C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                      C.POINTER(C.c_long), C.POINTER(C.c_long)]),
+    "moao_serve_submit": (i32, [vp, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "moao_serve_poll": (i32, [vp, C.c_longlong, C.POINTER(RequestResult)]),
+    "moao_serve_wait": (i32, [vp, C.c_longlong, C.c_double, C.POINTER(RequestResult)]),
+    "moao_serve_cancel": (i32, [vp, C.c_longlong]),
+    "moao_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
+    "moao_server_destroy": (None, [vp]),
     "moao_fits_read_f64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
     "moao_fits_read_i64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
     "moao_fits_write_f64": (i32, [C.c_char_p, C.c_long, C.c_long, vp]),

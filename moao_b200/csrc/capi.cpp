@@ -332,14 +332,7 @@ void moao_ctx_destroy(moao_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (auto& kv : c->geom) kv.second.buf.release();
-  c->ws_w.release();
-  c->ws_dinv.release();
-  c->ws_info.release();
-  c->ws_tmp.release();
-  for (moao::DevBuf* b : {&c->mx_a32, &c->mx_lr, &c->mx_lc, &c->mx_t32, &c->mx_w1, &c->mx_w2,
-                          &c->mx_x, &c->mx_r64, &c->mx_e64, &c->mx_qa, &c->mx_qb, &c->mx_ea,
-                          &c->mx_fb, &c->mx_colmax, &c->mx_norm})
-    b->release();
+  for (moao::DevBuf* b : c->workspaces()) b->release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& p : c->pending) {

@@ -51,6 +51,7 @@ struct moao_ctx {
   long long launches = 0;
   int nb = 256;  // outer panel width of the blocked factorisation
   moao_prec host_prec = MOAO_PREC_FP64;  // precision of moao_reconstructor_host
+  bool keep_cmm = false;  // mixed path: leave Cmm as given (no factor written back)
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
   moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
@@ -79,6 +80,20 @@ struct moao_ctx {
   };
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> event_pool;
+
+  // Every workspace buffer of the context (not the geometry caches).
+  std::vector<moao::DevBuf*> workspaces() {
+    return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
+            &mx_w1, &mx_w2,   &mx_x,    &mx_r64, &mx_e64, &mx_qa,  &mx_qb,    &mx_ea,
+            &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv};
+  }
+  // Device bytes held by the workspaces and the geometry caches.
+  size_t bytes_held() {
+    size_t b = 0;
+    for (moao::DevBuf* d : workspaces()) b += d->bytes;
+    for (auto& kv : geom) b += kv.second.buf.bytes;
+    return b;
+  }
 };
 
 namespace moao {
@@ -113,6 +128,17 @@ moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const doub
 // Factor the nb x nb diagonal block A in place (FP64) and write its inverse into D.
 moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long ldd, long nb,
                             long col0, int* d_info, double* W);
+// Device bytes of the mixed path's workspace for nmeas n, nmeasts m, panel nb,
+// nsl bf16 slices, ns int8 slices and nranges declared offset ranges.
+struct MixedSizes {
+  size_t a32 = 0, lr = 0, t32 = 0, w = 0, x = 0, r64 = 0, qa = 0, qb = 0, ea = 0, fb = 0,
+         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0;
+  size_t total() const {
+    return a32 + 2 * lr + t32 + 2 * w + x + 2 * r64 + qa + qb + ea + fb + colmax + norm +
+           2 * dinv + info + offsets;
+  }
+};
+MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges);
 // Mixed-precision reconstructor for one target (see mixed.cpp); reuse = 1 keeps
 // the factorisation of the previous call.
 moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,

@@ -198,6 +198,30 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
 
 }  // namespace
 
+MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
+  const long ldn = round_up(n, 64), ldq = round_up(n, 128);
+  MixedSizes z;
+  z.a32 = sizeof(float) * (size_t)n * n;
+  z.lr = nsl * sizeof(uint16_t) * (size_t)n * ldn;
+  z.t32 = sizeof(float) * (size_t)m * n;
+  z.w = sizeof(double) * (size_t)std::max(n, m) * nb;
+  z.x = nsl * sizeof(uint16_t) * (size_t)std::max(n, m) * nb;
+  z.r64 = sizeof(double) * (size_t)m * n;
+  z.qa = (size_t)ns * m * ldq;
+  z.qb = (size_t)ns * n * ldq;
+  z.ea = sizeof(int) * (size_t)m;
+  z.fb = sizeof(int) * (size_t)n;
+  z.colmax = sizeof(unsigned long long) * (size_t)n;
+  z.norm = sizeof(double) * 2;
+  z.dinv = sizeof(double) * (size_t)std::max(n, 1L) * nb;
+  z.info = 2 * sizeof(int);
+  if (nranges > 0)
+    z.offsets = sizeof(int) * (size_t)n + sizeof(float) * (size_t)128 * n +
+                sizeof(double) * ((size_t)nranges * n + (size_t)std::max(m, (long)nranges) * nranges +
+                                  (size_t)nranges * nranges);
+  return z;
+}
+
 // Adds the helper kernels launched during its lifetime to the context's count.
 struct HelperCount {
   moao_ctx* ctx;
@@ -216,26 +240,26 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   const int ns = ctx->ozaki_slices;
   const long ldx = nb;
   // ---- workspace
-  MOAO_TRY(ctx->mx_a32.ensure(sizeof(float) * (size_t)n * n));
   const int nsl = std::max(2, std::min(kMaxBfSlices, ctx->bf16_slices));
-  MOAO_TRY(ctx->mx_lr.ensure(nsl * sizeof(uint16_t) * (size_t)n * ldn));
-  MOAO_TRY(ctx->mx_lc.ensure(nsl * sizeof(uint16_t) * (size_t)n * ldn));
-  MOAO_TRY(ctx->mx_t32.ensure(sizeof(float) * (size_t)m * n));
-  const size_t wbytes = sizeof(double) * (size_t)std::max(n, m) * nb;
-  MOAO_TRY(ctx->mx_w1.ensure(wbytes));
-  MOAO_TRY(ctx->mx_w2.ensure(wbytes));
-  MOAO_TRY(ctx->mx_x.ensure(nsl * sizeof(uint16_t) * (size_t)std::max(n, m) * ldx));
-  MOAO_TRY(ctx->mx_r64.ensure(sizeof(double) * (size_t)m * n));
-  MOAO_TRY(ctx->mx_e64.ensure(sizeof(double) * (size_t)m * n));
-  MOAO_TRY(ctx->mx_qa.ensure((size_t)ns * m * ldq));
-  MOAO_TRY(ctx->mx_qb.ensure((size_t)ns * n * ldq));
-  MOAO_TRY(ctx->mx_ea.ensure(sizeof(int) * (size_t)m));
-  MOAO_TRY(ctx->mx_fb.ensure(sizeof(int) * (size_t)n));
-  MOAO_TRY(ctx->mx_colmax.ensure(sizeof(unsigned long long) * (size_t)n));
-  MOAO_TRY(ctx->mx_norm.ensure(sizeof(double) * 2));
-  MOAO_TRY(ctx->ws_dinv.ensure(sizeof(double) * (size_t)n * nb));
-  MOAO_TRY(ctx->ws_w.ensure(sizeof(double) * (size_t)std::max(n, 1L) * nb));
-  MOAO_TRY(ctx->ws_info.ensure(2 * sizeof(int)));
+  const MixedSizes z = mixed_sizes(n, m, nb, nsl, ns, ctx->offsets.n);
+  MOAO_TRY(ctx->mx_a32.ensure(z.a32));
+  MOAO_TRY(ctx->mx_lr.ensure(z.lr));
+  MOAO_TRY(ctx->mx_lc.ensure(z.lr));
+  MOAO_TRY(ctx->mx_t32.ensure(z.t32));
+  MOAO_TRY(ctx->mx_w1.ensure(z.w));
+  MOAO_TRY(ctx->mx_w2.ensure(z.w));
+  MOAO_TRY(ctx->mx_x.ensure(z.x));
+  MOAO_TRY(ctx->mx_r64.ensure(z.r64));
+  MOAO_TRY(ctx->mx_e64.ensure(z.r64));
+  MOAO_TRY(ctx->mx_qa.ensure(z.qa));
+  MOAO_TRY(ctx->mx_qb.ensure(z.qb));
+  MOAO_TRY(ctx->mx_ea.ensure(z.ea));
+  MOAO_TRY(ctx->mx_fb.ensure(z.fb));
+  MOAO_TRY(ctx->mx_colmax.ensure(z.colmax));
+  MOAO_TRY(ctx->mx_norm.ensure(z.norm));
+  MOAO_TRY(ctx->ws_dinv.ensure(z.dinv));
+  MOAO_TRY(ctx->ws_w.ensure(z.dinv));
+  MOAO_TRY(ctx->ws_info.ensure(z.info));
   float* A32 = ctx->mx_a32.as<float>();
   uint16_t* lr = ctx->mx_lr.as<uint16_t>();
   uint16_t* lc = ctx->mx_lc.as<uint16_t>();

@@ -141,7 +141,7 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
       MOAO_TRY(reconstructor_mixed(ctx, nmeas, nmeasts, d_Cmm, ldCmm,
                                    d_Ctm + nmeas * nmeasts * g, ldCtm, g > 0, r));
     }
-    MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
+    if (!ctx->keep_cmm) MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
     MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return MOAO_OK;
   }
