@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--config", default="elt", choices=["elt", "small"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--serving", action="store_true",
+                   help="serving-loop benchmark (Poisson arrivals, p50/p99) instead of the build loop")
+    p.add_argument("--serve-requests", type=int, default=24)
+    p.add_argument("--serve-slots", type=int, default=3)
     p.add_argument("--no-compare", action="store_true",
                    help="mixed path: skip timing the FP64 path beside it")
     return p.parse_args()
@@ -216,8 +220,132 @@ def read_traffic_ratio(name):
     return None
 
 
+# ----------------------------------------------------------------------------- serving
+SERVING_METRIC = "serving: reconstructor requests/s (R + Cvv + 512^2 PSF each) and p50/p99 latency"
+
+
+def serving_main(args):
+    """Poisson-arrival reconstructor requests on the serving loop (mixed path,
+    several slots) against the same requests run back to back on the FP64 path
+    with one slot. Sizes are log-uniform in nmeas (ELT geometry at several grid
+    sizes), each request has its own seeded 35-layer profile (exp(-h/5 km) x
+    LogNormal(0, 0.2) fractions, r0 0.129 m, L0 25 m) and asks for R, Cvv and
+    the PSF on the truth direction."""
+    import numpy as np
+    import torch
+    from moao_b200 import inputs as I
+    from moao_b200 import params as P
+    import moao_b200 as M
+    from moao_b200.serve import Server
+
+    torch.cuda.init()
+    rng = np.random.default_rng(2024)
+    nssps = [10, 14, 20, 28, 40, 52, 64]
+    systems = []
+    for nssp in nssps:
+        sp, ap = P.config_elt() if nssp == 64 else P.config_scaled(nssp, 35)
+        d = tempfile.mkdtemp(prefix=f"moao_serve_{nssp}_")
+        P.write_system(d, sp, ap)
+        x = I.intersample_inputs(nssp, sp.diam, sp.obs)
+        systems.append(dict(nssp=nssp, dir=d, sys=sp, x=x))
+    n_req = args.serve_requests
+
+    def profile(r):
+        h = np.linspace(0.0, 20000.0, 35)
+        f = np.exp(-h / 5000.0) * r.lognormal(0.0, 0.2, 35)
+        f /= f.sum()
+        return f * 0.129 ** (-5.0 / 3.0), h, np.full(35, 25.0)
+
+    def make_server(slots):
+        srv = Server(device=0, slots=slots, nb=args.nb)
+        ids, infos = [], []
+        for y in systems:
+            sf, af = os.path.join(y["dir"], "sys-params.txt"), os.path.join(y["dir"], "prof-1-atmos-night0.txt")
+            nts = M.Tomo(sf, af).getNMeasTS()
+            Dx = I.make_dx(y["x"].nact, nts, seed=y["nssp"])
+            sid = srv.add_system(sf, af, Dx=Dx, idx=y["x"].idx, abs2fi=y["x"].abs2fi, otf=y["x"].otf)
+            ids.append(sid)
+            infos.append(srv.system_info(sid))
+        return srv, ids, infos
+
+    # request list: log-uniform nmeas in [1000, 48000], nearest grid size
+    srv, ids, infos = make_server(1)
+    logn = np.log([i["nmeas"] for i in infos])
+    reqs = []
+    for k in range(n_req):
+        target = rng.uniform(np.log(1000.0), np.log(48000.0))
+        j = int(np.argmin(np.abs(logn - target)))
+        reqs.append((j, profile(np.random.default_rng(1000 + k))))
+
+    def submit(srv, ids, infos, j, prof, prec):
+        i = infos[j]
+        R = np.empty(i["nmeas"] * i["nmeasts"])
+        Cvv = np.empty(i["nact"] ** 2)
+        psf = np.empty(i["psf_n"] ** 2)
+        return srv.submit(ids[j], *prof, prec=prec, R=R, Cvv=Cvv, psf=psf)
+
+    def closed_loop(srv, ids, infos, prec, parallel):
+        # warm the slots once per system size
+        for j in range(len(ids)):
+            srv.wait(submit(srv, ids, infos, j, reqs[0][1], prec))
+        t0 = time.perf_counter()
+        if parallel:
+            rid = [submit(srv, ids, infos, j, p, prec) for j, p in reqs]
+            res = [srv.wait(r) for r in rid]
+        else:
+            res = [srv.wait(submit(srv, ids, infos, j, p, prec)) for j, p in reqs]
+        wall = time.perf_counter() - t0
+        lat = [r["latency_ms"] for r in res]
+        assert all(r["status"] == 0 for r in res), [r for r in res if r["status"]][:1]
+        return {"requests_per_s": len(res) / wall, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall}
+
+    base = closed_loop(srv, ids, infos, "fp64", parallel=False)
+    srv.close()
+    srv, ids, infos = make_server(args.serve_slots)
+    sat = closed_loop(srv, ids, infos, "mixed", parallel=True)
+    sweep = []
+    for frac in (0.5, 0.75, 0.9):
+        lam = frac * sat["requests_per_s"]
+        arr = np.cumsum(np.random.default_rng(int(frac * 100)).exponential(1.0 / lam, n_req))
+        t0 = time.perf_counter()
+        rid = []
+        for (j, p), ta in zip(reqs, arr):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            rid.append(submit(srv, ids, infos, j, p, "mixed"))
+        res = [srv.wait(r) for r in rid]
+        wall = time.perf_counter() - t0
+        lat = [r["latency_ms"] for r in res]
+        sweep.append({"rate_requests_per_s": lam, "throughput_requests_per_s": len(res) / wall,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "mean_queue_ms": float(np.mean([r["queue_ms"] for r in res]))})
+    st = srv.stats()
+    srv.close()
+    sustained = max((x for x in sweep if x["throughput_requests_per_s"] >= 0.9 * x["rate_requests_per_s"]),
+                    key=lambda x: x["rate_requests_per_s"], default=sweep[0])
+    line = {
+        "metric": SERVING_METRIC, "value": sustained["throughput_requests_per_s"],
+        "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
+        "latency_ms": {"p50": sustained["p50_ms"], "p99": sustained["p99_ms"],
+                       "at_rate_requests_per_s": sustained["rate_requests_per_s"]},
+        "config": {"workload": (f"{n_req} requests, nmeas log-uniform 1000-48000 over grids "
+                                f"{nssps} (ELT geometry), 35-layer seeded profiles, R + Cvv + PSF each"),
+                   "slots": args.serve_slots, "path": "mixed", "panel_nb": args.nb},
+        "saturation_closed_loop": sat, "sweep": sweep,
+        "baseline_sequential_fp64": base,
+        "speedup_vs_sequential_fp64": sat["requests_per_s"] / base["requests_per_s"],
+        "server_stats": st, "data": "synthetic",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.serving:
+        return serving_main(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
