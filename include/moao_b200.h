@@ -310,6 +310,44 @@ moao_status moao_server_get_stats(moao_server* s, moao_server_stats* out);
 /* Cancels queued requests, lets running ones finish, frees everything. */
 void moao_server_destroy(moao_server* s);
 
+/* ---- Batched instances: many independent reconstructor builds (covariance
+ * generation of Cmm and Ctm from each instance's tomo, factorisation, solves)
+ * captured as one CUDA graph over several streams and launched once. Each
+ * stream keeps one Cmm / Ctm pair and workspace sized for its largest
+ * instance, so device memory is streams x largest, not the sum. Instances run
+ * longest first onto the least-loaded stream. No reference counterpart. */
+typedef struct {
+  const moao_tomo* tomo;  /* system, profile and target of this instance */
+  double* d_R;            /* device out: nmeasts x nmeas (ld nmeasts), or NULL */
+  int nb;                 /* panel width (tile size); 0: tuned or default */
+  /* outputs */
+  int status;             /* MOAO_OK, MOAO_ERR_NOT_SPD, MOAO_ERR_TIMEOUT, MOAO_ERR_BAD_ARG */
+  int info;               /* failing Cholesky column */
+  int nb_used, stream;
+} moao_batch_item;
+typedef struct {
+  moao_prec prec;         /* mixed: fixed max_refine corrections, no residual checks */
+  int streams;            /* 0: tuned (default 4) */
+  /* outputs */
+  double ms_device;       /* device time of the graph launch */
+  double ms_build;        /* host time to capture and instantiate the graph */
+  long long graph_nodes;
+  int streams_used, failed;
+  double device_gb;       /* device bytes of the streams' buffers and workspaces */
+} moao_batch_opts;
+moao_status moao_batch_reconstructors(moao_ctx* ctx, int count, moao_batch_item* items,
+                                      moao_batch_opts* opts);
+/* Autotuner: for each nmeas size class (< 2k, 4k, 8k, 16k, 32k, larger) present
+ * in the samples, the panel width (from nb_candidates, default 128, 256, 384,
+ * 512) with the shortest measured single-instance build, then the stream count
+ * (2, 4, 8) with the shortest batch of all samples; stored on the context. */
+moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samples,
+                          moao_prec prec, const int* nb_candidates, int ncand);
+/* Tuned (or default) panel width per size class (6 entries) and stream count. */
+moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, int* streams);
+moao_status moao_tuning_save(moao_ctx* ctx, const char* path);
+moao_status moao_tuning_load(moao_ctx* ctx, const char* path);
+
 /* ---- FITS images (primary HDU, 1-D or 2-D), the file format of the
  * reference's inputs and check outputs (common/io/fits.cpp;
  * common/tomo_struct/intersample.cpp:208-300 reads idx, abs2fi, otftel).

@@ -65,6 +65,17 @@ class ServerStats(C.Structure):
                 ("peak_admitted_gb", C.c_double), ("budget_gb", C.c_double)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("tomo", vp), ("d_R", vp), ("nb", i32), ("status", i32), ("info", i32),
+                ("nb_used", i32), ("stream", i32)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("prec", i32), ("streams", i32), ("ms_device", C.c_double),
+                ("ms_build", C.c_double), ("graph_nodes", C.c_longlong),
+                ("streams_used", i32), ("failed", i32), ("device_gb", C.c_double)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "moao_status_string": (C.c_char_p, [i32]),
@@ -99,6 +110,11 @@ SIGNATURES = {
     "moao_serve_cancel": (i32, [vp, C.c_longlong]),
     "moao_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
     "moao_server_destroy": (None, [vp]),
+    "moao_batch_reconstructors": (i32, [vp, i32, vp, C.POINTER(BatchOpts)]),
+    "moao_autotune": (i32, [vp, i32, vp, i32, vp, i32]),
+    "moao_tuning_get": (i32, [vp, i32, vp, C.POINTER(i32)]),
+    "moao_tuning_save": (i32, [vp, C.c_char_p]),
+    "moao_tuning_load": (i32, [vp, C.c_char_p]),
     "moao_fits_read_f64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
     "moao_fits_read_i64": (i32, [C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_long), vp, C.c_long]),
     "moao_fits_write_f64": (i32, [C.c_char_p, C.c_long, C.c_long, vp]),

@@ -1,0 +1,474 @@
+// Batched instances: many independent reconstructor builds (covariance
+// generation, factorisation, solves) captured as one CUDA graph and launched
+// once.
+//
+// Instances are assigned to S streams, longest first onto the least-loaded
+// stream (estimated cost n^3/3 + n^2 m plus the covariance term); each stream
+// has its own context (workspaces sized before capture for the largest
+// instance it runs) and reuses one Cmm / Ctm pair for its instances in stream
+// order, so device memory is S x (largest instance), not the sum. Geometry
+// tables are uploaded before capture. Inside the capture nothing waits for the
+// device: each instance's failure flags are copied to a status array read after
+// the graph ran. The graph is one launch however many instances it holds; small
+// instances, whose kernels are short, overlap with each other and with the
+// large ones on the other streams.
+//
+// Autotuner: per nmeas size class and precision, the panel width (the tile
+// size of the blocked factorisation) with the shortest measured build, and
+// the number of streams with the shortest measured batch; kept on the context
+// and saved to / loaded from a text file.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "moao_b200.h"
+
+namespace moao {
+namespace {
+
+constexpr int kClasses = 6;  // nmeas < 2k, 4k, 8k, 16k, 32k, larger
+
+int size_class(long n) {
+  int c = 0;
+  for (long lim = 2048; c < kClasses - 1 && n >= lim; lim *= 2) ++c;
+  return c;
+}
+
+struct TuneEntry {
+  int nb = 0;  // 0: not tuned
+};
+
+}  // namespace
+}  // namespace moao
+
+// Tuning table kept per context (allocated on first use).
+struct moao_tuning {
+  moao::TuneEntry entry[2][moao::kClasses];  // [prec][class]
+  int streams[2] = {0, 0};
+};
+
+namespace moao {
+namespace {
+
+std::map<const moao_ctx*, moao_tuning>& tuning_tables() {
+  static std::map<const moao_ctx*, moao_tuning> t;
+  return t;
+}
+std::mutex& tuning_mutex() {
+  static std::mutex m;
+  return m;
+}
+
+int default_nb(long n) { return n < 4096 ? 128 : 256; }
+
+int tuned_nb(const moao_ctx* ctx, moao_prec prec, long n) {
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  auto it = tuning_tables().find(ctx);
+  if (it != tuning_tables().end()) {
+    const int nb = it->second.entry[prec == MOAO_PREC_MIXED][size_class(n)].nb;
+    if (nb > 0) return nb;
+  }
+  return default_nb(n);
+}
+
+int tuned_streams(const moao_ctx* ctx, moao_prec prec) {
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  auto it = tuning_tables().find(ctx);
+  if (it != tuning_tables().end() && it->second.streams[prec == MOAO_PREC_MIXED] > 0)
+    return it->second.streams[prec == MOAO_PREC_MIXED];
+  return 4;
+}
+
+struct Inst {
+  int item;
+  long n, m;
+  int nb;
+  double cost;
+  const DevGeometry* g;
+  int stream;
+};
+
+// Builds one instance on sub-context sc (stream sc->stream): covariances into
+// Cmm / Ctm, factorisation and solves, R copied to the caller, flags to status.
+moao_status enqueue_instance(moao_ctx* sc, const moao_tomo* tomo, const Inst& in, moao_prec prec,
+                             double* Cmm, double* Ctm, double* d_R, int* status) {
+  cudaStream_t s = sc->stream;
+  const long n = in.n, m = in.m;
+  sc->nb = in.nb;
+  MOAO_TRY(launch_matcov(*in.g, Cmm, (int)n, (int)n, 0, 0, (int)n, 1, s, &sc->launches));
+  MOAO_TRY(launch_matcov(*in.g, Ctm, (int)m, (int)n, 0, 0, (int)m, 3, s, &sc->launches));
+  int* d_info = sc->ws_info.as<int>();
+  if (prec == MOAO_PREC_MIXED) {
+    MOAO_TRY(moao_ctx_set_offsets_from_tomo(sc, tomo));
+    moao_solve_report rep{};
+    MOAO_TRY(reconstructor_mixed(sc, n, m, Cmm, n, Ctm, m, false, &rep));
+  } else {
+    MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 3 * sizeof(int), s));
+    MOAO_TRY(potrf_f64(sc, Cmm, n, n, sc->ws_dinv.as<double>(), d_info));
+    MOAO_TRY(solve_right_f64(sc, Cmm, n, n, sc->ws_dinv.as<double>(), Ctm, m, m));
+  }
+  MOAO_CUDA_TRY(cudaMemcpyAsync(status, d_info, 3 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  if (d_R)
+    MOAO_CUDA_TRY(cudaMemcpyAsync(d_R, Ctm, sizeof(double) * (size_t)m * n,
+                                  cudaMemcpyDeviceToDevice, s));
+  return MOAO_OK;
+}
+
+// Sub-contexts of a context for batched work (created on first use).
+std::vector<moao_ctx*>& sub_contexts(moao_ctx* ctx) {
+  static std::map<const moao_ctx*, std::vector<moao_ctx*>> subs;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  return subs[ctx];
+}
+
+}  // namespace
+
+void release_batch_state(moao_ctx* ctx) {
+  {
+    std::lock_guard<std::mutex> lk(tuning_mutex());
+    tuning_tables().erase(ctx);
+  }
+  std::vector<moao_ctx*>& v = sub_contexts(ctx);
+  for (moao_ctx* c : v) moao_ctx_destroy(c);
+  v.clear();
+}
+
+namespace {
+
+moao_status ensure_subs(moao_ctx* ctx, int S) {
+  std::vector<moao_ctx*>& v = sub_contexts(ctx);
+  while ((int)v.size() < S) {
+    moao_ctx* c = nullptr;
+    MOAO_TRY(moao_ctx_create(ctx->device, &c));
+    v.push_back(c);
+  }
+  return MOAO_OK;
+}
+
+moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_batch_opts* o) {
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  const moao_prec prec = o->prec;
+  std::vector<Inst> inst;
+  for (int i = 0; i < count; ++i) {
+    const Tomo_struct<double>& t = items[i].tomo->t;
+    Inst in;
+    in.item = i;
+    in.n = t.getNMeas();
+    in.m = t.getNMeasTS();
+    in.nb = items[i].nb > 0 ? items[i].nb : tuned_nb(ctx, prec, in.n);
+    if (in.nb % 64 || in.nb < 64 || in.nb > 2048)
+      return set_error(MOAO_ERR_BAD_ARG, "batch: panel width must be a multiple of 64 in [64, 2048]");
+    const double n = (double)in.n, m = (double)in.m;
+    in.cost = n * n * n / 3 + n * n * m + 40.0 * t.atm.nLayer * n * (n / 2 + m);
+    MOAO_TRY(device_geometry(ctx, items[i].tomo, &in.g));
+    in.stream = 0;
+    inst.push_back(in);
+  }
+  int S = o->streams > 0 ? o->streams : tuned_streams(ctx, prec);
+  S = std::max(1, std::min({S, count, 16}));
+  // longest first onto the least-loaded stream
+  std::vector<int> order(count);
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].cost > inst[b].cost; });
+  std::vector<double> load(S, 0.0);
+  std::vector<std::vector<int>> per(S);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    inst[i].stream = k;
+    load[k] += inst[i].cost;
+    per[k].push_back(i);
+  }
+  // memory: per stream its largest Cmm / Ctm pair and workspace
+  MOAO_TRY(ensure_subs(ctx, S));
+  std::vector<moao_ctx*>& subs = sub_contexts(ctx);
+  std::vector<DevBuf> cmm(S), ctm(S);
+  DevBuf status;
+  // DevBuf frees nothing by itself: release the batch's own buffers on every exit
+  struct Release {
+    std::vector<DevBuf>& a;
+    std::vector<DevBuf>& b;
+    DevBuf& c;
+    ~Release() {
+      for (DevBuf& x : a) x.release();
+      for (DevBuf& x : b) x.release();
+      c.release();
+    }
+  } release_guard{cmm, ctm, status};
+  size_t total = 0;
+  for (int k = 0; k < S; ++k) {
+    moao_ctx* sc = subs[k];
+    sc->graph_mode = (prec == MOAO_PREC_MIXED);
+    sc->timing = false;
+    long nmax = 0, mmax = 0;
+    size_t ws = 0;
+    for (int i : per[k]) {
+      nmax = std::max(nmax, inst[i].n);
+      mmax = std::max(mmax, inst[i].m);
+      const Inst& in = inst[i];
+      if (prec == MOAO_PREC_MIXED) {
+        const Tomo_struct<double>& t = items[in.item].tomo->t;
+        const int nro = t.sys.lgsCst > 0 ? 2 * t.sys.nLgs : 0;
+        const MixedSizes z = mixed_sizes(in.n, in.m, in.nb, std::max(2, std::min(kMaxBfSlices, sc->bf16_slices)),
+                                         sc->ozaki_slices, nro);
+        // size every workspace buffer for the largest instance of this stream
+        MOAO_TRY(sc->mx_a32.ensure(z.a32));
+        MOAO_TRY(sc->mx_lr.ensure(z.lr));
+        MOAO_TRY(sc->mx_lc.ensure(z.lr));
+        MOAO_TRY(sc->mx_t32.ensure(z.t32));
+        MOAO_TRY(sc->mx_w1.ensure(z.w));
+        MOAO_TRY(sc->mx_w2.ensure(z.w));
+        MOAO_TRY(sc->mx_x.ensure(z.x));
+        MOAO_TRY(sc->mx_r64.ensure(z.r64));
+        MOAO_TRY(sc->mx_e64.ensure(z.r64));
+        MOAO_TRY(sc->mx_qa.ensure(z.qa));
+        MOAO_TRY(sc->mx_qb.ensure(z.qb));
+        MOAO_TRY(sc->mx_ea.ensure(z.ea));
+        MOAO_TRY(sc->mx_fb.ensure(z.fb));
+        MOAO_TRY(sc->mx_colmax.ensure(z.colmax));
+        MOAO_TRY(sc->mx_norm.ensure(z.norm));
+        MOAO_TRY(sc->ws_dinv.ensure(z.dinv));
+        MOAO_TRY(sc->ws_w.ensure(z.dinv));
+        if (nro > 0) {
+          MOAO_TRY(sc->mx_rid.ensure(sizeof(int) * (size_t)in.n));
+          MOAO_TRY(sc->mx_y.ensure(sizeof(float) * (size_t)128 * in.n));
+          MOAO_TRY(sc->mx_y2.ensure(sizeof(double) * (size_t)nro * in.n));
+          MOAO_TRY(sc->mx_zu.ensure(sizeof(double) * (size_t)std::max(in.m, (long)nro) * nro));
+          MOAO_TRY(sc->mx_sinv.ensure(sizeof(double) * (size_t)nro * nro));
+        }
+      } else {
+        MOAO_TRY(sc->ws_dinv.ensure(sizeof(double) * (size_t)in.n * in.nb));
+        MOAO_TRY(sc->ws_w.ensure(sizeof(double) * (size_t)std::max(in.n, in.m) * in.nb));
+      }
+      ws = sc->bytes_held();
+    }
+    MOAO_TRY(sc->ws_info.ensure(3 * sizeof(int)));
+    MOAO_TRY(cmm[k].ensure(sizeof(double) * (size_t)nmax * nmax));
+    MOAO_TRY(ctm[k].ensure(sizeof(double) * (size_t)mmax * nmax));
+    total += ws + cmm[k].bytes + ctm[k].bytes;
+  }
+  MOAO_TRY(status.ensure(3 * sizeof(int) * (size_t)count));
+  MOAO_CUDA_TRY(cudaMemsetAsync(status.p, 0, 3 * sizeof(int) * (size_t)count, ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+
+  // ---- capture: fork S streams from the context's stream, join at the end
+  std::vector<cudaEvent_t> ev(S + 1);
+  for (auto& e : ev) MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  auto destroy_events = [&] {
+    for (auto& e : ev) cudaEventDestroy(e);
+  };
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  const auto host0 = std::chrono::steady_clock::now();
+  cudaStream_t s0 = ctx->stream;
+  cudaGraph_t graph = nullptr;
+  moao_status st = MOAO_OK;
+  cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) ce = cudaEventRecord(ev[S], s0);
+  for (int k = 0; k < S && ce == cudaSuccess && st == MOAO_OK; ++k) {
+    moao_ctx* sc = subs[k];
+    ce = cudaStreamWaitEvent(sc->stream, ev[S], 0);
+    for (int i : per[k]) {
+      if (ce != cudaSuccess || st != MOAO_OK) break;
+      const Inst& in = inst[i];
+      st = enqueue_instance(sc, items[in.item].tomo, in, prec, cmm[k].as<double>(),
+                            ctm[k].as<double>(), items[in.item].d_R,
+                            status.as<int>() + 3 * (size_t)in.item);
+    }
+    if (ce == cudaSuccess && st == MOAO_OK) ce = cudaEventRecord(ev[k], sc->stream);
+    if (ce == cudaSuccess && st == MOAO_OK) ce = cudaStreamWaitEvent(s0, ev[k], 0);
+  }
+  cudaError_t ce_end = cudaStreamEndCapture(s0, &graph);
+  for (int k = 0; k < S; ++k) subs[k]->graph_mode = false;
+  if (st != MOAO_OK || ce != cudaSuccess || ce_end != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    destroy_events();
+    cudaGetLastError();
+    if (st != MOAO_OK) return st;
+    return set_error(MOAO_ERR_CUDA, std::string("batch capture: ") +
+                                        cudaGetErrorString(ce != cudaSuccess ? ce : ce_end));
+  }
+  cudaGraphExec_t exec = nullptr;
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  size_t nodes = 0;
+  cudaGraphGetNodes(graph, nullptr, &nodes);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) {
+    destroy_events();
+    return set_error(MOAO_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ce));
+  }
+  const double build_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();
+  cudaEventRecord(t0, s0);
+  ce = cudaGraphLaunch(exec, s0);
+  cudaEventRecord(t1, s0);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s0);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaGraphExecDestroy(exec);
+  destroy_events();
+  if (ce != cudaSuccess) return set_error(MOAO_ERR_CUDA, std::string("batch graph launch: ") + cudaGetErrorString(ce));
+  std::vector<int> hs(3 * (size_t)count);
+  MOAO_CUDA_TRY(cudaMemcpy(hs.data(), status.p, hs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  int failed = 0;
+  for (const Inst& in : inst) {
+    moao_batch_item& it = items[in.item];
+    const int* f = &hs[3 * (size_t)in.item];
+    it.info = f[0];
+    it.nb_used = in.nb;
+    it.stream = in.stream;
+    it.status = f[1] ? MOAO_ERR_TIMEOUT : (f[2] ? MOAO_ERR_BAD_ARG : (f[0] ? MOAO_ERR_NOT_SPD : MOAO_OK));
+    failed += it.status != MOAO_OK;
+  }
+  o->ms_device = ms;
+  o->ms_build = build_ms;
+  o->graph_nodes = (long long)nodes;
+  o->streams_used = S;
+  o->device_gb = total / 1e9;
+  o->failed = failed;
+  return MOAO_OK;
+}
+
+}  // namespace
+}  // namespace moao
+
+using namespace moao;
+
+extern "C" {
+
+moao_status moao_batch_reconstructors(moao_ctx* ctx, int count, moao_batch_item* items,
+                                      moao_batch_opts* opts) {
+  if (!ctx || count < 0 || (count > 0 && !items) || !opts)
+    return set_error(MOAO_ERR_BAD_ARG, "batch: null argument");
+  if (opts->prec != MOAO_PREC_FP64 && opts->prec != MOAO_PREC_MIXED)
+    return set_error(MOAO_ERR_BAD_ARG, "batch: precision");
+  for (int i = 0; i < count; ++i)
+    if (!items[i].tomo) return set_error(MOAO_ERR_BAD_ARG, "batch: item without tomo");
+  if (count == 0) return MOAO_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return run_batch(ctx, count, items, opts);
+}
+
+moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samples,
+                          moao_prec prec, const int* nb_candidates, int ncand) {
+  if (!ctx || count <= 0 || !samples || (ncand > 0 && !nb_candidates))
+    return set_error(MOAO_ERR_BAD_ARG, "autotune: bad arguments");
+  static const int def[] = {128, 256, 384, 512};
+  const int* cand = ncand > 0 ? nb_candidates : def;
+  const int nc = ncand > 0 ? ncand : 4;
+  const int p = prec == MOAO_PREC_MIXED;
+  std::vector<double> best_ms(kClasses, 1e300);
+  std::vector<int> best_nb(kClasses, 0);
+  for (int i = 0; i < count; ++i) {
+    const long n = samples[i]->t.getNMeas();
+    const int c = size_class(n);
+    for (int j = 0; j < nc; ++j) {
+      if (cand[j] > n) continue;
+      moao_batch_item it{};
+      it.tomo = samples[i];
+      it.nb = cand[j];
+      moao_batch_opts o{};
+      o.prec = prec;
+      o.streams = 1;
+      MOAO_TRY(moao_batch_reconstructors(ctx, 1, &it, &o));  // warm-up
+      MOAO_TRY(moao_batch_reconstructors(ctx, 1, &it, &o));
+      if (o.ms_device < best_ms[c]) {
+        best_ms[c] = o.ms_device;
+        best_nb[c] = cand[j];
+      }
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(tuning_mutex());
+    moao_tuning& t = tuning_tables()[ctx];
+    for (int c = 0; c < kClasses; ++c)
+      if (best_nb[c] > 0) t.entry[p][c].nb = best_nb[c];
+  }
+  // stream count: the whole sample set as one batch
+  std::vector<moao_batch_item> items(count);
+  double best = 1e300;
+  int bestS = 4;
+  for (int S : {2, 4, 8}) {
+    if (S > count * 2) break;
+    for (int i = 0; i < count; ++i) {
+      items[i] = moao_batch_item{};
+      items[i].tomo = samples[i];
+    }
+    moao_batch_opts o{};
+    o.prec = prec;
+    o.streams = S;
+    MOAO_TRY(moao_batch_reconstructors(ctx, count, items.data(), &o));
+    if (o.ms_device < best) {
+      best = o.ms_device;
+      bestS = S;
+    }
+  }
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  tuning_tables()[ctx].streams[p] = bestS;
+  return MOAO_OK;
+}
+
+moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, int* streams) {
+  if (!ctx || !nb_per_class || !streams) return set_error(MOAO_ERR_BAD_ARG, "tuning_get: null");
+  const int p = prec == MOAO_PREC_MIXED;
+  for (int c = 0; c < kClasses; ++c) {
+    const long n = c == 0 ? 1024 : (1024L << c);
+    nb_per_class[c] = tuned_nb(ctx, prec, n);
+  }
+  *streams = tuned_streams(ctx, prec);
+  (void)p;
+  return MOAO_OK;
+}
+
+moao_status moao_tuning_save(moao_ctx* ctx, const char* path) {
+  if (!ctx || !path) return set_error(MOAO_ERR_BAD_ARG, "tuning_save: null");
+  std::ofstream f(path);
+  if (!f) return set_error(MOAO_ERR_IO, std::string("tuning_save: cannot create ") + path);
+  f << "# moao_b200 tuning: prec class nb / prec streams\n";
+  for (int p = 0; p < 2; ++p) {
+    int nbs[kClasses], S = 0;
+    moao_tuning_get(ctx, p ? MOAO_PREC_MIXED : MOAO_PREC_FP64, nbs, &S);
+    for (int c = 0; c < kClasses; ++c) f << "nb " << p << " " << c << " " << nbs[c] << "\n";
+    f << "streams " << p << " " << S << "\n";
+  }
+  return f ? MOAO_OK : set_error(MOAO_ERR_IO, "tuning_save: write failed");
+}
+
+moao_status moao_tuning_load(moao_ctx* ctx, const char* path) {
+  if (!ctx || !path) return set_error(MOAO_ERR_BAD_ARG, "tuning_load: null");
+  std::ifstream f(path);
+  if (!f) return set_error(MOAO_ERR_IO, std::string("tuning_load: cannot open ") + path);
+  moao_tuning t;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream is(line);
+    std::string key;
+    int p = 0, c = 0, v = 0;
+    is >> key;
+    if (key == "nb" && (is >> p >> c >> v) && p >= 0 && p < 2 && c >= 0 && c < kClasses &&
+        v % 64 == 0 && v >= 64 && v <= 2048)
+      t.entry[p][c].nb = v;
+    else if (key == "streams" && (is >> p >> v) && p >= 0 && p < 2 && v >= 1 && v <= 16)
+      t.streams[p] = v;
+    else
+      return set_error(MOAO_ERR_IO, "tuning_load: bad line: " + line);
+  }
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  tuning_tables()[ctx] = t;
+  return MOAO_OK;
+}
+
+}  // extern "C"

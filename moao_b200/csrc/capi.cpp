@@ -329,6 +329,7 @@ moao_status moao_ctx_create(int device, moao_ctx** out) {
 
 void moao_ctx_destroy(moao_ctx* c) {
   if (!c) return;
+  release_batch_state(c);
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (auto& kv : c->geom) kv.second.buf.release();

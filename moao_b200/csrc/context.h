@@ -52,6 +52,7 @@ struct moao_ctx {
   int nb = 256;  // outer panel width of the blocked factorisation
   moao_prec host_prec = MOAO_PREC_FP64;  // precision of moao_reconstructor_host
   bool keep_cmm = false;  // mixed path: leave Cmm as given (no factor written back)
+  bool graph_mode = false;  // mixed path under stream capture: no host waits or reads
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
   moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
@@ -143,6 +144,8 @@ MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges);
 // the factorisation of the previous call.
 moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,
                                 double* Ctm, long ldCtm, bool reuse, moao_solve_report* rep);
+// Destroys the batch engine's sub-contexts and tuning table of ctx.
+void release_batch_state(moao_ctx* ctx);
 // Writes the mixed factorisation's (FP32) factor into the lower triangle of Cmm.
 moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm);
 // R = B * L^-T * L^-1 in place on B (m x n, ldb) using the factor and dinv.

@@ -80,39 +80,6 @@ struct Maps {
 
 constexpr long kYRows = 128;  // rows of the offset-indicator solve (one tile)
 
-// Inverse of a small dense matrix (row-major k x k) by Gauss-Jordan elimination
-// with partial pivoting; false if singular.
-bool invert_small(std::vector<double>& a, int k) {
-  std::vector<double> inv(k * k, 0.0);
-  for (int i = 0; i < k; ++i) inv[i * k + i] = 1.0;
-  for (int c = 0; c < k; ++c) {
-    int p = c;
-    for (int r = c + 1; r < k; ++r)
-      if (std::fabs(a[r * k + c]) > std::fabs(a[p * k + c])) p = r;
-    if (!(std::fabs(a[p * k + c]) > 0)) return false;
-    if (p != c)
-      for (int j = 0; j < k; ++j) {
-        std::swap(a[p * k + j], a[c * k + j]);
-        std::swap(inv[p * k + j], inv[c * k + j]);
-      }
-    const double d = 1.0 / a[c * k + c];
-    for (int j = 0; j < k; ++j) {
-      a[c * k + j] *= d;
-      inv[c * k + j] *= d;
-    }
-    for (int r = 0; r < k; ++r) {
-      if (r == c) continue;
-      const double f = a[r * k + c];
-      if (f == 0) continue;
-      for (int j = 0; j < k; ++j) {
-        a[r * k + j] -= f * a[c * k + j];
-        inv[r * k + j] -= f * inv[c * k + j];
-      }
-    }
-  }
-  a.swap(inv);
-  return true;
-}
 
 // Products s_i * s_j of bf16 slices kept for a given slice count, smallest
 // first: the tensor core's FP32 accumulation truncates each addition (a bias of
@@ -214,7 +181,7 @@ MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
   z.colmax = sizeof(unsigned long long) * (size_t)n;
   z.norm = sizeof(double) * 2;
   z.dinv = sizeof(double) * (size_t)std::max(n, 1L) * nb;
-  z.info = 2 * sizeof(int);
+  z.info = 3 * sizeof(int);
   if (nranges > 0)
     z.offsets = sizeof(int) * (size_t)n + sizeof(float) * (size_t)128 * n +
                 sizeof(double) * ((size_t)nranges * n + (size_t)std::max(m, (long)nranges) * nranges +
@@ -314,17 +281,15 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   const int csl = std::max(2, std::min(nsl, ctx->corr_slices));
   const Products full = products_for(nsl), corr = products_for(csl);
 
+  // In graph mode (stream capture) nothing here waits for the device or reads
+  // device memory on the host: failures stay in d_info[0..2] for the caller and
+  // refinement runs exactly max_refine corrections.
+  const bool graph = ctx->graph_mode;
   cudaEvent_t* ev = ctx->ev;
-  cudaEventRecord(ev[3], s);
+  if (!graph) cudaEventRecord(ev[3], s);
   if (!reuse || ctx->mx_factored_n != n) {
-    MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 2 * sizeof(int), s));
-    if (nro > 0) {
-      std::vector<int> hrid(n, -1);
-      for (int w = 0; w < nro; ++w)
-        for (int j = off.begin[w]; j < off.end[w]; ++j) hrid[j] = w;
-      // pageable source: the copy is staged before the call returns
-      MOAO_CUDA_TRY(cudaMemcpyAsync(rid, hrid.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    }
+    MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 3 * sizeof(int), s));
+    if (nro > 0) MOAO_TRY(fill_range_ids(rid, n, off, s));
     MOAO_TRY(cvt_lower_minus_offsets(Cmm, ldCmm, A32, n, n, rid, off, s));
     for (long k0 = 0; k0 < n; k0 += nb) {
       const long kb = std::min(nb, n - k0);
@@ -348,15 +313,17 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
                          (int)(kb / 64), full, rest, rest, A32 + (k0 + kb) + (k0 + kb) * n, n,
                          true, err, (double)rest * rest * kb));
     }
-    int info[2] = {0, 0};
-    MOAO_CUDA_TRY(cudaMemcpyAsync(info, d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    MOAO_CUDA_TRY(cudaStreamSynchronize(s));
-    if (info[1]) return set_error(MOAO_ERR_TIMEOUT, "tensor-core update: bounded wait expired");
-    rep->info = info[0];
-    if (info[0]) {
-      ctx->mx_factored_n = -1;
-      return set_error(MOAO_ERR_NOT_SPD, "mixed Cholesky: non-positive pivot at column " +
-                                             std::to_string(info[0]));
+    if (!graph) {
+      int info[2] = {0, 0};
+      MOAO_CUDA_TRY(cudaMemcpyAsync(info, d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+      if (info[1]) return set_error(MOAO_ERR_TIMEOUT, "tensor-core update: bounded wait expired");
+      rep->info = info[0];
+      if (info[0]) {
+        ctx->mx_factored_n = -1;
+        return set_error(MOAO_ERR_NOT_SPD, "mixed Cholesky: non-positive pivot at column " +
+                                               std::to_string(info[0]));
+      }
     }
     // int8 slices of sym(Cmm) for the refinement residual
     MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
@@ -366,23 +333,12 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       MOAO_TRY(fill_range_indicators(Y32, kYRows, n, off, s));
       MOAO_TRY(mixed_solve(ctx, n, kYRows, Y32, dinv, mp.yA, mp, W1, W2, xs, ldx, full, nsl, err));
       MOAO_TRY(range_sums(Y32, kYRows, nro, off, ZU, s));
-      std::vector<double> yu((size_t)nro * nro), a((size_t)nro * nro), sc((size_t)nro * nro);
-      MOAO_CUDA_TRY(cudaMemcpyAsync(yu.data(), ZU, sizeof(double) * nro * nro, cudaMemcpyDeviceToHost, s));
-      MOAO_CUDA_TRY(cudaStreamSynchronize(s));
-      for (int v = 0; v < nro; ++v)
-        for (int w = 0; w < nro; ++w)
-          a[v * nro + w] = yu[(size_t)w * nro + v] + (v == w ? 1.0 / off.value[v] : 0.0);
-      if (!invert_small(a, nro))
-        return set_error(MOAO_ERR_BAD_ARG,
-                         "mixed reconstructor: offsets give a singular capacitance matrix");
-      for (int v = 0; v < nro; ++v)
-        for (int w = 0; w < nro; ++w) sc[(size_t)w * nro + v] = a[v * nro + w];
-      MOAO_CUDA_TRY(cudaMemcpyAsync(Sinv, sc.data(), sizeof(double) * nro * nro, cudaMemcpyHostToDevice, s));
+      MOAO_TRY(capacitance_inverse(ZU, off, Sinv, d_info + 2, s));
       MOAO_TRY(mul_small_left(Sinv, nro, Y32, kYRows, n, Y2, s));
     }
     ctx->mx_factored_n = n;
   }
-  cudaEventRecord(ev[4], s);
+  if (!graph) cudaEventRecord(ev[4], s);
   // ---- solve
   MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
   MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, full, nsl, err));
@@ -392,7 +348,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   } else {
     MOAO_TRY(cvt_f32_to_f64(T32, m, R64, m, m, n, false, s));
   }
-  cudaEventRecord(ev[5], s);
+  if (!graph) cudaEventRecord(ev[5], s);
   // ---- refinement
   TcTensor ta[kMaxOzakiSlices], tb[kMaxOzakiSlices];
   for (int i = 0; i < ns; ++i) {
@@ -401,7 +357,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   }
   double* dnorm = ctx->mx_norm.as<double>();
   double ctm2 = 0, e2 = 0;
-  MOAO_TRY(sumsq(ctx, Ctm, ldCtm, m, n, dnorm, &ctm2));
+  if (!graph) MOAO_TRY(sumsq(ctx, Ctm, ldCtm, m, n, dnorm, &ctm2));
   auto residual = [&]() -> moao_status {
     // E = Ctm - R sym(Cmm) from the int8 slice products
     MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
@@ -442,14 +398,16 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       MOAO_TRY(range_sums(R64, m, m, off, ZU, s));
       MOAO_TRY(subtract_offset_products(E64, m, m, n, ZU, rid, off, s));
     }
-    MOAO_TRY(sumsq(ctx, E64, m, m, n, dnorm, &e2));
-    rep->refine_resid = std::sqrt(e2 / std::max(ctm2, 1e-300));
+    if (!graph) {
+      MOAO_TRY(sumsq(ctx, E64, m, m, n, dnorm, &e2));
+      rep->refine_resid = std::sqrt(e2 / std::max(ctm2, 1e-300));
+    }
     return MOAO_OK;
   };
   int steps = 0;
   for (; steps < ctx->max_refine; ++steps) {
     MOAO_TRY(residual());
-    if (rep->refine_resid <= ctx->refine_tol) break;
+    if (!graph && rep->refine_resid <= ctx->refine_tol) break;
     MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
     MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, corr, csl, err));
     if (nro > 0) {
@@ -459,16 +417,20 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
     }
   }
-  if (ctx->final_residual) MOAO_TRY(residual());
+  if (ctx->final_residual && !graph) MOAO_TRY(residual());
   rep->refine_steps = steps;
   // ---- outputs: R in FP64, the FP32 factor into the lower triangle of Cmm
   MOAO_CUDA_TRY(cudaMemcpy2DAsync(Ctm, ldCtm * sizeof(double), R64, m * sizeof(double),
                                   m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+  if (graph) return MOAO_OK;
   cudaEventRecord(ev[6], s);
-  int herr = 0;
-  MOAO_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int herr[2] = {0, 0};
+  MOAO_CUDA_TRY(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   MOAO_CUDA_TRY(cudaStreamSynchronize(s));
-  if (herr) return set_error(MOAO_ERR_TIMEOUT, "tensor-core kernel: bounded wait expired");
+  if (herr[0]) return set_error(MOAO_ERR_TIMEOUT, "tensor-core kernel: bounded wait expired");
+  if (herr[1])
+    return set_error(MOAO_ERR_BAD_ARG,
+                     "mixed reconstructor: offsets give a singular capacitance matrix");
   float ms = 0;
   cudaEventElapsedTime(&ms, ev[3], ev[4]);
   rep->ms_factor += ms;

@@ -76,6 +76,12 @@ moao_status mul_small_left(const double* S, int k, const float* Y, long ldy, lon
 moao_status woodbury_apply(const float* Z, long ldz, long m, long n, const double* ZU, int k,
                            const double* Y2, double* R, long ldr, bool accumulate,
                            cudaStream_t st);
+// rid[j] = the range holding index j, or -1.
+moao_status fill_range_ids(int* rid, long n, const OffsetRanges& off, cudaStream_t st);
+// Sinv (k x k, column-major) = (diag(1 / value) + YU)^-1 on the device, k = off.n;
+// sets *bad to 1 when a pivot is zero.
+moao_status capacitance_inverse(const double* YU, const OffsetRanges& off, double* Sinv, int* bad,
+                                cudaStream_t st);
 // E(i, j) -= RU(i, w) value[w] for j in range w (the offsets' part of R*A).
 moao_status subtract_offset_products(double* E, long lde, long m, long n, const double* RU,
                                      const int* rid, const OffsetRanges& off, cudaStream_t st);

@@ -329,6 +329,59 @@ __global__ void woodbury_kernel(const float* __restrict__ Z, long ldz, long m, l
   }
 }
 
+__global__ void fill_range_ids_kernel(int* __restrict__ rid, long n, const RangeList rl) {
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
+    int w = -1;
+    for (int r = 0; r < rl.n; ++r)
+      if (j >= rl.begin[r] && j < rl.end[r]) w = r;
+    rid[j] = w;
+  }
+}
+
+// S^-1 for S = diag(1 / value) + YU (k x k, k <= 32), by Gauss-Jordan elimination
+// with partial pivoting in one block; Sinv column-major. *bad = 1 if singular.
+__global__ void capacitance_inverse_kernel(const double* __restrict__ YU, int k,
+                                           const OffsetValues ov, double* __restrict__ Sinv,
+                                           int* bad) {
+  __shared__ double a[kMaxOffsetRanges][2 * kMaxOffsetRanges + 1];
+  __shared__ int piv;
+  const int t = threadIdx.x;  // one thread per column of [S | I]
+  for (int r = 0; r < k; ++r) {
+    if (t < k) a[r][t] = YU[(long)t * k + r] + (r == t ? 1.0 / ov.v[r] : 0.0);
+    else if (t < 2 * k) a[r][t] = (r == t - k) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int c = 0; c < k; ++c) {
+    if (t == 0) {
+      int p = c;
+      for (int r = c + 1; r < k; ++r)
+        if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+      piv = p;
+      if (!(fabs(a[p][c]) > 0)) *bad = 1;
+    }
+    __syncthreads();
+    if (t < 2 * k && piv != c) {
+      const double x = a[piv][t];
+      a[piv][t] = a[c][t];
+      a[c][t] = x;
+    }
+    __syncthreads();
+    const double d = a[c][c];
+    __syncthreads();
+    if (t < 2 * k) a[c][t] /= d;
+    __syncthreads();
+    for (int r = 0; r < k; ++r) {
+      if (r == c) continue;
+      const double f = a[r][c];
+      __syncthreads();
+      if (t < 2 * k) a[r][t] -= f * a[c][t];
+      __syncthreads();
+    }
+  }
+  if (t < k)
+    for (int r = 0; r < k; ++r) Sinv[(long)t * k + r] = a[r][k + t];
+}
+
 __global__ void subtract_offset_kernel(double* __restrict__ E, long lde, long m, long n,
                                        const double* __restrict__ RU,
                                        const int* __restrict__ rid, const OffsetValues ov) {
@@ -400,6 +453,24 @@ moao_status woodbury_apply(const float* Z, long ldz, long m, long n, const doubl
   if (k < 1 || k > kMaxOffsetRanges) return set_error(MOAO_ERR_BAD_ARG, "woodbury_apply: k");
   dim3 grid((unsigned)((m + 255) / 256), (unsigned)((n + 63) / 64));
   woodbury_kernel<<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, accumulate ? 1 : 0);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status fill_range_ids(int* rid, long n, const OffsetRanges& off, cudaStream_t st) {
+  if (n <= 0) return MOAO_OK;
+  fill_range_ids_kernel<<<blocks_for(n), 256, 0, st>>>(rid, n, ranges_of(off));
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status capacitance_inverse(const double* YU, const OffsetRanges& off, double* Sinv, int* bad,
+                                cudaStream_t st) {
+  if (off.n <= 0) return MOAO_OK;
+  capacitance_inverse_kernel<<<1, 2 * kMaxOffsetRanges, 0, st>>>(YU, off.n, values_of(off), Sinv,
+                                                                 bad);
   ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
