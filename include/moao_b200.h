@@ -327,7 +327,8 @@ typedef struct {
 } moao_batch_item;
 typedef struct {
   moao_prec prec;         /* mixed: fixed max_refine corrections, no residual checks */
-  int streams;            /* 0: tuned (default 4) */
+  int streams;            /* most streams to use; 0: tuned (default 4) */
+  double hbm_budget_gb;   /* device bytes for the streams' buffers; <= 0: 85% of free */
   /* outputs */
   double ms_device;       /* device time of the graph launch */
   double ms_build;        /* host time to capture and instantiate the graph */

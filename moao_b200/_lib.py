@@ -71,7 +71,8 @@ class BatchItem(C.Structure):
 
 
 class BatchOpts(C.Structure):
-    _fields_ = [("prec", i32), ("streams", i32), ("ms_device", C.c_double),
+    _fields_ = [("prec", i32), ("streams", i32), ("hbm_budget_gb", C.c_double),
+                ("ms_device", C.c_double),
                 ("ms_build", C.c_double), ("graph_nodes", C.c_longlong),
                 ("streams_used", i32), ("failed", i32), ("device_gb", C.c_double)]
 

@@ -40,7 +40,8 @@ def batch_reconstructors(tomos: Sequence[Tomo], outputs=None, prec: str = "fp64"
     per = [{"status": items[i].status, "status_name": STATUS.get(items[i].status),
             "info": items[i].info, "nb": items[i].nb_used, "stream": items[i].stream}
            for i in range(n)]
-    run = {k: getattr(opts, k) for k, _ in BatchOpts._fields_ if k not in ("prec", "streams")}
+    run = {k: getattr(opts, k) for k, _ in BatchOpts._fields_
+           if k not in ("prec", "streams", "hbm_budget_gb")}
     return per, run
 
 

@@ -176,20 +176,73 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   }
   int S = o->streams > 0 ? o->streams : tuned_streams(ctx, prec);
   S = std::max(1, std::min({S, count, 16}));
-  // longest first onto the least-loaded stream
+  // Device bytes of one instance: Cmm, Ctm and the workspace of its path.
+  MOAO_TRY(ensure_subs(ctx, S));
+  const moao_ctx* proto = sub_contexts(ctx)[0];
+  auto bytes_of_inst = [&](const Inst& in) {
+    size_t b = sizeof(double) * ((size_t)in.n * in.n + (size_t)in.m * in.n);
+    if (prec == MOAO_PREC_MIXED) {
+      const Tomo_struct<double>& t = items[in.item].tomo->t;
+      const int nro = t.sys.lgsCst > 0 ? 2 * t.sys.nLgs : 0;
+      b += mixed_sizes(in.n, in.m, in.nb, std::max(2, std::min(kMaxBfSlices, proto->bf16_slices)),
+                       proto->ozaki_slices, nro).total();
+    } else {
+      b += sizeof(double) * (size_t)in.nb * ((size_t)in.n + std::max(in.n, in.m));
+    }
+    return b;
+  };
+  // Budget: what is free plus what the sub-contexts already hold (reused).
+  size_t fr = 0, tot = 0, held = 0;
+  MOAO_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+  for (moao_ctx* c : sub_contexts(ctx)) held += c->bytes_held();
+  const size_t budget = o->hbm_budget_gb > 0 ? (size_t)(o->hbm_budget_gb * 1e9)
+                                             : (size_t)(0.85 * (double)(fr + held));
+  // Longest first onto the least-loaded stream; a new stream is opened only
+  // while its first (largest) instance fits the budget, since a stream holds
+  // buffers for its largest instance and instances arrive largest first.
   std::vector<int> order(count);
   std::iota(order.begin(), order.end(), 0);
   std::sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].cost > inst[b].cost; });
-  std::vector<double> load(S, 0.0);
-  std::vector<std::vector<int>> per(S);
+  std::vector<double> load;
+  std::vector<size_t> foot;
+  std::vector<std::vector<int>> per;
+  size_t planned = 0;
   for (int i : order) {
-    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    const size_t f = bytes_of_inst(inst[i]);
+    int k = -1;
+    if (!load.empty()) k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    const bool can_open = (int)load.size() < S && planned + f <= budget;
+    if (can_open && (k < 0 || load[k] > 0)) {
+      load.push_back(0.0);
+      foot.push_back(0);
+      per.emplace_back();
+      k = (int)load.size() - 1;
+    }
+    if (k < 0) return set_error(MOAO_ERR_OOM, "batch: the largest instance exceeds the device budget");
+    if (f > foot[k]) {
+      if (planned - foot[k] + f > budget)
+        return set_error(MOAO_ERR_OOM, "batch: instances exceed the device budget");
+      planned += f - foot[k];
+      foot[k] = f;
+    }
     inst[i].stream = k;
     load[k] += inst[i].cost;
     per[k].push_back(i);
   }
+  S = (int)per.size();
+  // Workspaces kept from earlier batches: drop those much larger than this
+  // plan needs and those of streams this batch does not use.
+  {
+    std::vector<moao_ctx*>& v = sub_contexts(ctx);
+    for (size_t k = 0; k < v.size(); ++k) {
+      const size_t want = (int)k < S ? foot[k] : 0;
+      if (v[k]->bytes_held() > want + want / 2) {
+        cudaStreamSynchronize(v[k]->stream);
+        for (DevBuf* b : v[k]->workspaces()) b->release();
+      }
+    }
+  }
   // memory: per stream its largest Cmm / Ctm pair and workspace
-  MOAO_TRY(ensure_subs(ctx, S));
   std::vector<moao_ctx*>& subs = sub_contexts(ctx);
   std::vector<DevBuf> cmm(S), ctm(S);
   DevBuf status;
