@@ -43,7 +43,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="moao", choices=["moao", "reference"])
     p.add_argument("--path", default="mixed", choices=["fp64", "mixed"])
-    p.add_argument("--nb", type=int, default=256)
+    p.add_argument("--nb", type=int, default=0,
+                   help="panel width (0: 512 for the mixed path, 1024 for FP64, their fastest)")
+    p.add_argument("--nb-fp64", type=int, default=1024, help="panel width of the FP64 comparison arm")
     p.add_argument("--config", default="elt", choices=["elt", "small"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -261,7 +263,7 @@ def serving_main(args):
         return f * 0.129 ** (-5.0 / 3.0), h, np.full(35, 25.0)
 
     def make_server(slots):
-        srv = Server(device=0, slots=slots, nb=args.nb)
+        srv = Server(device=0, slots=slots, nb=args.nb or 512)
         ids, infos = [], []
         for y in systems:
             sf, af = os.path.join(y["dir"], "sys-params.txt"), os.path.join(y["dir"], "prof-1-atmos-night0.txt")
@@ -336,7 +338,7 @@ def serving_main(args):
                        "at_rate_requests_per_s": sustained["rate_requests_per_s"]},
         "config": {"workload": (f"{n_req} requests, nmeas log-uniform 1000-48000 over grids "
                                 f"{nssps} (ELT geometry), 35-layer seeded profiles, R + Cvv + PSF each"),
-                   "slots": args.serve_slots, "path": "mixed", "panel_nb": args.nb},
+                   "slots": args.serve_slots, "path": "mixed", "panel_nb": args.nb or 512},
         "saturation_closed_loop": sat, "sweep": sweep,
         "baseline_sequential_fp64": base,
         "speedup_vs_sequential_fp64": sat["requests_per_s"] / base["requests_per_s"],
@@ -481,13 +483,15 @@ def main():
     else:
         torch.cuda.set_device(0)
     import moao_b200 as M
+    from moao_b200.replicas import max_over_ranks
 
     dev = torch.cuda.current_device()
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = M.Context(dev)
     ctx.set_stream(stream.cuda_stream)
-    ctx.set_block(args.nb)
+    nb_main = args.nb or (512 if args.path == "mixed" else 1024)
+    ctx.set_block(nb_main)
     t = M.Tomo(sf, af)
     nm, nts = t.getNMeas(), t.getNMeasTS()
     Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")   # column-major nm x nm
@@ -542,11 +546,7 @@ def main():
             out["clocks"] = clocks.stop()
             ctx.set_kernel_timing(False)
         out["per_step"] = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
-        total = ev[0].elapsed_time(ev[-1])
-        if dist:
-            tt = torch.tensor([total], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total = float(tt.item())
+        total = max_over_ranks(ev[0].elapsed_time(ev[-1]), dist, "cuda")
         out["total_ms"] = total
         return out
 
@@ -562,6 +562,7 @@ def main():
     rel_err, fp64_arm = None, None
     if args.path == "mixed":
         R_mixed = Ctm.clone()
+        ctx.set_block(args.nb_fp64)
         if args.no_compare:
             step("fp64")
             torch.cuda.synchronize()
@@ -571,7 +572,7 @@ def main():
             fp64_arm = {"value": v64, "unit": UNIT, "ms_per_step": arm["total_ms"] / args.steps,
                         "latency_ms": {"p50": float(np.percentile(arm["per_step"], 50)),
                                        "p99": float(np.percentile(arm["per_step"], 99))},
-                        "mixed_over_fp64": value / v64}
+                        "panel_nb": args.nb_fp64, "mixed_over_fp64": value / v64}
         rel_err = float(torch.linalg.norm(R_mixed - Ctm) / torch.linalg.norm(Ctm))
         del R_mixed
 
@@ -591,11 +592,7 @@ def main():
             step(args.path)             # host profile -> geometry recomputed and re-uploaded
             R_host.copy_(Ctm, non_blocking=True)
             torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
         e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(geom_bytes), "d2h_bytes_per_step": int(nm * nts * 8)}
 
@@ -636,7 +633,7 @@ def main():
                  "bf16x3 split (fp32 accumulate) tensor-core updates + f64 diagonal blocks + int8 Ozaki f64 residual",
         "data": "synthetic (seeded ELT-scale system; reference parameter-file format)",
         "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "path": args.path,
-                   "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": args.nb,
+                   "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": nb_main,
                    "l2": f"inputs larger than L2 (Cmm {nm * nm * 8 / 1e9:.1f} GB regenerated every step)",
                    "parallelism": f"replicas x{world}"},
         "stages_ms_per_step": {f: stats[f]["ms"] / args.steps for f in stats},
