@@ -87,6 +87,14 @@ moao_status moao_ctx_set_stream(moao_ctx* ctx, void* stream);
 moao_status moao_ctx_use_own_stream(moao_ctx* ctx);
 void* moao_ctx_stream(moao_ctx* ctx);
 moao_status moao_ctx_synchronize(moao_ctx* ctx);
+/* Storage of the factor and solve operands on the tensor cores in the mixed
+ * path: MOAO_FACTOR_F16X2 (default) = 2 fp16 slices scaled by a power of two
+ * per row (~22 bits, 3 products); MOAO_FACTOR_BF16X3 = 3 bf16 slices (~24
+ * bits, 6 products). After refinement both reach the same R; F16X2 does half
+ * the tensor work and stores a third less. No reference counterpart. */
+enum { MOAO_FACTOR_BF16X3 = 0, MOAO_FACTOR_F16X2 = 1 };
+moao_status moao_ctx_set_factor_format(moao_ctx* ctx, int format);
+
 /* Block-constant offsets of Cmm known to the caller, for the mixed-precision
  * reconstructor: value[w] is part of every entry (i, j) with begin[w] <= i, j
  * < end[w] (0..32 non-overlapping ranges, values > 0; nranges 0 clears). The
@@ -108,7 +116,7 @@ moao_status moao_ctx_set_host_precision(moao_ctx* ctx, moao_prec prec);
 
 /* Number of kernels this library launched on the context since creation. */
 long long moao_ctx_launch_count(const moao_ctx* ctx);
-/* Panel width of the blocked factorisation (default 256; multiple of 64). */
+/* Panel width of the blocked factorisation (default 512; multiple of 64). */
 moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
 
 /* Options of the mixed-precision reconstructor: bf16 slices of the factor in

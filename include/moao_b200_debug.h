@@ -15,6 +15,8 @@ extern "C" {
 /* Tensor-core GEMM on the context stream (device pointers):
  *   kind 0 (bf16): C[f32, M x N, col-major, ldc] = alpha * sum_p A_{pa[p]} B_{pb[p]}^T + beta * C
  *   kind 1 (int8): C[f64] += alpha * 2^(erow[r] + ecol[c] + shift) * sum_p A_{pa[p]} B_{pb[p]}^T
+ *   kind 2 (fp16): C[f32] = alpha * 2^(erow[r] + ecol[c] + shift) * sum_p A_{pa[p]} B_{pb[p]}^T
+ *                  + beta * C (erow and ecol NULL: no scaling)
  * A holds na slices of M x K row-major (lda elements per row), slice i at
  * A + i * M * lda; B holds nb slices of N x K row-major likewise. lower = 1
  * writes only C(r, c) with r >= c. Synchronises and returns MOAO_ERR_TIMEOUT

@@ -150,6 +150,12 @@ class Context:
                                        max_refine, tol, int(final_residual)),
               "moao_ctx_set_mixed")
 
+    def set_factor_format(self, fmt: str):
+        """'bf16x3' (3 bf16 slices, 6 products) or 'f16x2' (2 fp16 slices scaled
+        per row, 3 products) for the mixed path's tensor-core operands."""
+        code = {"bf16x3": 0, "f16x2": 1}[fmt]
+        check(lib().moao_ctx_set_factor_format(self._h, code), "moao_ctx_set_factor_format")
+
     def set_offsets(self, begin, end, value):
         """Block-constant offsets of Cmm for the mixed path (see moao_ctx_set_offsets);
         empty sequences clear them."""

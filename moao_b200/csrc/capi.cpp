@@ -461,6 +461,15 @@ moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* c, const moao_tomo* tp) {
   return moao_ctx_set_offsets(c, (int)b.size(), b.data(), e.data(), v.data());
 }
 
+moao_status moao_ctx_set_factor_format(moao_ctx* c, int format) {
+  if (!c || (format != MOAO_FACTOR_BF16X3 && format != MOAO_FACTOR_F16X2))
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_factor_format: BF16X3 or F16X2");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->factor_format = format;
+  c->mx_factored_n = -1;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_host_precision(moao_ctx* c, moao_prec prec) {
   if (!c || (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED))
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_precision: FP64 or MIXED");

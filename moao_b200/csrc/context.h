@@ -49,7 +49,7 @@ struct moao_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   long long launches = 0;
-  int nb = 256;  // outer panel width of the blocked factorisation
+  int nb = 512;  // outer panel width of the blocked factorisation
   moao_prec host_prec = MOAO_PREC_FP64;  // precision of moao_reconstructor_host
   bool keep_cmm = false;  // mixed path: leave Cmm as given (no factor written back)
   bool graph_mode = false;  // mixed path under stream capture: no host waits or reads
@@ -59,12 +59,13 @@ struct moao_ctx {
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
-  moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv;
+  moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv, mx_exps;
   long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
   // Block-constant offsets of Cmm known to the caller (moao_ctx_set_offsets):
   // the mixed path factors Cmm minus them and adds them back exactly.
   moao::OffsetRanges offsets;
   int bf16_slices = 3;       // bf16 slices of the factor (3: ~24 bits, 6 products)
+  int factor_format = 1;     // MOAO_FACTOR_F16X2 (default) or MOAO_FACTOR_BF16X3
   int corr_slices = 2;       // bf16 slices of the factor in the correction solves
   int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
   int max_refine = 1;        // refinement corrections per target
@@ -86,7 +87,7 @@ struct moao_ctx {
   std::vector<moao::DevBuf*> workspaces() {
     return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
             &mx_w1, &mx_w2,   &mx_x,    &mx_r64, &mx_e64, &mx_qa,  &mx_qb,    &mx_ea,
-            &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv};
+            &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv, &mx_exps};
   }
   // Device bytes held by the workspaces and the geometry caches.
   size_t bytes_held() {
@@ -133,10 +134,10 @@ moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long 
 // nsl bf16 slices, ns int8 slices and nranges declared offset ranges.
 struct MixedSizes {
   size_t a32 = 0, lr = 0, t32 = 0, w = 0, x = 0, r64 = 0, qa = 0, qb = 0, ea = 0, fb = 0,
-         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0;
+         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0, exps = 0;
   size_t total() const {
     return a32 + 2 * lr + t32 + 2 * w + x + 2 * r64 + qa + qb + ea + fb + colmax + norm +
-           2 * dinv + info + offsets;
+           2 * dinv + info + offsets + exps;
   }
 };
 MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges);

@@ -98,9 +98,12 @@ Products products_for(int slices) {
 // [ka, ka + nk*64) of the A slices and [kb, ...) of the B slices.
 moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, const TcTensor* B,
                       int b_row0, int kb, int nk, const Products& pr, long M, long N, float* C,
-                      long ldc, bool lower, int* err, double flops) {
+                      long ldc, bool lower, int* err, double flops, const int* erow = nullptr,
+                      const int* ecol = nullptr) {
   TcGemm g;
-  g.kind = kTcBf16;
+  g.kind = A[0].kind;
+  g.erow = erow;
+  g.ecol = ecol;
   g.epi = kTcEpiF32;
   g.M = M;
   g.N = N;
@@ -127,14 +130,36 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
   return tc_gemm(g, ctx->stream, &ctx->launches);
 }
 
+// fp16 operands: power-of-two scales of the stored factor and solve slices.
+//   erp: per panel p, the row exponents of L(:, panel p) (erp + p*n, indexed by row)
+//   ecf: per column j of L, its exponent (the Lc copy, row j = L(:, j))
+//   ex:  row exponents of the current solve block
+struct Scales {
+  bool f16 = false;
+  int* erp = nullptr;
+  int* ecf = nullptr;
+  int* ex = nullptr;
+};
+constexpr int kF16Bias = 14;  // stored slices below 2^14 in magnitude (fp16 max 65504)
+
+// Slices of the m x kb solve block W2 (FP64) into xr for the tensor core.
+moao_status split_block(const Scales& sc, const double* W2, long m, long kb, int slices,
+                        const BfSlices& xr, long ldx, cudaStream_t s) {
+  BfSlices none{};
+  if (!sc.f16) return split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s);
+  MOAO_TRY(scale_exponents(W2, m, m, kb, kF16Bias, sc.ex, nullptr, s));
+  return split_f16(W2, m, m, kb, slices, xr, ldx, sc.ex, none, 0, nullptr, s);
+}
+
 // In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1, with the long
 // updates as the given slice products.
 moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double* dinv,
                         const TcTensor* xA, const Maps& mp, double* W1, double* W2,
-                        void* const* xs, long ldx, const Products& pr, int slices, int* err) {
+                        void* const* xs, long ldx, const Products& pr, int slices, int* err,
+                        const Scales& sc) {
   const long nb = ctx->nb;
   cudaStream_t s = ctx->stream;
-  BfSlices xr{}, none{};
+  BfSlices xr{};
   for (int k = 0; k < slices; ++k) xr.p[k] = xs[k];
   for (long k0 = 0; k0 < n; k0 += nb) {
     const long kb = std::min(nb, n - k0);
@@ -143,9 +168,11 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
     const long rest = n - k0 - kb;
     if (rest > 0) {
-      MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
+      MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
       MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lrB, (int)(k0 + kb), (int)k0, (int)((kb + 63) / 64),
-                         pr, m, rest, T32 + (k0 + kb) * m, m, false, err, 2.0 * m * rest * kb));
+                         pr, m, rest, T32 + (k0 + kb) * m, m, false, err, 2.0 * m * rest * kb,
+                         sc.f16 ? sc.ex : nullptr,
+                         sc.f16 ? sc.erp + (k0 / nb) * n + (k0 + kb) : nullptr));
     }
   }
   const long nblk = (n + nb - 1) / nb;
@@ -155,9 +182,10 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
     MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
     MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
     if (k0 > 0) {
-      MOAO_TRY(split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s));
+      MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
       MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
-                         T32, m, false, err, 2.0 * m * k0 * kb));
+                         T32, m, false, err, 2.0 * m * k0 * kb, sc.f16 ? sc.ex : nullptr,
+                         sc.f16 ? sc.ecf : nullptr));
     }
   }
   return MOAO_OK;
@@ -182,6 +210,7 @@ MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
   z.norm = sizeof(double) * 2;
   z.dinv = sizeof(double) * (size_t)std::max(n, 1L) * nb;
   z.info = 3 * sizeof(int);
+  z.exps = sizeof(int) * ((size_t)((n + nb - 1) / nb) * n + (size_t)n + (size_t)std::max(m, 128L));
   if (nranges > 0)
     z.offsets = sizeof(int) * (size_t)n + sizeof(float) * (size_t)128 * n +
                 sizeof(double) * ((size_t)nranges * n + (size_t)std::max(m, (long)nranges) * nranges +
@@ -207,7 +236,9 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   const int ns = ctx->ozaki_slices;
   const long ldx = nb;
   // ---- workspace
-  const int nsl = std::max(2, std::min(kMaxBfSlices, ctx->bf16_slices));
+  const bool f16 = ctx->factor_format == MOAO_FACTOR_F16X2;
+  const int tck = f16 ? kTcF16 : kTcBf16;
+  const int nsl = f16 ? 2 : std::max(2, std::min(kMaxBfSlices, ctx->bf16_slices));
   const MixedSizes z = mixed_sizes(n, m, nb, nsl, ns, ctx->offsets.n);
   MOAO_TRY(ctx->mx_a32.ensure(z.a32));
   MOAO_TRY(ctx->mx_lr.ensure(z.lr));
@@ -227,6 +258,12 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   MOAO_TRY(ctx->ws_dinv.ensure(z.dinv));
   MOAO_TRY(ctx->ws_w.ensure(z.dinv));
   MOAO_TRY(ctx->ws_info.ensure(z.info));
+  MOAO_TRY(ctx->mx_exps.ensure(z.exps));
+  Scales sc;
+  sc.f16 = f16;
+  sc.erp = ctx->mx_exps.as<int>();
+  sc.ecf = sc.erp + (size_t)((n + nb - 1) / nb) * n;
+  sc.ex = sc.ecf + n;
   float* A32 = ctx->mx_a32.as<float>();
   uint16_t* lr = ctx->mx_lr.as<uint16_t>();
   uint16_t* lc = ctx->mx_lc.as<uint16_t>();
@@ -272,11 +309,11 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   for (int k = 0; k < nsl; ++k) {
     uint16_t* lrk = lr + (size_t)k * n * ldn;
     uint16_t* lck = lc + (size_t)k * n * ldn;
-    MOAO_TRY(make_tc_map(&mp.lrA[k], lrk, kTcBf16, n, n, ldn));
-    MOAO_TRY(make_tc_map(&mp.lrB[k], lrk, kTcBf16, n, n, ldn, 256));
-    MOAO_TRY(make_tc_map(&mp.lcB[k], lck, kTcBf16, n, n, ldn, 256));
-    MOAO_TRY(make_tc_map(&mp.xA[k], xs[k], kTcBf16, m, nb, ldx));
-    MOAO_TRY(make_tc_map(&mp.yA[k], xs[k], kTcBf16, kYRows, nb, ldx));
+    MOAO_TRY(make_tc_map(&mp.lrA[k], lrk, tck, n, n, ldn));
+    MOAO_TRY(make_tc_map(&mp.lrB[k], lrk, tck, n, n, ldn, 256));
+    MOAO_TRY(make_tc_map(&mp.lcB[k], lck, tck, n, n, ldn, 256));
+    MOAO_TRY(make_tc_map(&mp.xA[k], xs[k], tck, m, nb, ldx));
+    MOAO_TRY(make_tc_map(&mp.yA[k], xs[k], tck, kYRows, nb, ldx));
   }
   const int csl = std::max(2, std::min(nsl, ctx->corr_slices));
   const Products full = products_for(nsl), corr = products_for(csl);
@@ -308,10 +345,18 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
         rr.p[k] = lr + (size_t)k * n * ldn + (k0 + kb) * ldn + k0;
         cc.p[k] = lc + (size_t)k * n * ldn + k0 * ldn + (k0 + kb);
       }
-      MOAO_TRY(split_bf16(W2, rest, rest, kb, nsl, rr, ldn, cc, ldn, s));
+      const int* er = nullptr;
+      if (f16) {
+        int* erk = sc.erp + (k0 / nb) * n + (k0 + kb);  // rows k0+kb.. of panel k0/nb
+        MOAO_TRY(scale_exponents(W2, rest, rest, kb, kF16Bias, erk, sc.ecf + k0, s));
+        MOAO_TRY(split_f16(W2, rest, rest, kb, nsl, rr, ldn, erk, cc, ldn, sc.ecf + k0, s));
+        er = erk;
+      } else {
+        MOAO_TRY(split_bf16(W2, rest, rest, kb, nsl, rr, ldn, cc, ldn, s));
+      }
       MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k0 + kb), (int)k0, mp.lrB, (int)(k0 + kb), (int)k0,
                          (int)(kb / 64), full, rest, rest, A32 + (k0 + kb) + (k0 + kb) * n, n,
-                         true, err, (double)rest * rest * kb));
+                         true, err, (double)rest * rest * kb, er, er));
     }
     if (!graph) {
       int info[2] = {0, 0};
@@ -331,7 +376,8 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     if (nro > 0) {
       // Y = U^T M_B^-1 (one 128-row solve), S = D^-1 + Y U, Y2 = S^-1 Y
       MOAO_TRY(fill_range_indicators(Y32, kYRows, n, off, s));
-      MOAO_TRY(mixed_solve(ctx, n, kYRows, Y32, dinv, mp.yA, mp, W1, W2, xs, ldx, full, nsl, err));
+      MOAO_TRY(mixed_solve(ctx, n, kYRows, Y32, dinv, mp.yA, mp, W1, W2, xs, ldx, full, nsl, err,
+                           sc));
       MOAO_TRY(range_sums(Y32, kYRows, nro, off, ZU, s));
       MOAO_TRY(capacitance_inverse(ZU, off, Sinv, d_info + 2, s));
       MOAO_TRY(mul_small_left(Sinv, nro, Y32, kYRows, n, Y2, s));
@@ -341,7 +387,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   if (!graph) cudaEventRecord(ev[4], s);
   // ---- solve
   MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
-  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, full, nsl, err));
+  MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, full, nsl, err, sc));
   if (nro > 0) {
     MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
     MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, R64, m, false, s));
@@ -409,7 +455,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(residual());
     if (!graph && rep->refine_resid <= ctx->refine_tol) break;
     MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
-    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, corr, csl, err));
+    MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, corr, csl, err, sc));
     if (nro > 0) {
       MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
       MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, R64, m, true, s));

@@ -44,6 +44,15 @@ moao_status add_f32_to_f64(const float* s, long lds, double* d, long ldd, long m
 // column-major (stride ldc).
 moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
                        long ldr, BfSlices cmaj, long ldc, cudaStream_t st);
+// Per-row (erow[m]) and/or per-column (ecol[n]) exponents of a column-major
+// m x n block: the smallest e with max |x| < 2^e, minus bias (null skips one).
+moao_status scale_exponents(const double* A, long lda, long m, long n, int bias, int* erow,
+                            int* ecol, cudaStream_t st);
+// fp16 split of x * 2^-e into ns slices: row-major copy scaled by erow[r],
+// column-major copy by ecol[c] (either copy may be skipped with a null p[0]).
+moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
+                      cudaStream_t st);
 // int8 slices of the rows of A (m x n, column-major): per-row exponents in e[m],
 // slice s at out + s*m*ldo, row-major with row stride ldo.
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,

@@ -11,6 +11,7 @@
 //                    each q_p the rounded remainder of the previous slice, so the
 //                    products of slices accumulate exactly in int32.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -100,7 +101,7 @@ __device__ __forceinline__ int exponent_of(double mx) {
 
 // Row maxima of a column-major m x n block: 32 rows per block, 8 column strides.
 __global__ void row_exponent_kernel(const double* __restrict__ A, long lda, long m, long n,
-                                    int* __restrict__ e) {
+                                    int* __restrict__ e, int bias) {
   __shared__ double red[8][33];
   const long r = (long)blockIdx.x * 32 + threadIdx.x;
   double mx = 0;
@@ -110,7 +111,63 @@ __global__ void row_exponent_kernel(const double* __restrict__ A, long lda, long
   __syncthreads();
   if (threadIdx.y == 0 && r < m) {
     for (int k = 1; k < 8; ++k) mx = fmax(mx, red[k][threadIdx.x]);
-    e[r] = exponent_of(mx);
+    e[r] = exponent_of(mx) - bias;
+  }
+}
+
+// Column maxima of a column-major m x n block: one block per column.
+__global__ void col_exponent_kernel(const double* __restrict__ A, long lda, long m, long n,
+                                    int* __restrict__ e, int bias) {
+  __shared__ double red[32];
+  const long c = blockIdx.x;
+  double mx = 0;
+  for (long r = threadIdx.x; r < m; r += blockDim.x) mx = fmax(mx, fabs(A[c * lda + r]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, red[w]);
+    e[c] = exponent_of(mx) - bias;
+  }
+}
+
+// 32x32 tiles, 32x8 threads. fp16 slices of x * 2^-e: slice k = fp16 of what
+// the previous slices left (in FP64), e = erow[r] for the row-major copy and
+// ecol[c] for the column-major one, so either copy can be scaled back exactly
+// by a power of two per row of the operand it feeds.
+__global__ void split_f16_kernel(const double* __restrict__ src, long lds, long m, long n, int ns,
+                                 BfSlices rmaj, long ldr, const int* __restrict__ erow,
+                                 BfSlices cmaj, long ldc, const int* __restrict__ ecol) {
+  __shared__ __half t[kMaxBfSlices][32][34];
+  const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long r = r0 + tx, c = c0 + jj;
+    double x = 0;
+    if (r < m && c < n) x = src[c * lds + r];
+    if (rmaj.p[0]) {
+      double rem = (r < m) ? ldexp(x, -erow[r]) : 0.0;
+      for (int k = 0; k < ns; ++k) {
+        const __half h = __double2half(rem);
+        rem -= (double)__half2float(h);
+        t[k][tx][jj] = h;
+      }
+    }
+    if (cmaj.p[0] && r < m && c < n) {
+      double rem = ldexp(x, -ecol[c]);
+      for (int k = 0; k < ns; ++k) {
+        const __half h = __double2half(rem);
+        rem -= (double)__half2float(h);
+        static_cast<__half*>(cmaj.p[k])[c * ldc + r] = h;
+      }
+    }
+  }
+  if (!rmaj.p[0]) return;
+  __syncthreads();
+  for (int ii = ty; ii < 32; ii += 8) {
+    const long r = r0 + ii, c = c0 + tx;
+    if (r < m && c < n)
+      for (int k = 0; k < ns; ++k) static_cast<__half*>(rmaj.p[k])[r * ldr + c] = t[k][ii][tx];
   }
 }
 
@@ -524,10 +581,39 @@ moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSl
   return MOAO_OK;
 }
 
+moao_status scale_exponents(const double* A, long lda, long m, long n, int bias, int* erow,
+                            int* ecol, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  if (erow) {
+    row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, erow, bias);
+    ++tl_launches;
+  }
+  if (ecol) {
+    col_exponent_kernel<<<(unsigned)n, 256, 0, st>>>(A, lda, m, n, ecol, bias);
+    ++tl_launches;
+  }
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
+                      cudaStream_t st) {
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_f16: slices");
+  if ((rmaj.p[0] && !erow) || (cmaj.p[0] && !ecol))
+    return set_error(MOAO_ERR_BAD_ARG, "split_f16: exponents missing");
+  dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+  split_f16_kernel<<<grid, dim3(32, 8), 0, st>>>(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc, ecol);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
                              int8_t* out, long ldo, cudaStream_t st) {
   if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
-  row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e);
+  row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e, 0);
   ++tl_launches;
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
   split_rows_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, m, n, e, ns, out, ldo, m * ldo);

@@ -13,6 +13,8 @@
 //
 // Kinds:
 //   BF16 -> FP32 accumulate (kind::f16);   epilogue C32 = alpha*acc + beta*C32
+//   FP16 -> FP32 accumulate (kind::f16);   epilogue C32 = alpha*acc*2^(erow[r]+ecol[c]+shift)
+//           + beta*C32 (power-of-two scales of operands stored scaled into fp16 range)
 //   INT8 -> INT32 accumulate (kind::i8), exact for K*64*64*pairs < 2^31;
 //           epilogue C64 += acc * 2^(erow[r] + ecol[c] + shift)
 // Waits on mbarriers are bounded; on expiry the kernel records an error code in
@@ -43,12 +45,17 @@ constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quadrant
 constexpr int THREADS = (4 + EPI_WARPS) * 32;
 constexpr int ACC_COLS = TBN;           // fp32 / int32 columns of one accumulator
 constexpr int TMEM_COLS = 2 * ACC_COLS; // double-buffered accumulator
-constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int STAGE_C = 32 * 32 * 4;    // per epilogue warp: one 32x32 FP32 chunk for TMA
+constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ +
+                       EPI_WARPS * 32 * sizeof(float) /*per-warp column scales*/ +
+                       (size_t)EPI_WARPS * STAGE_C /*per-warp C staging*/;
 constexpr unsigned long long kSpinLimit = 1ull << 28;
 
 struct __align__(64) TcParams {
   CUtensorMap mapA[kTcMaxMaps];
   CUtensorMap mapB[kTcMaxMaps];
+  CUtensorMap mapC;        // FP32 C (rows inner) for the TMA reduce-add epilogue
+  int c_tma;               // 1: C += alpha*acc*scales through cp.reduce.async.bulk.tensor
   TcSegment seg[kTcMaxSegs];
   int nseg;
   int M, N;
@@ -116,6 +123,17 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// C += (staged chunk) through the TMA unit: a 32-row x 32-column FP32 box at
+// (row x, column y) of the C tensor map, reduced (added) into global memory.
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, int x, int y,
+                                                  const void* src) {
+  asm volatile(
+      "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];\n"
+      ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(src))
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+
 // Shared-memory matrix descriptor for a K-major tile written by TMA with the
 // 128-byte swizzle: 8-row core groups 1024 bytes apart (SBO), LBO = 16 bytes
 // (unused for swizzled K-major), descriptor version 1 (tcgen05), SWIZZLE_128B.
@@ -129,7 +147,7 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                          uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -161,6 +179,7 @@ constexpr uint32_t idesc_of(int dfmt, int abfmt) {
          (uint32_t)((TBN >> 3) << 17) | (uint32_t)((TBM >> 4) << 24);
 }
 constexpr uint32_t kIdescBf16 = idesc_of(1, 1);
+constexpr uint32_t kIdescF16 = idesc_of(1, 0);
 constexpr uint32_t kIdescI8 = idesc_of(2, 1);
 
 // First row tile of column tile nt that reaches the written (lower) part.
@@ -200,6 +219,10 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
   uint64_t* tfull_bar = empty_bar + STAGES;  // [2]
   uint64_t* tempty_bar = tfull_bar + 2;      // [2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
+  // per epilogue warp: 2^ecol of the 32 columns of its current chunk, and a
+  // 32x32 FP32 staging chunk for the TMA reduce-add of C
+  float* col_scale = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES + 256);
+  float* c_stage = col_scale + EPI_WARPS * 32;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -261,7 +284,8 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
-    const uint32_t idesc = (p.kind == kTcBf16) ? kIdescBf16 : kIdescI8;
+    const uint32_t idesc =
+        (p.kind == kTcBf16) ? kIdescBf16 : (p.kind == kTcF16 ? kIdescF16 : kIdescI8);
     int it = 0, tc = 0;
     bool ok = true;
     for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x, ++tc) {
@@ -283,7 +307,7 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
         for (int kk = 0; kk < 4; ++kk) {
           const uint64_t off = (uint64_t)((kk * 32) >> 4);
           const uint32_t accum = (k | kk) ? 1u : 0u;
-          if (p.kind == kTcBf16) mma_bf16(acc, da + off, db + off, idesc, accum);
+          if (p.kind != kTcI8) mma_f16(acc, da + off, db + off, idesc, accum);
           else mma_i8(acc, da + off, db + off, idesc, accum);
         }
         mma_commit(&empty_bar[st]);
@@ -301,11 +325,25 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
       decode_tile(p, v, &mt, &nt);
       const int m0 = mt * TBM, n0 = nt * TBN;
       const int buf = tc & 1;
-      if (!mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3)) break;
+      // every lane waits; the warp leaves together if any lane gave up
+      const bool got = mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3);
+      if (!__all_sync(0xffffffffu, got)) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const int r = m0 + q * 32 + lane;
-      const bool live = kblocks > 0 && !*(volatile int*)p.err;
+      // warp-uniform (lane 0's reading): the loop below holds warp-collective
+      // tcgen05.ld and __syncwarp
+      const bool live =
+          __shfl_sync(0xffffffffu, (int)(kblocks > 0 && !*(volatile int*)p.err), 0) != 0;
+      float* wscale = col_scale + (warp - 4) * 32;
       for (int c0 = half * (TBN / 2); c0 < (half + 1) * (TBN / 2) && live; c0 += 32) {
+        if (p.epi == kTcEpiF32 && p.erow) {
+          // one coalesced load of the chunk's column exponents, shared by the warp
+          const int c = n0 + c0 + lane;
+          const int e = c < p.N ? p.ecol[c] : 0;
+          __syncwarp();
+          wscale[lane] = __int_as_float((min(max(e, -126), 127) + 127) << 23);
+          __syncwarp();
+        }
         uint32_t v32[32];
         const uint32_t taddr =
             tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * ACC_COLS + c0);
@@ -321,6 +359,11 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
               "=r"(v32[31])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (p.c_tma) {
+          // the previous chunk's reduction must have read the staging buffer
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+          __syncwarp();
+        }
         if (r < p.M) {
           // Mask of the chunk's columns that this row writes.
           uint32_t mask = 0;
@@ -332,16 +375,34 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
           // All loads of C first (independent, in flight together), then the
           // stores: interleaving them would serialise each load behind the
           // previous store, since the compiler cannot rule out aliasing.
-          if (p.epi == kTcEpiF32) {
+          if (p.epi == kTcEpiF32 && p.c_tma) {
+            // staged in shared memory column by column (lane = row: conflict-free), then
+            // added into C by one bulk tensor reduction per chunk; masked entries add 0
+            float* stg = c_stage + (warp - 4) * (STAGE_C / 4);
+            float ra = p.alpha;
+            if (p.erow)
+              ra *= __int_as_float((min(max(p.erow[r] + p.shift, -126), 127) + 127) << 23);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const float sj = p.erow ? ra * wscale[j] : ra;
+              stg[j * 32 + lane] = (mask >> j & 1u) ? sj * __uint_as_float(v32[j]) : 0.f;
+            }
+          } else if (p.epi == kTcEpiF32) {
             float* dst = static_cast<float*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
             float old[32];
+            // alpha * 2^(erow[r] + shift) from the exponent bits (normal range)
+            float ra = p.alpha;
+            if (p.erow)
+              ra *= __int_as_float((min(max(p.erow[r] + p.shift, -126), 127) + 127) << 23);
 #pragma unroll
             for (int j = 0; j < 32; ++j)
               old[j] = (p.beta != 0.f && (mask >> j & 1u)) ? dst[(size_t)j * p.ldc] : 0.f;
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              if (mask >> j & 1u)
-                dst[(size_t)j * p.ldc] = p.alpha * __uint_as_float(v32[j]) + p.beta * old[j];
+              if (mask >> j & 1u) {
+                const float sj = p.erow ? ra * wscale[j] : ra;
+                dst[(size_t)j * p.ldc] = sj * __uint_as_float(v32[j]) + p.beta * old[j];
+              }
           } else {
             double* dst = static_cast<double*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
             const int er = p.erow[r] + p.shift;
@@ -360,12 +421,21 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
                     old[j] + (double)p.alpha * ldexp((double)(int)v32[j], er + ec[j]);
           }
         }
+        if (p.c_tma) {
+          // make the staged chunk visible to the TMA unit, then one lane adds it to C
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          __syncwarp();
+          if (lane == 0)
+            tma_reduce_add_2d(&p.mapC, m0 + q * 32, n0 + c0, c_stage + (warp - 4) * (STAGE_C / 4));
+        }
       }
       // release this accumulator buffer to the MMA issuer
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty_bar[buf]);
     }
+    // every reduction into C complete before the CTA's shared memory goes away
+    if (p.c_tma && lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -397,7 +467,7 @@ moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows,
     return set_error(MOAO_ERR_BAD_ARG, "tc map: box rows must be 128 (A) or 256 (B)");
   auto fn = encode_fn();
   if (!fn) return set_error(MOAO_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  const int esz = (kind == kTcBf16) ? 2 : 1;
+  const int esz = (kind == kTcI8) ? 1 : 2;
   if ((reinterpret_cast<uintptr_t>(base) & 15) || ((row_stride_elems * esz) & 15))
     return set_error(MOAO_ERR_BAD_ARG, "tc map: base or row stride not 16-byte aligned");
   if (rows <= 0 || kcols <= 0 || box_rows <= 0 || box_rows > 256)
@@ -406,7 +476,10 @@ moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows,
   cuuint64_t strides[1] = {(cuuint64_t)(row_stride_elems * esz)};
   cuuint32_t box[2] = {(cuuint32_t)(KBYTES / esz), (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(&t->map, esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+  const CUtensorMapDataType dt = kind == kTcBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                 : kind == kTcF16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                  : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  CUresult r = fn(&t->map, dt,
                   2, const_cast<void*>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -425,8 +498,10 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
     return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: bad operand lists");
   if (g.epi == kTcEpiF64Scaled && (g.kind != kTcI8 || !g.erow || !g.ecol))
     return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: scaled epilogue needs int8 and exponents");
-  if (g.epi == kTcEpiF32 && g.kind != kTcBf16)
-    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: fp32 epilogue needs bf16 operands");
+  if (g.epi == kTcEpiF32 && g.kind == kTcI8)
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: fp32 epilogue needs bf16 or fp16 operands");
+  if (g.epi == kTcEpiF32 && (!g.erow) != (!g.ecol))
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: row and column exponents go together");
   TcParams p;
   std::memset(&p, 0, sizeof(p));
   for (int i = 0; i < g.nA; ++i) {
@@ -478,6 +553,23 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   }
   if (total == 0) return MOAO_OK;
   p.total_tiles = (int)total;
+  // C += alpha * acc (beta 1) through TMA reductions when C's layout allows a
+  // tensor map: 16-byte aligned base and row stride.
+  p.c_tma = 0;
+  if (g.epi == kTcEpiF32 && g.beta == 1.f && !(reinterpret_cast<uintptr_t>(g.C) & 15) &&
+      (g.ldc % 4) == 0) {
+    auto fn = encode_fn();
+    if (fn) {
+      cuuint64_t dims[2] = {(cuuint64_t)g.M, (cuuint64_t)g.N};
+      cuuint64_t strides[1] = {(cuuint64_t)g.ldc * sizeof(float)};
+      cuuint32_t box[2] = {32, 32};
+      cuuint32_t estr[2] = {1, 1};
+      if (fn(&p.mapC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, g.C, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        p.c_tma = 1;
+    }
+  }
   static int num_sms = 0;
   if (!num_sms) {
     int dev = 0;
@@ -505,17 +597,17 @@ extern "C" moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long 
                                           long ldc, float alpha, float beta, const int* erow,
                                           const int* ecol, int shift, int lower) {
   using namespace moao;
-  if (!ctx || !A || !B || !C || !pa || !pb || kind < 0 || kind > 1 || na < 1 ||
+  if (!ctx || !A || !B || !C || !pa || !pb || kind < 0 || kind > 2 || na < 1 ||
       na > kTcMaxMaps || nb < 1 || nb > kTcMaxMaps || npairs < 1 || npairs > kTcMaxSegs ||
       ldc < M || lda < K || ldb < K)
     return set_error(MOAO_ERR_BAD_ARG, "debug_tc_gemm: bad arguments");
   std::lock_guard<std::mutex> lk(ctx->mu);
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
-  const int esz = kind == 0 ? 2 : 1;
+  const int esz = kind == kTcI8 ? 1 : 2;
   TcTensor ta[kTcMaxMaps], tb[kTcMaxMaps];
   TcGemm g;
   g.kind = kind;
-  g.epi = kind == 0 ? kTcEpiF32 : kTcEpiF64Scaled;
+  g.epi = kind == kTcI8 ? kTcEpiF64Scaled : kTcEpiF32;
   g.M = M;
   g.N = N;
   for (int i = 0; i < na; ++i) {

@@ -11,7 +11,10 @@ namespace moao {
 
 constexpr int kTcMaxMaps = 6;
 constexpr int kTcMaxSegs = 8;
-enum TcKind { kTcBf16 = 0, kTcI8 = 1 };
+// kTcF16: fp16 operands (kind::f16 like bf16, FP32 accumulation); with
+// erow/ecol the FP32 epilogue scales by 2^(erow[r] + ecol[c] + shift), so the
+// operands can be stored scaled per row into fp16's range.
+enum TcKind { kTcBf16 = 0, kTcI8 = 1, kTcF16 = 2 };
 enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1 };
 
 // A K-major operand: rows x kcols elements, row stride in elements.
@@ -45,7 +48,8 @@ struct TcGemm {
   float alpha = 1.f, beta = 0.f;
   void* C = nullptr;           // float (kTcEpiF32) or double (kTcEpiF64Scaled), column-major
   long ldc = 0;
-  const int* erow = nullptr;   // kTcEpiF64Scaled: C += acc * 2^(erow[r] + ecol[c] + shift)
+  const int* erow = nullptr;   // kTcEpiF64Scaled: C += acc * 2^(erow[r] + ecol[c] + shift);
+                               // kTcEpiF32 (optional): acc scaled the same way
   const int* ecol = nullptr;
   int shift = 0;
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired

@@ -38,6 +38,7 @@ def case(name):
 
 def run_mixed(ctx, nm, nts, Cmm, Ctm, nb=256, slices=5, refine=1, bf16_slices=3):
     ctx.set_block(nb)
+    ctx.set_factor_format("bf16x3")
     ctx.set_mixed(bf16_slices=bf16_slices, ozaki_slices=slices, max_refine=refine,
                   final_residual=True)
     try:
@@ -47,6 +48,7 @@ def run_mixed(ctx, nm, nts, Cmm, Ctm, nb=256, slices=5, refine=1, bf16_slices=3)
     finally:
         ctx.set_block(256)
         ctx.set_mixed()
+        ctx.set_factor_format("f16x2")
     return host(dC), host(dT), rep
 
 
@@ -118,3 +120,27 @@ def test_mixed_not_spd(ctx):
     with pytest.raises(M.NotSPDError) as e:
         M.reconstructor(n, 2, dev(C), n, dev(np.ones((2, n))), 2, 1, prec="mixed", ctx=ctx)
     assert e.value.column == 201
+
+
+@pytest.mark.parametrize("name", ["elt16", "elt24"])
+def test_f16x2_factor_with_offsets(ctx, name):
+    """2 fp16 slices scaled per row (3 products) with the model's LGS offsets
+    declared and one correction: R within 1e-5 of the oracle."""
+    import torch
+    sf, af = systems.files(name)
+    t = M.Tomo(sf, af)
+    g = O.Geometry.from_tomo(t)
+    nm, nts = g.nmeas, g.nmeasts
+    Cmm = O.matcov(g, nm, nm, 0, 0, 1, nthreads=16)
+    Ctm = O.matcov(g, nts, nm, 0, 0, 3, nthreads=16)
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    c2 = M.Context(0)
+    c2.set_factor_format("f16x2")
+    c2.set_mixed(max_refine=1)
+    c2.set_offsets_from_tomo(t)
+    dC, dT = dev(Cmm), dev(Ctm)
+    M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=c2)
+    c2.synchronize()
+    err = O.rel_fro(host(dT), R_ref)
+    assert err <= 1e-5, err
+    c2.close()

@@ -91,3 +91,71 @@ def test_int8_scaled_fp64(ctx, Mr, Nr, K, pairs):
                                    dec.data_ptr(), shift, 0), "tc_gemm int8")
     got = dC.cpu().numpy().T
     assert np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-300)) < 1e-15
+
+
+def test_f16_scaled_products(ctx):
+    """fp16 operands stored scaled by 2^-e per row (two slices, 3 products): the
+    epilogue's 2^(erow[r] + ecol[c]) restores the product of the unscaled values
+    to ~2^-22 relative; rows span 2^-30..2^20 in magnitude."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(5)
+    Mr, Nr, K = 320, 260, 192
+    X = torch.randn(Mr, K, device="cuda", generator=g, dtype=torch.float64)
+    Y = torch.randn(Nr, K, device="cuda", generator=g, dtype=torch.float64)
+    X *= torch.pow(2.0, torch.randint(-30, 20, (Mr, 1), device="cuda", generator=g).double())
+    Y *= torch.pow(2.0, torch.randint(-30, 20, (Nr, 1), device="cuda", generator=g).double())
+
+    def slices(Z):
+        e = torch.frexp(Z.abs().amax(dim=1)).exponent.to(torch.int32) - 14
+        s = Z * torch.pow(2.0, -e.double())[:, None]
+        hi = s.to(torch.float16)
+        lo = (s - hi.double()).to(torch.float16)
+        return torch.stack([hi, lo]).contiguous(), e.contiguous()
+    A, ea = slices(X)
+    B, eb = slices(Y)
+    Cm = torch.zeros(Nr, Mr, device="cuda")
+    pairs = [(1, 0), (0, 1), (0, 0)]
+    check(lib().moao_debug_tc_gemm(ctx.handle, 2, Mr, Nr, K, A.data_ptr(), K, 2, B.data_ptr(), K, 2,
+                                   3, _ints([p[0] for p in pairs]), _ints([p[1] for p in pairs]),
+                                   Cm.data_ptr(), Mr, -1.0, 0.0, ea.data_ptr(), eb.data_ptr(), 0, 0),
+          "tc_gemm f16")
+    want = -(X @ Y.T)
+    got = Cm.T.double()
+    # error relative to each entry's natural scale |x_r| |y_c| sqrt(K)
+    scale = X.abs().amax(1)[:, None] * Y.abs().amax(1)[None, :] * K ** 0.5
+    err = ((got - want).abs() / scale).max().item()
+    assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("kind,lower", [(0, 1), (2, 0), (2, 1)])
+def test_accumulate_epilogue_through_tma_reduce(ctx, kind, lower):
+    """beta = 1 with a 16-byte aligned C and ldc % 4 == 0 takes the TMA reduce-add
+    epilogue: C += alpha * products, entries above the diagonal (lower = 1) and
+    outside M x N (M, N not multiples of 32) left untouched."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(7 + kind + lower)
+    Mr, Nr, K = 300, 220 if not lower else 300, 128
+    ldc = 304
+    dt = torch.bfloat16 if kind == 0 else torch.float16
+    A = torch.randn(1, Mr, K, device="cuda", generator=g).to(dt)
+    B = torch.randn(1, Nr, K, device="cuda", generator=g).to(dt)
+    Cfull = torch.randn(Nr + 1, ldc, device="cuda", generator=g)   # column-major, ld 304, spare column
+    C0 = Cfull.clone()
+    ea = torch.full((Mr,), 1, dtype=torch.int32, device="cuda")
+    eb = torch.full((Nr,), -2, dtype=torch.int32, device="cuda")
+    exps = kind == 2
+    check(lib().moao_debug_tc_gemm(ctx.handle, kind, Mr, Nr, K, A.data_ptr(), K, 1, B.data_ptr(), K, 1,
+                                   1, _ints([0]), _ints([0]), Cfull.data_ptr(), ldc, -0.5, 1.0,
+                                   ea.data_ptr() if exps else None, eb.data_ptr() if exps else None,
+                                   0, lower), "tc_gemm reduce")
+    prod = (A[0].float() @ B[0].float().T) * (0.5 if exps else 1.0)   # 2^(1-2) with exponents
+    want = C0.clone()
+    upd = -0.5 * prod.T                                                # [Nr, Mr] in C's layout
+    if lower:
+        r = torch.arange(Mr, device="cuda")[None, :]
+        c = torch.arange(Nr, device="cuda")[:, None]
+        upd = torch.where(r >= c, upd, torch.zeros_like(upd))
+    want[:Nr, :Mr] += upd
+    err = (Cfull - want).abs().max() / upd.abs().max()
+    assert err < 1e-5, float(err)
+    assert torch.equal(Cfull[:, Mr:], C0[:, Mr:]) and torch.equal(Cfull[Nr:], C0[Nr:])
