@@ -75,8 +75,42 @@ __device__ __forceinline__ double dphi_unit(double x) {
   return -0.5 * (x2a * pg + z * pa);
 }
 
+// The same function of s = x^2, without the square root and cube root:
+// y = s^(-1/6) = x^(-1/3) by Newton's iteration for y^-6 = s,
+//   y <- y (7 - s y^6) / 6        (quadratic convergence, no division),
+// started from a single-precision seed 2^(-log2(s) / 6) (relative error
+// ~1e-6, so two steps reach double precision). Then x^(5/3) = s y, x = s y^3,
+// 1/x = y^3 and x^(1/3) = x y^2. Below s = 1e-30 (a float seed would lose
+// range) the direct form is used. Not inlined: the 9 or 16 stencil points of
+// a layer call one copy, which keeps the kernel inside the instruction cache
+// (inlined, the kernel stalled on instruction fetch; this form is ~8% faster).
+__device__ __noinline__ double dphi_unit_s(double s) {
+  if (!(s > 1e-30)) return s > 0 ? dphi_unit(sqrt(s)) : 0.0;
+  double y = (double)exp2f(__log2f((float)s) * (-1.0f / 6.0f));
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const double y2 = y * y;
+    y = y * fma(-s, y2 * y2 * y2, 7.0) * (1.0 / 6.0);
+  }
+  const double y3 = y * y * y;
+  const double x = s * y3;
+  if (x > kXlim) {
+    const double xi = y3;
+    return kK2 - kK3 * exp(-x) * (x * y * y) * (1.0 + xi * (kA1 + xi * (kA2 + xi * kA3)));
+  }
+  const double x53 = s * y;        // x^(5/3)
+  const double z = 0.25 * s;       // (x/2)^2
+  double pg = c_Gma[10];
+#pragma unroll
+  for (int n = 9; n >= 0; --n) pg = fma(pg, z, c_Gma[n]);
+  double pa = c_Ga[10];
+#pragma unroll
+  for (int n = 9; n >= 1; --n) pa = fma(pa, z, c_Ga[n]);
+  return -0.5 * (x53 * pg + z * pa);
+}
+
 __device__ __forceinline__ double D(double x, double y, double tpl) {
-  return dphi_unit(tpl * sqrt(x * x + y * y));
+  return dphi_unit_s((tpl * tpl) * (x * x + y * y));
 }
 
 constexpr int kMaxJobs = 160;
