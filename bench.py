@@ -213,13 +213,13 @@ def fp64_peak_tflops(torch):
     return 2 * n ** 3 / best / 1e9
 
 
-def read_traffic_ratio(name):
-    """bytes of DRAM traffic per unit of work of a kernel, from its committed ncu
-    summary (line 'dram_bytes_per_work: X'), or None."""
+def read_traffic_ratio(name, key="dram_bytes_per_work"):
+    """A figure from a committed ncu summary (line 'key: X'), by default the
+    bytes of DRAM traffic per unit of work of the kernel, or None."""
     p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
-            if line.startswith("dram_bytes_per_work:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
@@ -555,7 +555,7 @@ def main():
                                          main_run["launches"], main_run["clocks"])
     value = world * args.steps / (total_ms / 1000.0)
     stats = {f: ctx.kernel_stats(f) for f in ("gemm_f64", "matcov", "matcov_table", "potrf_leaf",
-                                              "tc_bf16", "tc_int8")}
+                                              "tc_split", "tc_int8")}
 
     # The mixed path is reported beside the FP64 path of the same build: its
     # builds/s in this run and the relative Frobenius error of R between them.
@@ -596,33 +596,61 @@ def main():
         e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(geom_bytes), "d2h_bytes_per_step": int(nm * nts * 8)}
 
-    # ---- roofline of the dominant kernel (largest share of device time)
+    # ---- roofline of the dominant kernel family (largest share of device time),
+    # and of the largest tensor-core family beside it
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak_src = "of measured" if peaks else "of fallback"
+
+    def roofline_of(fam):
+        s = stats[fam]
+        if s["ms"] <= 0 or s["launches"] <= 0:
+            return None
+        share = round(s["ms"] / total_ms, 4)
+        if fam == "gemm_f64":
+            peak = fp64_peak_tflops(torch)
+            achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
+            ratio = read_traffic_ratio("gemm_f64_elt.txt")
+            return {"kernel": "gemm_f64_kernel (FP64 DMMA m16n8k16)", "bound": "tensor",
+                    "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                    "frac": round(achieved / peak, 4),
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
+                    "traffic": (ratio * s["work"] / s["launches"]) if ratio else None,
+                    "launches": s["launches"], "share": share}
+        if fam in ("tc_split", "tc_int8"):
+            bf16 = float(peaks.get("bf16_tflops", 1590.0))
+            peak = bf16 * (2.0 if fam == "tc_int8" else 1.0)
+            achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
+            what = "int8" if fam == "tc_int8" else "fp16/bf16 split"
+            return {"kernel": f"tc_gemm_kernel ({what} tcgen05, TMA, TMEM)", "bound": "tensor",
+                    "achieved": round(achieved, 3), "peak": round(peak, 3),
+                    "unit": "TFLOP/s" if fam == "tc_split" else "TOP/s",
+                    "frac": round(achieved / peak, 4),
+                    "peak_source": (f"bf16_tflops (burst) {peak_src}" if fam == "tc_split" else
+                                    f"2 x bf16_tflops {peak_src} (the dense int8 rate is twice bf16)"),
+                    "traffic": None, "launches": s["launches"], "share": share}
+        if fam == "matcov":
+            # HBM framing (bytes stored); the kernel itself is bound by its FP64 pipe
+            hbm = float(peaks.get("hbm_gbs", 6650.0))
+            bytes_alg = 8.0 * s["work"]
+            achieved = bytes_alg / (s["ms"] / 1000.0) / 1e9
+            ratio = read_traffic_ratio("matcov_block_elt.txt")
+            pipe = read_traffic_ratio("matcov_block_elt.txt", "fp64_pipe_active")
+            return {"kernel": "matcov_block_kernel (covariance generation, FP64)", "bound": "hbm",
+                    "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                    "frac": round(achieved / hbm, 5), "peak_source": f"hbm_gbs {peak_src}",
+                    "traffic": (8.0 * s["work"] / s["launches"]),
+                    "traffic_note": ("bytes stored per launch; at ELT size Cmm (18 GB) exceeds L2 so "
+                                     "DRAM writes equal them (ncu on a small case: "
+                                     f"{ratio} B per element, the rest still in L2)"),
+                    "real_bound": "FP64 pipe", "fp64_pipe_active": pipe,
+                    "launches": s["launches"], "share": share}
+        return {"kernel": fam, "ms": s["ms"], "share": share}
+
     fam = max(stats, key=lambda f: stats[f]["ms"])
-    s = stats[fam]
-    roof = None
-    if fam == "gemm_f64" and s["ms"] > 0:
-        peak = fp64_peak_tflops(torch)
-        achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
-        ratio = read_traffic_ratio("gemm_f64_elt.txt")
-        roof = {"kernel": "gemm_f64_kernel (FP64 DMMA m16n8k16)", "bound": "tensor",
-                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4),
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "traffic": (ratio * s["work"] / s["launches"]) if ratio else None,
-                "launches": s["launches"], "share": round(s["ms"] / total_ms, 4)}
-    elif fam in ("tc_bf16", "tc_int8") and s["ms"] > 0:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
-        peak = float(peaks.get("bf16_tflops", 1590.0)) * (2.0 if fam == "tc_int8" else 1.0)
-        achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
-        roof = {"kernel": f"tc_gemm_kernel ({'int8' if fam == 'tc_int8' else 'bf16'} tcgen05, TMA, TMEM)",
-                "bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
-                "unit": "TFLOP/s" if fam == "tc_bf16" else "TOP/s", "frac": round(achieved / peak, 4),
-                "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst)" if fam == "tc_bf16" else
-                                "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate is twice bf16)"),
-                "traffic": None, "launches": s["launches"], "share": round(s["ms"] / total_ms, 4)}
-    elif s["ms"] > 0:
-        roof = {"kernel": fam, "ms": s["ms"], "share": round(s["ms"] / total_ms, 4)}
+    roof = roofline_of(fam)
+    tensor_fams = [f for f in ("tc_split", "tc_int8", "gemm_f64") if f != fam and stats[f]["ms"] > 0]
+    roof_tensor = roofline_of(max(tensor_fams, key=lambda f: stats[f]["ms"])) if tensor_fams else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -630,7 +658,8 @@ def main():
         "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.path == "fp64" else
-                 "bf16x3 split (fp32 accumulate) tensor-core updates + f64 diagonal blocks + int8 Ozaki f64 residual",
+                 ("fp16x2 row-scaled split (fp32 accumulate) tensor-core updates + f64 diagonal blocks "
+                  "+ int8 Ozaki f64 residual"),
         "data": "synthetic (seeded ELT-scale system; reference parameter-file format)",
         "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "path": args.path,
                    "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": nb_main,
@@ -640,6 +669,7 @@ def main():
         "rel_fro_err_R_vs_fp64": rel_err,
         "fp64_path": fp64_arm,
         "roofline": roof,
+        "roofline_tensor": roof_tensor,
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": e2e,

@@ -126,7 +126,7 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
   g.C = C;
   g.ldc = ldc;
   g.err = err;
-  KernelTimer kt(ctx, "tc_bf16", flops * pr.n);
+  KernelTimer kt(ctx, "tc_split", flops * pr.n);
   return tc_gemm(g, ctx->stream, &ctx->launches);
 }
 
