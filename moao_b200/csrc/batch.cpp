@@ -292,6 +292,7 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
         MOAO_TRY(sc->ws_dinv.ensure(z.dinv));
         MOAO_TRY(sc->ws_w.ensure(z.dinv));
         MOAO_TRY(sc->mx_exps.ensure(z.exps));
+        MOAO_TRY(sc->mx_dsl.ensure(z.dsl));
         if (nro > 0) {
           MOAO_TRY(sc->mx_rid.ensure(sizeof(int) * (size_t)in.n));
           MOAO_TRY(sc->mx_y.ensure(sizeof(float) * (size_t)128 * in.n));

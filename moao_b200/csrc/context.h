@@ -59,7 +59,7 @@ struct moao_ctx {
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
-  moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv, mx_exps;
+  moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv, mx_exps, mx_dsl;
   long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
   // Block-constant offsets of Cmm known to the caller (moao_ctx_set_offsets):
   // the mixed path factors Cmm minus them and adds them back exactly.
@@ -87,7 +87,8 @@ struct moao_ctx {
   std::vector<moao::DevBuf*> workspaces() {
     return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
             &mx_w1, &mx_w2,   &mx_x,    &mx_r64, &mx_e64, &mx_qa,  &mx_qb,    &mx_ea,
-            &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv, &mx_exps};
+            &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv, &mx_exps,
+            &mx_dsl};
   }
   // Device bytes held by the workspaces and the geometry caches.
   size_t bytes_held() {
@@ -134,10 +135,10 @@ moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long 
 // nsl bf16 slices, ns int8 slices and nranges declared offset ranges.
 struct MixedSizes {
   size_t a32 = 0, lr = 0, t32 = 0, w = 0, x = 0, r64 = 0, qa = 0, qb = 0, ea = 0, fb = 0,
-         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0, exps = 0;
+         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0, exps = 0, dsl = 0;
   size_t total() const {
     return a32 + 2 * lr + t32 + 2 * w + x + 2 * r64 + qa + qb + ea + fb + colmax + norm +
-           2 * dinv + info + offsets + exps;
+           2 * dinv + info + offsets + exps + dsl;
   }
 };
 MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges);

@@ -76,6 +76,9 @@ struct Maps {
   TcTensor lcB[kMaxBfSlices];  // Lc slices as B operands
   TcTensor xA[kMaxBfSlices];   // solve-panel slices as A operands (m rows)
   TcTensor yA[kMaxBfSlices];   // the same slices for the 128-row offset solve
+  TcTensor pA[kMaxBfSlices];   // the same slices for a factor panel (nmeas rows)
+  TcTensor drB[kMaxBfSlices];  // rows of the inverse diagonal blocks (fp16 format)
+  TcTensor dcB[kMaxBfSlices];  // columns of the inverse diagonal blocks (fp16 format)
 };
 
 constexpr long kYRows = 128;  // rows of the offset-indicator solve (one tile)
@@ -139,6 +142,8 @@ struct Scales {
   int* erp = nullptr;
   int* ecf = nullptr;
   int* ex = nullptr;
+  int* edr = nullptr;  // row exponents of the inverse diagonal blocks (indexed by global row)
+  int* edc = nullptr;  // column exponents of the inverse diagonal blocks
 };
 constexpr int kF16Bias = 14;  // stored slices below 2^14 in magnitude (fp16 max 65504)
 
@@ -146,9 +151,51 @@ constexpr int kF16Bias = 14;  // stored slices below 2^14 in magnitude (fp16 max
 moao_status split_block(const Scales& sc, const double* W2, long m, long kb, int slices,
                         const BfSlices& xr, long ldx, cudaStream_t s) {
   BfSlices none{};
+  const long kpad = std::min(round_up(kb, 64), ldx);
+  if (kpad > kb)  // the tensor core reads K in steps of 64: padding columns must hold zeros
+    for (int k = 0; k < slices; ++k)
+      MOAO_CUDA_TRY(cudaMemset2DAsync(static_cast<uint16_t*>(xr.p[k]) + kb, ldx * sizeof(uint16_t),
+                                      0, (kpad - kb) * sizeof(uint16_t), m, s));
   if (!sc.f16) return split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s);
   MOAO_TRY(scale_exponents(W2, m, m, kb, kF16Bias, sc.ex, nullptr, s));
   return split_f16(W2, m, m, kb, slices, xr, ldx, sc.ex, none, 0, nullptr, s);
+}
+
+// fp16 format: C32 (m x kb, ldc) = W (m x kb, FP64) times the inverse diagonal
+// block starting at row k0, transposed (forward: Dinv^T, rows of the drB copy)
+// or not (backward: Dinv, rows of the dcB copy), on the tensor cores.
+moao_status block_product(moao_ctx* ctx, const Scales& sc, const TcTensor* A, const double* W,
+                          long m, long k0, long kb, const TcTensor* B, const int* eB,
+                          const Products& pr, float* C32, long ldc, const BfSlices& xr, long ldx,
+                          int slices, int* err) {
+  MOAO_TRY(split_block(sc, W, m, kb, slices, xr, ldx, ctx->stream));
+  TcGemm g;
+  g.kind = A[0].kind;
+  g.epi = kTcEpiF32;
+  g.M = m;
+  g.N = kb;
+  int na = 0, nbm = 0;
+  for (int p = 0; p < pr.n; ++p) {
+    na = std::max(na, pr.a[p] + 1);
+    nbm = std::max(nbm, pr.b[p] + 1);
+  }
+  for (int i = 0; i < na; ++i) g.A[i] = &A[i];
+  for (int i = 0; i < nbm; ++i) g.B[i] = &B[i];
+  g.nA = na;
+  g.nB = nbm;
+  for (int p = 0; p < pr.n; ++p)
+    g.seg[p] = TcSegment{pr.a[p], pr.b[p], 0, 0, (int)((kb + 63) / 64), 0};
+  g.nseg = pr.n;
+  g.b_row0 = (int)k0;
+  g.alpha = 1.f;
+  g.beta = 0.f;
+  g.C = C32;
+  g.ldc = ldc;
+  g.erow = sc.ex;
+  g.ecol = eB + k0;
+  g.err = err;
+  KernelTimer kt(ctx, "tc_split", 2.0 * m * kb * kb * pr.n);
+  return tc_gemm(g, ctx->stream, &ctx->launches);
 }
 
 // In-place mixed solve on T32 (m x n, ld m): T <- T L^-T L^-1, with the long
@@ -164,8 +211,14 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
   for (long k0 = 0; k0 < n; k0 += nb) {
     const long kb = std::min(nb, n - k0);
     MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
-    MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, true, 0.0, W2, m));
-    MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    if (sc.f16) {
+      MOAO_TRY(block_product(ctx, sc, xA, W1, m, k0, kb, mp.drB, sc.edr, pr, T32 + k0 * m, m,
+                             xr, ldx, slices, err));
+      MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W2, m, m, kb, false, s));
+    } else {
+      MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, true, 0.0, W2, m));
+      MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    }
     const long rest = n - k0 - kb;
     if (rest > 0) {
       MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
@@ -179,8 +232,14 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
   for (long b = nblk - 1; b >= 0; --b) {
     const long k0 = b * nb, kb = std::min(nb, n - k0);
     MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
-    MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
-    MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    if (sc.f16) {
+      MOAO_TRY(block_product(ctx, sc, xA, W1, m, k0, kb, mp.dcB, sc.edc, pr, T32 + k0 * m, m,
+                             xr, ldx, slices, err));
+      MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W2, m, m, kb, false, s));
+    } else {
+      MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
+      MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+    }
     if (k0 > 0) {
       MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
       MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
@@ -210,7 +269,9 @@ MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
   z.norm = sizeof(double) * 2;
   z.dinv = sizeof(double) * (size_t)std::max(n, 1L) * nb;
   z.info = 3 * sizeof(int);
-  z.exps = sizeof(int) * ((size_t)((n + nb - 1) / nb) * n + (size_t)n + (size_t)std::max(m, 128L));
+  z.exps = sizeof(int) * ((size_t)((n + nb - 1) / nb) * n + (size_t)n +
+                          (size_t)std::max(std::max(m, n), 128L) + 2 * (size_t)n);
+  z.dsl = 2 * nsl * sizeof(uint16_t) * (size_t)n * nb;
   if (nranges > 0)
     z.offsets = sizeof(int) * (size_t)n + sizeof(float) * (size_t)128 * n +
                 sizeof(double) * ((size_t)nranges * n + (size_t)std::max(m, (long)nranges) * nranges +
@@ -264,6 +325,14 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   sc.erp = ctx->mx_exps.as<int>();
   sc.ecf = sc.erp + (size_t)((n + nb - 1) / nb) * n;
   sc.ex = sc.ecf + n;
+  sc.edr = sc.ex + std::max(std::max(m, n), 128L);
+  sc.edc = sc.edr + n;
+  uint16_t *dr = nullptr, *dcl = nullptr;  // inverse diagonal blocks: row / column copies
+  if (f16) {
+    MOAO_TRY(ctx->mx_dsl.ensure(z.dsl));
+    dr = ctx->mx_dsl.as<uint16_t>();
+    dcl = dr + (size_t)nsl * n * nb;
+  }
   float* A32 = ctx->mx_a32.as<float>();
   uint16_t* lr = ctx->mx_lr.as<uint16_t>();
   uint16_t* lc = ctx->mx_lc.as<uint16_t>();
@@ -314,7 +383,14 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(make_tc_map(&mp.lcB[k], lck, tck, n, n, ldn, 256));
     MOAO_TRY(make_tc_map(&mp.xA[k], xs[k], tck, m, nb, ldx));
     MOAO_TRY(make_tc_map(&mp.yA[k], xs[k], tck, kYRows, nb, ldx));
+    if (f16) {
+      MOAO_TRY(make_tc_map(&mp.pA[k], xs[k], tck, n, nb, ldx));
+      MOAO_TRY(make_tc_map(&mp.drB[k], dr + (size_t)k * n * nb, tck, n, nb, nb, 256));
+      MOAO_TRY(make_tc_map(&mp.dcB[k], dcl + (size_t)k * n * nb, tck, n, nb, nb, 256));
+    }
   }
+  BfSlices xsl{};
+  for (int k = 0; k < nsl; ++k) xsl.p[k] = xs[k];
   const int csl = std::max(2, std::min(nsl, ctx->corr_slices));
   const Products full = products_for(nsl), corr = products_for(csl);
 
@@ -328,18 +404,38 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, 3 * sizeof(int), s));
     if (nro > 0) MOAO_TRY(fill_range_ids(rid, n, off, s));
     MOAO_TRY(cvt_lower_minus_offsets(Cmm, ldCmm, A32, n, n, rid, off, s));
+    // the ragged last diagonal block leaves K columns of its copies unused: zeros
+    if (f16) MOAO_CUDA_TRY(cudaMemsetAsync(dr, 0, z.dsl, s));
     for (long k0 = 0; k0 < n; k0 += nb) {
       const long kb = std::min(nb, n - k0);
       float* Akk = A32 + k0 + k0 * n;
       MOAO_TRY(cvt_f32_to_f64(Akk, n, W1, kb, kb, kb, true, s));
       MOAO_TRY(potrf_inv_block(ctx, W1, kb, dinv + k0, n, kb, k0, d_info, ctx->ws_w.as<double>()));
       MOAO_TRY(cvt_f64_to_f32(W1, kb, Akk, n, kb, kb, true, s));
+      if (f16) {
+        // fp16 copies of the inverse diagonal block: its rows (for X Dinv^T) and its
+        // columns (for X Dinv), each scaled by a power of two per row
+        BfSlices br{}, bc{};
+        for (int k = 0; k < nsl; ++k) {
+          br.p[k] = dr + (size_t)k * n * nb + (size_t)k0 * nb;
+          bc.p[k] = dcl + (size_t)k * n * nb + (size_t)k0 * nb;
+        }
+        MOAO_TRY(scale_exponents(dinv + k0, n, kb, kb, kF16Bias, sc.edr + k0, sc.edc + k0, s));
+        MOAO_TRY(split_f16(dinv + k0, n, kb, kb, nsl, br, nb, sc.edr + k0, bc, nb, sc.edc + k0, s));
+      }
       const long rest = n - k0 - kb;
       if (rest <= 0) break;
       float* P = A32 + (k0 + kb) + k0 * n;
       MOAO_TRY(cvt_f32_to_f64(P, n, W1, rest, rest, kb, false, s));
-      MOAO_TRY(gemm(ctx, rest, kb, kb, 1.0, W1, rest, dinv + k0, n, true, 0.0, W2, rest));
-      MOAO_TRY(cvt_f64_to_f32(W2, rest, P, n, rest, kb, false, s));
+      if (f16) {
+        // panel P <- P Dinv^T on the tensor cores, then its FP64 copy for the split
+        MOAO_TRY(block_product(ctx, sc, mp.pA, W1, rest, k0, kb, mp.drB, sc.edr, full, P, n, xsl,
+                               ldx, nsl, err));
+        MOAO_TRY(cvt_f32_to_f64(P, n, W2, rest, rest, kb, false, s));
+      } else {
+        MOAO_TRY(gemm(ctx, rest, kb, kb, 1.0, W1, rest, dinv + k0, n, true, 0.0, W2, rest));
+        MOAO_TRY(cvt_f64_to_f32(W2, rest, P, n, rest, kb, false, s));
+      }
       BfSlices rr{}, cc{};
       for (int k = 0; k < nsl; ++k) {
         rr.p[k] = lr + (size_t)k * n * ldn + (k0 + kb) * ldn + k0;
