@@ -86,10 +86,45 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometr
     cr[2 * i] = (int)std::lround((t.X[i] - bornemin) / g.pitch - 0.5);
     cr[2 * i + 1] = (int)std::lround((t.Y[i] - bornemin) / g.pitch - 0.5);
   }
+  // cell -> valid index of the common grid, and the tiles that hold valid cells
+  const int N = g.nssp_grid;
+  std::vector<int> cell((size_t)N * N, -1);
+  for (int i = 0; i < ngrid; ++i)
+    if (cr[2 * i] >= 0 && cr[2 * i] < N && cr[2 * i + 1] >= 0 && cr[2 * i + 1] < N)
+      cell[(size_t)cr[2 * i + 1] * N + cr[2 * i]] = i;
+  std::vector<int> ta, tb;
+  auto tiles = [&](int T, std::vector<int>& out) {
+    for (int r0 = 0; r0 < N; r0 += T)
+      for (int c0 = 0; c0 < N; c0 += T) {
+        bool any = false;
+        for (int r = r0; r < std::min(N, r0 + T) && !any; ++r)
+          for (int c = c0; c < std::min(N, c0 + T) && !any; ++c) any = cell[(size_t)r * N + c] >= 0;
+        if (any) {
+          out.push_back(c0);
+          out.push_back(r0);
+        }
+      }
+  };
+  tiles(4, ta);
+  tiles(8, tb);
+  g.ntiles_a = (int)ta.size() / 2;
+  g.ntiles_b = (int)tb.size() / 2;
+  g.bornemin = bornemin;
+  for (int w = 0; w < nW; ++w) {
+    bool ok = g.G[w] == 1.0 && g.cth[w] == 1.0 && g.sth[w] == 0.0 && t.Nssp[w] == N &&
+              t.Nsubap[w] == ngrid && N > 1;
+    for (int l = 0; l < nL && ok; ++l) {
+      const double sz = t.sspSizeL[(size_t)w * nL + l];
+      const double spacing = g.pitch * (1. - t.atm.h[l] * g.gsAlt[w]);
+      ok = std::fabs(sz - spacing) <= 1e-12 * std::fabs(sz);
+    }
+    g.aligned[w] = ok ? 1 : 0;
+  }
   int npairs = 0;
   const long ntab = toeplitz_table_doubles(g, &npairs);
   const size_t tab_doubles = npairs ? (size_t)ntab + (size_t)npairs /* pair list */ + 4 : 0;
-  const size_t grid_doubles = ((size_t)ngrid * 2 * sizeof(int) + 7) / 8;
+  const size_t grid_doubles =
+      ((size_t)ngrid * 2 * sizeof(int) + cell.size() * sizeof(int) + (ta.size() + tb.size()) * sizeof(int) + 7) / 8;
   const size_t total = 2 * nu + 2 * Nx + 3 * (size_t)Nx + nngs + nlay;
   // table base rounded up to 32 doubles (256 bytes): the gather reads double4
   const size_t tab_off = (total + grid_doubles + 31) / 32 * 32;
@@ -123,8 +158,18 @@ moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometr
   MOAO_CUDA_TRY(cudaMemcpyAsync(d, h.data(), total * sizeof(double), cudaMemcpyHostToDevice,
                                 ctx->stream));
   g.grid_cr = reinterpret_cast<int*>(d + total);
-  MOAO_CUDA_TRY(cudaMemcpyAsync(g.grid_cr, cr.data(), cr.size() * sizeof(int),
-                                cudaMemcpyHostToDevice, ctx->stream));
+  g.cell_idx = g.grid_cr + cr.size();
+  g.tiles_a = g.cell_idx + cell.size();
+  g.tiles_b = g.tiles_a + ta.size();
+  {
+    std::vector<int> ints(cr);
+    ints.insert(ints.end(), cell.begin(), cell.end());
+    ints.insert(ints.end(), ta.begin(), ta.end());
+    ints.insert(ints.end(), tb.begin(), tb.end());
+    MOAO_CUDA_TRY(cudaMemcpyAsync(g.grid_cr, ints.data(), ints.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // pageable source goes out of scope
+  }
   g.ttab = npairs ? d + tab_off : nullptr;
   // h is pageable, so the copy has completed on return from the call above
   // only for small sizes; synchronise before h goes out of scope.

@@ -267,6 +267,217 @@ __global__ void __launch_bounds__(kTileI* kTileJ)
   if (mask & 8u) store(ry, cy, cyy);
 }
 
+// ---- Edge-aligned WFS pairs without an offset table (an LGS against an NGS or
+// the truth sensor): shared stencil points.
+//
+// On every layer the projected subaperture of such a WFS spans [centre - s,
+// centre + s] with 2 s the projected grid spacing, so its edges are the grid
+// lines between neighbouring centres. The 4-point stencils then only ever
+// evaluate DPHI at (edge or centre of i) - (edge or centre of j): XX at
+// (x-edges, y-centres), YY at (x-centres, y-edges), XY at (x-edge of i minus
+// x-centre of j, y-centre of i minus y-edge of j), YX the reverse. A block
+// handles a 4x4-cell tile of WFS m against an 8x8-cell tile of WFS n: it
+// evaluates the 4 x 1,440 distinct points of a layer once into shared memory
+// and each of its 1,024 pairs gathers its 16 values, 5.6 evaluations per pair
+// instead of 16.
+constexpr int kEA = 4, kEB = 8;                              // cells per tile side
+constexpr int kEPts = (kEA + 1) * kEA * (kEB + 1) * kEB;     // points per covariance
+constexpr int kEThreads = 256;
+constexpr int kEPairs = kEA * kEA * kEB * kEB / kEThreads;   // pairs per thread (4)
+
+struct EdgeJob {
+  int m, n;        // row WFS, column WFS
+  int rb, cb;      // global row / column of the first slope of each WFS
+  int tile_base;
+};
+
+struct EdgeLaunch {
+  int njobs, total_tiles, type;
+  int r0, c0, nrows, ncols;
+  long long ld;
+  EdgeJob jobs[kMaxJobs];
+};
+
+// Projected centre of grid column (or row) c of WFS w on a layer:
+// ((bornemin + pitch (c + 1/2)) + pup) (1 - h gsAlt) + alpha h, the same
+// expression as the host projection (tomo.cpp projectedSubap) with no rotation
+// and unit magnification.
+__device__ __forceinline__ double grid_centre(const DevGeometry& g, int c, double pup,
+                                              double rr, double shift) {
+  const double x = g.bornemin + g.pitch / 2. * (2. * c + 1.);
+  return (x + pup) * rr + shift;
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(kEThreads, 3)
+    matcov_edge_kernel(const __grid_constant__ EdgeLaunch d, const DevGeometry g,
+                       OutT* __restrict__ out) {
+  __shared__ double pts[4][kEPts];  // XX, YY, XY, YX of the current layer
+  __shared__ double exi[kEA + 1], cxi[kEA], eyi[kEA + 1], cyi[kEA];
+  __shared__ double exj[kEB + 1], cxj[kEB], eyj[kEB + 1], cyj[kEB];
+  __shared__ int s_job;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    int k = 0;
+    while (k + 1 < d.njobs && d.jobs[k + 1].tile_base <= (int)blockIdx.x) ++k;
+    s_job = k;
+  }
+  __syncthreads();
+  const EdgeJob& jb = d.jobs[s_job];
+  const int t = blockIdx.x - jb.tile_base;
+  const int ta = t % g.ntiles_a, tb = t / g.ntiles_a;
+  const int ci0 = g.tiles_a[2 * ta], ri0 = g.tiles_a[2 * ta + 1];
+  const int cj0 = g.tiles_b[2 * tb], rj0 = g.tiles_b[2 * tb + 1];
+  const int N = g.nssp_grid, m = jb.m, n = jb.n;
+  const int Nm = g.Nsubap[m], Nn = g.Nsubap[n];
+
+  // this thread's pairs: i cell tid % 16 of the 4x4 tile, j cells tid / 16 + 16 q
+  const int ai = tid % (kEA * kEA) % kEA, bi = tid % (kEA * kEA) / kEA;
+  const int ci = ci0 + ai, ri = ri0 + bi;
+  const int vi = (ci < N && ri < N) ? g.cell_idx[ri * N + ci] : -1;
+  const int r1 = d.r0 + d.nrows, c1 = d.c0 + d.ncols;
+  const bool lower = (d.type == 1 || d.type == 5);
+  auto want = [&](int r, int c) {
+    return r >= d.r0 && r < r1 && c >= d.c0 && c < c1 && (!lower || r >= c);
+  };
+  unsigned mask[kEPairs];
+  int vj[kEPairs], aj[kEPairs], bj[kEPairs];
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < kEPairs; ++q) {
+    const int jc = tid / (kEA * kEA) + (kEThreads / (kEA * kEA)) * q;
+    aj[q] = jc % kEB;
+    bj[q] = jc / kEB;
+    const int cj = cj0 + aj[q], rj = rj0 + bj[q];
+    vj[q] = (cj < N && rj < N) ? g.cell_idx[rj * N + cj] : -1;
+    mask[q] = 0;
+    if (vi >= 0 && vj[q] >= 0) {
+      const int rx = jb.rb + vi, ry = jb.rb + Nm + vi;
+      const int cx = jb.cb + vj[q], cy = jb.cb + Nn + vj[q];
+      mask[q] = (want(rx, cx) ? 1u : 0u) | (want(rx, cy) ? 2u : 0u) | (want(ry, cx) ? 4u : 0u) |
+                (want(ry, cy) ? 8u : 0u);
+    }
+    any |= mask[q] != 0;
+  }
+  if (!__syncthreads_or(any)) return;  // the whole block: nothing to write
+
+  double acc[kEPairs][4];
+#pragma unroll
+  for (int q = 0; q < kEPairs; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0;
+  const int nL = g.nLayer;
+  const double sspm = g.diam / g.Nssp[m], sspn = g.diam / g.Nssp[n];
+  const double kk = kLambda2 / (sspm * sspn);
+  for (int l = 0; l < nL; ++l) {
+    const double sml = g.layer[3 * nL + m * nL + l], snl = g.layer[3 * nL + n * nL + l];
+    if (!(sml > 0 && snl > 0)) continue;
+    const double h = g.layer[3 * nL + g.nW * nL + l];
+    const double s1 = sml * 0.5, s2 = snl * 0.5;
+    const double tpl = g.layer[l];
+    const double w = 0.5 * kk * g.layer[2 * nL + l] * g.layer[nL + l];
+    // edges and centres of the two tiles on this layer
+    if (tid < 2 * (kEA + 1)) {
+      const int e = tid % (kEA + 1);
+      const bool y = tid >= kEA + 1;
+      const double rr = 1. - h * g.gsAlt[m];
+      const double c = y ? grid_centre(g, (y ? ri0 : ci0) + e, g.YPup[m], rr, g.alphaY[m] * h)
+                         : grid_centre(g, ci0 + e, g.XPup[m], rr, g.alphaX[m] * h);
+      if (y) {
+        eyi[e] = c - s1;
+        if (e < kEA) cyi[e] = c;
+      } else {
+        exi[e] = c - s1;
+        if (e < kEA) cxi[e] = c;
+      }
+    } else if (tid >= 32 && tid < 32 + 2 * (kEB + 1)) {
+      const int e = (tid - 32) % (kEB + 1);
+      const bool y = tid - 32 >= kEB + 1;
+      const double rr = 1. - h * g.gsAlt[n];
+      const double c = y ? grid_centre(g, rj0 + e, g.YPup[n], rr, g.alphaY[n] * h)
+                         : grid_centre(g, cj0 + e, g.XPup[n], rr, g.alphaX[n] * h);
+      if (y) {
+        eyj[e] = c - s2;
+        if (e < kEB) cyj[e] = c;
+      } else {
+        exj[e] = c - s2;
+        if (e < kEB) cxj[e] = c;
+      }
+    }
+    __syncthreads();
+    // Layouts put the i-tile indices innermost: the 16 lanes of a half-warp that
+    // share a j cell then gather from consecutive words (no bank conflicts).
+    for (int p = tid; p < 4 * kEPts; p += kEThreads) {
+      const int kind = p / kEPts, r = p % kEPts;
+      double dx, dy;
+      if (kind == 0) {  // XX: [ej][rj][ei][ri]
+        const int rI = r % kEA, ei = r / kEA % (kEA + 1), rj = r / (kEA * (kEA + 1)) % kEB,
+                  ej = r / (kEA * (kEA + 1) * kEB);
+        dx = exi[ei] - exj[ej];
+        dy = cyi[rI] - cyj[rj];
+      } else if (kind == 1) {  // YY: [cj][fj][ci][fi]
+        const int fi = r % (kEA + 1), cI = r / (kEA + 1) % kEA,
+                  fj = r / ((kEA + 1) * kEA) % (kEB + 1), cj = r / ((kEA + 1) * kEA * (kEB + 1));
+        dx = cxi[cI] - cxj[cj];
+        dy = eyi[fi] - eyj[fj];
+      } else if (kind == 2) {  // XY: [cj][fj][ei][ri]
+        const int rI = r % kEA, ei = r / kEA % (kEA + 1), fj = r / (kEA * (kEA + 1)) % (kEB + 1),
+                  cj = r / (kEA * (kEA + 1) * (kEB + 1));
+        dx = exi[ei] - cxj[cj];
+        dy = cyi[rI] - eyj[fj];
+      } else {  // YX: [ej][rj][ci][fi]
+        const int fi = r % (kEA + 1), cI = r / (kEA + 1) % kEA,
+                  rj = r / ((kEA + 1) * kEA) % kEB, ej = r / ((kEA + 1) * kEA * kEB);
+        dx = cxi[cI] - exj[ej];
+        dy = eyi[fi] - cyj[rj];
+      }
+      pts[kind][r] = D(dx, dy, tpl);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kEPairs; ++q) {
+      if (!mask[q]) continue;
+      const int a = ai, b = bi, c = aj[q], e = bj[q];
+      auto XX = [&](int ei, int ej) {
+        return pts[0][((ej * kEB + e) * (kEA + 1) + ei) * kEA + b];
+      };
+      auto YY = [&](int fi, int fj) {
+        return pts[1][((c * (kEB + 1) + fj) * kEA + a) * (kEA + 1) + fi];
+      };
+      auto XY = [&](int ei, int fj) {
+        return pts[2][((c * (kEB + 1) + fj) * (kEA + 1) + ei) * kEA + b];
+      };
+      auto YX = [&](int fi, int ej) {
+        return pts[3][((ej * kEB + e) * kEA + a) * (kEA + 1) + fi];
+      };
+      // the reference's stencils (cov_XX/YY/XY/YX, matcov_kernels.cpp:147-193), in its
+      // order: right/top edges are index + 1, left/bottom edges index + 0
+      if (mask[q] & 1u)
+        acc[q][0] += (-XX(a + 1, c + 1) + XX(a + 1, c) + XX(a, c + 1) - XX(a, c)) * w;
+      if (mask[q] & 2u)
+        acc[q][1] += (-XY(a + 1, e + 1) + XY(a + 1, e) + XY(a, e + 1) - XY(a, e)) * w;
+      if (mask[q] & 4u)
+        acc[q][2] += (-YX(b + 1, c + 1) + YX(b + 1, c) + YX(b, c + 1) - YX(b, c)) * w;
+      if (mask[q] & 8u)
+        acc[q][3] += (-YY(b + 1, e + 1) + YY(b + 1, e) + YY(b, e + 1) - YY(b, e)) * w;
+    }
+    __syncthreads();
+  }
+  const long long ld = d.ld;
+#pragma unroll
+  for (int q = 0; q < kEPairs; ++q) {
+    if (!mask[q]) continue;
+    const int rx = jb.rb + vi, ry = jb.rb + Nm + vi;
+    const int cx = jb.cb + vj[q], cy = jb.cb + Nn + vj[q];
+    auto store = [&](int r, int c, double val) {
+      out[(size_t)(c - d.c0) * ld + (r - d.r0)] = (OutT)val;
+      if (d.type == 5 && r != c) out[(size_t)(r - d.c0) * ld + (c - d.r0)] = (OutT)val;
+    };
+    if (mask[q] & 1u) store(rx, cx, acc[q][0]);
+    if (mask[q] & 2u) store(rx, cy, acc[q][1]);
+    if (mask[q] & 4u) store(ry, cx, acc[q][2]);
+    if (mask[q] & 8u) store(ry, cy, acc[q][3]);
+  }
+}
+
 // Ctt (type 4): truth-sensor auto-covariance from the unprojected positions,
 // compute_element_ts_tile (common/kernels/matcov_kernels.cpp:423-483). The
 // reference indexes the truth sensor at Nsubap_ts * (nW - 1), which assumes
@@ -447,6 +658,39 @@ moao_status launch_impl(const DevGeometry& g, OutT* data, int nrows, int ncols, 
       jb.tiles_i = (jb.ni + kTileI - 1) / kTileI;
       jobs.push_back(jb);
     }
+  }
+  // Edge-aligned pairs without an offset table go to the shared-point kernel.
+  std::vector<Job> plain;
+  std::vector<EdgeJob> edge;
+  for (const Job& jb : jobs) {
+    const bool tab = g.ttab && g.tpair[jb.m][jb.n] >= 0;
+    if (!tab && jb.m != jb.n && g.aligned[jb.m] && g.aligned[jb.n] && g.cell_idx &&
+        g.ntiles_a > 0 && g.ntiles_b > 0) {
+      EdgeJob e{};
+      e.m = jb.m; e.n = jb.n; e.rb = jb.rb; e.cb = jb.cb;
+      edge.push_back(e);
+    } else {
+      plain.push_back(jb);
+    }
+  }
+  jobs.swap(plain);
+  const int per_job = g.ntiles_a * g.ntiles_b;
+  for (size_t base = 0; base < edge.size(); base += kMaxJobs) {
+    EdgeLaunch d{};
+    d.type = type_mat;
+    d.r0 = xoffset; d.c0 = yoffset; d.nrows = nrows; d.ncols = ncols; d.ld = lda;
+    int tiles = 0;
+    for (size_t k = base; k < edge.size() && k < base + kMaxJobs; ++k) {
+      EdgeJob e = edge[k];
+      e.tile_base = tiles;
+      tiles += per_job;
+      d.jobs[d.njobs++] = e;
+    }
+    d.total_tiles = tiles;
+    if (tiles == 0) continue;
+    matcov_edge_kernel<OutT><<<tiles, kEThreads, 0, s>>>(d, g, data);
+    if (launches) ++*launches;
+    MOAO_CUDA_TRY(cudaGetLastError());
   }
   // Launch in chunks of kMaxJobs jobs.
   for (size_t base = 0; base < jobs.size(); base += kMaxJobs) {

@@ -66,6 +66,15 @@ struct DevGeometry {
   // Offset tables of the equal-projection WFS pairs (see matcov.cu), or null.
   double* ttab = nullptr;
   int tpair[kMaxWfs][kMaxWfs];  // table index of the pair (m, n), or -1
+  // Edge-aligned WFS (unrotated, unit magnification, the common grid): on every
+  // layer the projected subaperture edges are the midlines between neighbouring
+  // centres, so neighbouring subapertures share stencil points (matcov.cu).
+  int aligned[kMaxWfs];
+  double bornemin = 0;          // pupil coordinate of the grid's first edge
+  int* cell_idx = nullptr;      // [nssp_grid^2]: valid index of grid cell (row * N + col), or -1
+  int* tiles_a = nullptr;       // 4x4-cell tiles holding a valid cell: (col0, row0) pairs
+  int* tiles_b = nullptr;       // 8x8-cell tiles likewise
+  int ntiles_a = 0, ntiles_b = 0;
 };
 
 // Builds the offset tables of g's equal-projection WFS pairs into g.ttab (device
