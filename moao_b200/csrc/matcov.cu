@@ -81,10 +81,12 @@ __device__ __forceinline__ double dphi_unit(double x) {
 // started from a single-precision seed 2^(-log2(s) / 6) (relative error
 // ~1e-6, so two steps reach double precision). Then x^(5/3) = s y, x = s y^3,
 // 1/x = y^3 and x^(1/3) = x y^2. Below s = 1e-30 (a float seed would lose
-// range) the direct form is used. Not inlined: the 9 or 16 stencil points of
-// a layer call one copy, which keeps the kernel inside the instruction cache
-// (inlined, the kernel stalled on instruction fetch; this form is ~8% faster).
-__device__ __noinline__ double dphi_unit_s(double s) {
+// range) the direct form is used. The per-pair kernels call the non-inlined
+// copy below: their 9 or 16 stencil points per layer then share one body,
+// which keeps them inside the instruction cache (inlined, they stalled on
+// instruction fetch; ~8% slower). The shared-point kernel has one call site
+// and inlines it.
+__device__ __forceinline__ double dphi_unit_s_inl(double s) {
   if (!(s > 1e-30)) return s > 0 ? dphi_unit(sqrt(s)) : 0.0;
   double y = (double)exp2f(__log2f((float)s) * (-1.0f / 6.0f));
 #pragma unroll
@@ -108,6 +110,8 @@ __device__ __noinline__ double dphi_unit_s(double s) {
   for (int n = 9; n >= 1; --n) pa = fma(pa, z, c_Ga[n]);
   return -0.5 * (x53 * pg + z * pa);
 }
+
+__device__ __noinline__ double dphi_unit_s(double s) { return dphi_unit_s_inl(s); }
 
 __device__ __forceinline__ double D(double x, double y, double tpl) {
   return dphi_unit_s((tpl * tpl) * (x * x + y * y));
@@ -280,10 +284,33 @@ __global__ void __launch_bounds__(kTileI* kTileJ)
 // evaluates the 4 x 1,440 distinct points of a layer once into shared memory
 // and each of its 1,024 pairs gathers its 16 values, 5.6 evaluations per pair
 // instead of 16.
+//
+// Each covariance's points form an outer sum s = a[r] + b[c] of two short
+// arrays of scaled squared 1-D separations (x part and y part), so a layer
+// first fills the 306 entries of those arrays and each point then costs one
+// addition before DPHI. Point tables are row-major [r][c]; the i-cell indices
+// (a = column, b = row of the i tile) enter rows and columns with strides that
+// map the 16 lanes of a half-warp (a, b in 0..3) onto 16 distinct banks, and
+// every stencil value of a pair sits at a compile-time offset from one of
+// three per-thread bases:
+//   XX [ix = 5 ej + ei][iy = 4 rj + ri]      stride 36, base A = (5c + a) 36 + 4e + b
+//   YY [iy = 5 fj + fi][ix = 4 cj + ci]      stride 36, base Y = (5e + b) 36 + 4c + a
+//   XY [ix = 5 cj + ei][iy = 4 fj + ri]      stride 36, base A
+//   YX [ix = 4 ej + ci][iy = 5 rj + fi]      stride 44, base X = (4c + a) 44 + 5e + b
+// (e* edge, c* centre index along x; f* edge, r* centre index along y; i
+// indices run over the 4x4 tile, j indices over the 8x8 tile.)
 constexpr int kEA = 4, kEB = 8;                              // cells per tile side
-constexpr int kEPts = (kEA + 1) * kEA * (kEB + 1) * kEB;     // points per covariance
 constexpr int kEThreads = 256;
 constexpr int kEPairs = kEA * kEA * kEB * kEB / kEThreads;   // pairs per thread (4)
+constexpr int kEKind = (kEA + 1) * kEA * (kEB + 1) * kEB;    // points per covariance (1,440)
+constexpr int kEOffYY = 45 * 36, kEOffXY = kEOffYY + 45 * 36, kEOffYX = kEOffXY + 40 * 36;
+constexpr int kEPtsTotal = kEOffYX + 36 * 44;                // 6,264 doubles
+// scaled squared separations: row array then column array of each covariance
+constexpr int kESqXXr = 0, kESqXXc = 45, kESqYYr = 77, kESqYYc = 122, kESqXYr = 154,
+              kESqXYc = 194, kESqYXr = 230, kESqYXc = 266, kESqTotal = 306;
+constexpr size_t kESmem = (size_t)(kEPtsTotal + kESqTotal) * sizeof(double);
+static_assert(kEKind == 45 * 32 && kEKind == 40 * 36 && kEKind % 32 == 0,
+              "a covariance's points must fill whole warps");
 
 struct EdgeJob {
   int m, n;        // row WFS, column WFS
@@ -312,9 +339,9 @@ template <typename OutT>
 __global__ void __launch_bounds__(kEThreads, 3)
     matcov_edge_kernel(const __grid_constant__ EdgeLaunch d, const DevGeometry g,
                        OutT* __restrict__ out) {
-  __shared__ double pts[4][kEPts];  // XX, YY, XY, YX of the current layer
-  __shared__ double exi[kEA + 1], cxi[kEA], eyi[kEA + 1], cyi[kEA];
-  __shared__ double exj[kEB + 1], cxj[kEB], eyj[kEB + 1], cyj[kEB];
+  extern __shared__ double esm[];
+  double* pts = esm;                 // XX | YY | XY | YX point tables of the current layer
+  double* sq = esm + kEPtsTotal;     // the 8 separation arrays
   __shared__ int s_job;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -331,24 +358,23 @@ __global__ void __launch_bounds__(kEThreads, 3)
   const int N = g.nssp_grid, m = jb.m, n = jb.n;
   const int Nm = g.Nsubap[m], Nn = g.Nsubap[n];
 
-  // this thread's pairs: i cell tid % 16 of the 4x4 tile, j cells tid / 16 + 16 q
-  const int ai = tid % (kEA * kEA) % kEA, bi = tid % (kEA * kEA) / kEA;
-  const int ci = ci0 + ai, ri = ri0 + bi;
+  // this thread's pairs: i cell (a, b) = tid % 16 of the 4x4 tile, j cells
+  // (c, e + 2 q) of the 8x8 tile with c = tid / 16 % 8, e = tid / 128
+  const int a = tid % kEA, b = tid / kEA % kEA;
+  const int c = tid / (kEA * kEA) % kEB, e = tid / (kEA * kEA * kEB);
+  const int ci = ci0 + a, ri = ri0 + b;
   const int vi = (ci < N && ri < N) ? g.cell_idx[ri * N + ci] : -1;
   const int r1 = d.r0 + d.nrows, c1 = d.c0 + d.ncols;
   const bool lower = (d.type == 1 || d.type == 5);
-  auto want = [&](int r, int c) {
-    return r >= d.r0 && r < r1 && c >= d.c0 && c < c1 && (!lower || r >= c);
+  auto want = [&](int r, int cc) {
+    return r >= d.r0 && r < r1 && cc >= d.c0 && cc < c1 && (!lower || r >= cc);
   };
   unsigned mask[kEPairs];
-  int vj[kEPairs], aj[kEPairs], bj[kEPairs];
+  int vj[kEPairs];
   bool any = false;
 #pragma unroll
   for (int q = 0; q < kEPairs; ++q) {
-    const int jc = tid / (kEA * kEA) + (kEThreads / (kEA * kEA)) * q;
-    aj[q] = jc % kEB;
-    bj[q] = jc / kEB;
-    const int cj = cj0 + aj[q], rj = rj0 + bj[q];
+    const int cj = cj0 + c, rj = rj0 + e + 2 * q;
     vj[q] = (cj < N && rj < N) ? g.cell_idx[rj * N + cj] : -1;
     mask[q] = 0;
     if (vi >= 0 && vj[q] >= 0) {
@@ -360,6 +386,9 @@ __global__ void __launch_bounds__(kEThreads, 3)
     any |= mask[q] != 0;
   }
   if (!__syncthreads_or(any)) return;  // the whole block: nothing to write
+  const int bA = (5 * c + a) * 36 + 4 * e + b;
+  const int bY = kEOffYY + (5 * e + b) * 36 + 4 * c + a;
+  const int bX = kEOffYX + (4 * c + a) * 44 + 5 * e + b;
 
   double acc[kEPairs][4];
 #pragma unroll
@@ -371,93 +400,69 @@ __global__ void __launch_bounds__(kEThreads, 3)
     const double sml = g.layer[3 * nL + m * nL + l], snl = g.layer[3 * nL + n * nL + l];
     if (!(sml > 0 && snl > 0)) continue;
     const double h = g.layer[3 * nL + g.nW * nL + l];
-    const double s1 = sml * 0.5, s2 = snl * 0.5;
     const double tpl = g.layer[l];
+    const double t2 = tpl * tpl;
     const double w = 0.5 * kk * g.layer[2 * nL + l] * g.layer[nL + l];
-    // edges and centres of the two tiles on this layer
-    if (tid < 2 * (kEA + 1)) {
-      const int e = tid % (kEA + 1);
-      const bool y = tid >= kEA + 1;
-      const double rr = 1. - h * g.gsAlt[m];
-      const double c = y ? grid_centre(g, (y ? ri0 : ci0) + e, g.YPup[m], rr, g.alphaY[m] * h)
-                         : grid_centre(g, ci0 + e, g.XPup[m], rr, g.alphaX[m] * h);
-      if (y) {
-        eyi[e] = c - s1;
-        if (e < kEA) cyi[e] = c;
-      } else {
-        exi[e] = c - s1;
-        if (e < kEA) cxi[e] = c;
-      }
-    } else if (tid >= 32 && tid < 32 + 2 * (kEB + 1)) {
-      const int e = (tid - 32) % (kEB + 1);
-      const bool y = tid - 32 >= kEB + 1;
-      const double rr = 1. - h * g.gsAlt[n];
-      const double c = y ? grid_centre(g, rj0 + e, g.YPup[n], rr, g.alphaY[n] * h)
-                         : grid_centre(g, cj0 + e, g.XPup[n], rr, g.alphaX[n] * h);
-      if (y) {
-        eyj[e] = c - s2;
-        if (e < kEB) cyj[e] = c;
-      } else {
-        exj[e] = c - s2;
-        if (e < kEB) cxj[e] = c;
-      }
+    // 1. separations: value = t2 ((C_m(o_m + u) - [edge] s_m/2) - (C_n(o_n + v) - [edge] s_n/2))^2
+    for (int k = tid; k < kESqTotal; k += kEThreads) {
+      int arr, u0;
+      if (k < kESqXXc) { arr = 0; u0 = kESqXXr; }
+      else if (k < kESqYYr) { arr = 1; u0 = kESqXXc; }
+      else if (k < kESqYYc) { arr = 2; u0 = kESqYYr; }
+      else if (k < kESqXYr) { arr = 3; u0 = kESqYYc; }
+      else if (k < kESqXYc) { arr = 4; u0 = kESqXYr; }
+      else if (k < kESqYXr) { arr = 5; u0 = kESqXYc; }
+      else if (k < kESqYXc) { arr = 6; u0 = kESqYXr; }
+      else { arr = 7; u0 = kESqYXc; }
+      // axis (x = 0), i edge, j edge of each array: XXr XXc YYr YYc XYr XYc YXr YXc
+      const bool yax = (0xA6u >> arr) & 1u;     // XXc, YYr, XYc, YXc
+      const bool iedge = (0x95u >> arr) & 1u;   // XXr, YYr, XYr, YXc
+      const bool jedge = (0x65u >> arr) & 1u;   // XXr, YYr, XYc, YXr
+      const int nu = iedge ? kEA + 1 : kEA;
+      const int idx = k - u0, u = idx % nu, v = idx / nu;
+      const double rm = 1. - h * g.gsAlt[m], rn = 1. - h * g.gsAlt[n];
+      const double xm = yax ? grid_centre(g, ri0 + u, g.YPup[m], rm, g.alphaY[m] * h)
+                            : grid_centre(g, ci0 + u, g.XPup[m], rm, g.alphaX[m] * h);
+      const double xn = yax ? grid_centre(g, rj0 + v, g.YPup[n], rn, g.alphaY[n] * h)
+                            : grid_centre(g, cj0 + v, g.XPup[n], rn, g.alphaX[n] * h);
+      const double dv = (iedge ? xm - sml * 0.5 : xm) - (jedge ? xn - snl * 0.5 : xn);
+      sq[k] = t2 * (dv * dv);
     }
     __syncthreads();
-    // Layouts put the i-tile indices innermost: the 16 lanes of a half-warp that
-    // share a j cell then gather from consecutive words (no bank conflicts).
-    for (int p = tid; p < 4 * kEPts; p += kEThreads) {
-      const int kind = p / kEPts, r = p % kEPts;
-      double dx, dy;
-      if (kind == 0) {  // XX: [ej][rj][ei][ri]
-        const int rI = r % kEA, ei = r / kEA % (kEA + 1), rj = r / (kEA * (kEA + 1)) % kEB,
-                  ej = r / (kEA * (kEA + 1) * kEB);
-        dx = exi[ei] - exj[ej];
-        dy = cyi[rI] - cyj[rj];
-      } else if (kind == 1) {  // YY: [cj][fj][ci][fi]
-        const int fi = r % (kEA + 1), cI = r / (kEA + 1) % kEA,
-                  fj = r / ((kEA + 1) * kEA) % (kEB + 1), cj = r / ((kEA + 1) * kEA * (kEB + 1));
-        dx = cxi[cI] - cxj[cj];
-        dy = eyi[fi] - eyj[fj];
-      } else if (kind == 2) {  // XY: [cj][fj][ei][ri]
-        const int rI = r % kEA, ei = r / kEA % (kEA + 1), fj = r / (kEA * (kEA + 1)) % (kEB + 1),
-                  cj = r / (kEA * (kEA + 1) * (kEB + 1));
-        dx = exi[ei] - cxj[cj];
-        dy = cyi[rI] - eyj[fj];
-      } else {  // YX: [ej][rj][ci][fi]
-        const int fi = r % (kEA + 1), cI = r / (kEA + 1) % kEA,
-                  rj = r / ((kEA + 1) * kEA) % kEB, ej = r / ((kEA + 1) * kEA * kEB);
-        dx = cxi[cI] - exj[ej];
-        dy = eyi[fi] - cyj[rj];
+    // 2. points: 4 x 1,440, each covariance a whole number of warps
+    for (int p = tid; p < 4 * kEKind; p += kEThreads) {
+      const int kind = p / kEKind, f = p - kind * kEKind;
+      int r, cc, dst;
+      double sr, sc;
+      if (kind == 0) {         // XX 45 x 32
+        r = f >> 5; cc = f & 31; dst = r * 36 + cc;
+        sr = sq[kESqXXr + r]; sc = sq[kESqXXc + cc];
+      } else if (kind == 1) {  // YY 45 x 32
+        r = f >> 5; cc = f & 31; dst = kEOffYY + r * 36 + cc;
+        sr = sq[kESqYYr + r]; sc = sq[kESqYYc + cc];
+      } else if (kind == 2) {  // XY 40 x 36
+        r = f / 36; cc = f - r * 36; dst = kEOffXY + r * 36 + cc;
+        sr = sq[kESqXYr + r]; sc = sq[kESqXYc + cc];
+      } else {                 // YX 36 x 40
+        r = f / 40; cc = f - r * 40; dst = kEOffYX + r * 44 + cc;
+        sr = sq[kESqYXr + r]; sc = sq[kESqYXc + cc];
       }
-      pts[kind][r] = D(dx, dy, tpl);
+      pts[dst] = dphi_unit_s_inl(sr + sc);
     }
     __syncthreads();
+    // 3. the reference's stencils (cov_XX/YY/XY/YX, matcov_kernels.cpp:147-193), in its
+    // order: right/top edges are index + 1, left/bottom edges index + 0
 #pragma unroll
     for (int q = 0; q < kEPairs; ++q) {
       if (!mask[q]) continue;
-      const int a = ai, b = bi, c = aj[q], e = bj[q];
-      auto XX = [&](int ei, int ej) {
-        return pts[0][((ej * kEB + e) * (kEA + 1) + ei) * kEA + b];
-      };
-      auto YY = [&](int fi, int fj) {
-        return pts[1][((c * (kEB + 1) + fj) * kEA + a) * (kEA + 1) + fi];
-      };
-      auto XY = [&](int ei, int fj) {
-        return pts[2][((c * (kEB + 1) + fj) * (kEA + 1) + ei) * kEA + b];
-      };
-      auto YX = [&](int fi, int ej) {
-        return pts[3][((ej * kEB + e) * kEA + a) * (kEA + 1) + fi];
-      };
-      // the reference's stencils (cov_XX/YY/XY/YX, matcov_kernels.cpp:147-193), in its
-      // order: right/top edges are index + 1, left/bottom edges index + 0
-      if (mask[q] & 1u)
-        acc[q][0] += (-XX(a + 1, c + 1) + XX(a + 1, c) + XX(a, c + 1) - XX(a, c)) * w;
-      if (mask[q] & 2u)
-        acc[q][1] += (-XY(a + 1, e + 1) + XY(a + 1, e) + XY(a, e + 1) - XY(a, e)) * w;
-      if (mask[q] & 4u)
-        acc[q][2] += (-YX(b + 1, c + 1) + YX(b + 1, c) + YX(b, c + 1) - YX(b, c)) * w;
-      if (mask[q] & 8u)
-        acc[q][3] += (-YY(b + 1, e + 1) + YY(b + 1, e) + YY(b, e + 1) - YY(b, e)) * w;
+      const double* XX = pts + bA + 8 * q;             // XX(a + di, c + dj) at 36 di + 180 dj
+      const double* XY = pts + kEOffXY + bA + 8 * q;   // XY(a + di, e + dj) at 36 di + 4 dj
+      const double* YX = pts + bX + 10 * q;            // YX(b + di, c + dj) at di + 176 dj
+      const double* YY = pts + bY + 360 * q;           // YY(b + di, e + dj) at 36 di + 180 dj
+      if (mask[q] & 1u) acc[q][0] += (-XX[216] + XX[36] + XX[180] - XX[0]) * w;
+      if (mask[q] & 2u) acc[q][1] += (-XY[40] + XY[36] + XY[4] - XY[0]) * w;
+      if (mask[q] & 4u) acc[q][2] += (-YX[177] + YX[1] + YX[176] - YX[0]) * w;
+      if (mask[q] & 8u) acc[q][3] += (-YY[216] + YY[36] + YY[180] - YY[0]) * w;
     }
     __syncthreads();
   }
@@ -467,9 +472,9 @@ __global__ void __launch_bounds__(kEThreads, 3)
     if (!mask[q]) continue;
     const int rx = jb.rb + vi, ry = jb.rb + Nm + vi;
     const int cx = jb.cb + vj[q], cy = jb.cb + Nn + vj[q];
-    auto store = [&](int r, int c, double val) {
-      out[(size_t)(c - d.c0) * ld + (r - d.r0)] = (OutT)val;
-      if (d.type == 5 && r != c) out[(size_t)(r - d.c0) * ld + (c - d.r0)] = (OutT)val;
+    auto store = [&](int r, int cc, double val) {
+      out[(size_t)(cc - d.c0) * ld + (r - d.r0)] = (OutT)val;
+      if (d.type == 5 && r != cc) out[(size_t)(r - d.c0) * ld + (cc - d.r0)] = (OutT)val;
     };
     if (mask[q] & 1u) store(rx, cx, acc[q][0]);
     if (mask[q] & 2u) store(rx, cy, acc[q][1]);
@@ -688,7 +693,9 @@ moao_status launch_impl(const DevGeometry& g, OutT* data, int nrows, int ncols, 
     }
     d.total_tiles = tiles;
     if (tiles == 0) continue;
-    matcov_edge_kernel<OutT><<<tiles, kEThreads, 0, s>>>(d, g, data);
+    MOAO_CUDA_TRY(cudaFuncSetAttribute(matcov_edge_kernel<OutT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kESmem));
+    matcov_edge_kernel<OutT><<<tiles, kEThreads, kESmem, s>>>(d, g, data);
     if (launches) ++*launches;
     MOAO_CUDA_TRY(cudaGetLastError());
   }
