@@ -262,13 +262,9 @@ bool use_mma16() {
 
 template <bool TRANSB, bool LOWERC, int VEC, bool MMA16>
 moao_status launch_gemm_t(const KParams& p, cudaStream_t s) {
-  static bool configured = false;
+  static std::atomic<unsigned long long> configured{0};
   auto kern = gemm_f64_kernel<TRANSB, LOWERC, VEC, MMA16>;
-  if (!configured) {
-    MOAO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)SMEM_BYTES));
-    configured = true;
-  }
+  MOAO_CUDA_TRY(set_smem_limit(kern, (int)SMEM_BYTES, configured));
   dim3 grid((unsigned)((p.M + BM - 1) / BM), (unsigned)((p.N + BN - 1) / BN));
   kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(p);
   MOAO_CUDA_TRY(cudaGetLastError());
@@ -284,67 +280,141 @@ moao_status launch_gemm(const KParams& p, cudaStream_t s) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // ---------------------------------------------------------------------------
-// Leaf factorisation of a diagonal block (n <= 64) in shared memory, fused with
-// the inversion of the resulting triangular factor.
+// Leaf factorisation of a diagonal block (n <= 64), fused with the inversion of
+// the resulting triangular factor, as one more level of the block recursion
+// inside one CTA:
+//   L11, D11 = L11^-1      one warp, 32 x 32 in registers (factor_inv_32)
+//   L21 = A21 D11^T        all threads
+//   A22 -= L21 L21^T       all threads (lower)
+//   L22, D22               one warp
+//   D21 = -D22 (L21 D11)   all threads
+// In factor_inv_32 lane l holds row l. Cholesky step j: d = A(j,j) from lane
+// j, r = 1/sqrt(d), L(l,j) = A(l,j) r, then A(l,k) -= L(l,j) L(k,j) for k > j
+// with L(k,j) shuffled from lane k. Inverse (right-looking forward
+// substitution, the row reusing the factor's registers): step i, lane i turns
+// its row into row i of L^-1 (times r_i = 1/L(i,i)), and every lane l > i
+// subtracts L(l,i) times that row, shuffled from lane i.
 // ---------------------------------------------------------------------------
 constexpr int LEAF = 64;
 constexpr int LEAF_LD = LEAF + 1;
+constexpr int HALF = 32;
 
-__global__ void __launch_bounds__(256) potrf_inv_leaf_kernel(double* A, long lda, double* Linv,
-                                                             long ldi, int n, long col0,
-                                                             int* info) {
+// Factor and invert the nn x nn (nn <= 32) lower block at (o, o) of S into
+// the same place of Lo (factor) and Do (inverse). One full warp.
+__device__ __noinline__ void factor_inv_32(const double* S, double* Lo, double* Do, int o, int nn,
+                                           long col0, int* info) {
+  const int l = threadIdx.x & 31;
+  double a[HALF];
+#pragma unroll
+  for (int k = 0; k < HALF; ++k)
+    a[k] = (l < nn && k <= l) ? S[(o + l) + (o + k) * LEAF_LD] : (k == l ? 1.0 : 0.0);
+  bool reported = false;
+  double r_own = 1.0;
+#pragma unroll
+  for (int j = 0; j < HALF; ++j) {
+    double d = __shfl_sync(0xffffffffu, a[j], j);
+    if (!(d > 0.0)) {
+      // keep going without NaNs; info reports the first such column
+      if (l == 0 && !reported && j < nn) {
+        reported = true;
+        atomicCAS(info, 0, (int)(col0 + o + j + 1));
+      }
+      d = 1.0;
+    }
+    const double r = rsqrt(d);
+    const double lj = (l == j ? d : a[j]) * r;
+    a[j] = lj;
+    if (l == j) r_own = r;
+#pragma unroll
+    for (int k = j + 1; k < HALF; ++k) a[k] = fma(-lj, __shfl_sync(0xffffffffu, lj, k), a[k]);
+  }
+  if (l < nn) {
+#pragma unroll
+    for (int k = 0; k < HALF; ++k)
+      if (k <= l && k < nn) Lo[(o + l) + (o + k) * LEAF_LD] = a[k];
+  }
+#pragma unroll
+  for (int i = 0; i < HALF; ++i) {
+    const double lli = a[i];
+#pragma unroll
+    for (int c = 0; c <= i; ++c) {
+      const double wc = __shfl_sync(0xffffffffu, c == i ? r_own : a[c] * r_own, i);
+      if (l == i) a[c] = wc;
+      else if (l > i) a[c] = c == i ? -lli * wc : fma(-lli, wc, a[c]);
+    }
+  }
+  if (l < nn) {
+#pragma unroll
+    for (int k = 0; k < HALF; ++k)
+      if (k <= l && k < nn) Do[(o + l) + (o + k) * LEAF_LD] = a[k];
+  }
+}
+
+__global__ void __launch_bounds__(256, 1) potrf_inv_leaf_kernel(double* A, long lda, double* Linv,
+                                                                long ldi, int n, long col0,
+                                                                int* info) {
   extern __shared__ __align__(16) double leaf_smem[];
-  double* L = leaf_smem;                 // L[i + j*LEAF_LD]
-  double* W = leaf_smem + LEAF * LEAF_LD;  // inverse
-  __shared__ int s_bad;
+  double* S = leaf_smem;                       // input lower, later L21 D11
+  double* Lf = leaf_smem + LEAF * LEAF_LD;     // factor
+  double* Di = leaf_smem + 2 * LEAF * LEAF_LD; // inverse
   const int tid = threadIdx.x;
+  const int warp = tid >> 5;
   for (int e = tid; e < LEAF * LEAF; e += blockDim.x) {
     const int i = e % LEAF, j = e / LEAF;
-    L[i + j * LEAF_LD] = (i < n && j < n && i >= j) ? A[(long)j * lda + i] : 0.0;
-    W[i + j * LEAF_LD] = 0.0;
-  }
-  if (tid == 0) s_bad = 0;
-  __syncthreads();
-  // Right-looking column Cholesky.
-  for (int j = 0; j < n; ++j) {
-    if (tid == 0) {
-      const double d = L[j + j * LEAF_LD];
-      if (!(d > 0.0)) {
-        if (!s_bad) {
-          s_bad = 1;
-          atomicCAS(info, 0, (int)(col0 + j + 1));
-        }
-        L[j + j * LEAF_LD] = 1.0;  // keep going without NaNs; info reports it
-      } else {
-        L[j + j * LEAF_LD] = sqrt(d);
-      }
-    }
-    __syncthreads();
-    const double piv = L[j + j * LEAF_LD];
-    for (int i = j + 1 + tid; i < n; i += blockDim.x) L[i + j * LEAF_LD] /= piv;
-    __syncthreads();
-    const int rem = n - j - 1;
-    for (int e = tid; e < rem * rem; e += blockDim.x) {
-      const int i = j + 1 + e % rem, k = j + 1 + e / rem;
-      if (i >= k) L[i + k * LEAF_LD] -= L[i + j * LEAF_LD] * L[k + j * LEAF_LD];
-    }
-    __syncthreads();
-  }
-  // Inverse of the lower factor, one column per thread (forward substitution).
-  if (tid < n) {
-    const int j = tid;
-    W[j + j * LEAF_LD] = 1.0 / L[j + j * LEAF_LD];
-    for (int i = j + 1; i < n; ++i) {
-      double sum = 0.0;
-      for (int k = j; k < i; ++k) sum += L[i + k * LEAF_LD] * W[k + j * LEAF_LD];
-      W[i + j * LEAF_LD] = -sum / L[i + i * LEAF_LD];
-    }
+    S[i + j * LEAF_LD] = (i < n && j < n && i >= j) ? A[(long)j * lda + i] : 0.0;
+    Lf[i + j * LEAF_LD] = 0.0;
+    Di[i + j * LEAF_LD] = 0.0;
   }
   __syncthreads();
+  const int n1 = n < HALF ? n : HALF, n2 = n - n1;
+  if (warp == 0) factor_inv_32(S, Lf, Di, 0, n1, col0, info);
+  __syncthreads();
+  if (n2 > 0) {
+    // L21 = A21 D11^T : L21(i,k) = sum_{m <= k} A21(i,m) D11(k,m)
+    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
+      const int i = e % HALF, k = e / HALF;
+      if (i >= n2) continue;
+      double acc = 0.0;
+      for (int m = 0; m <= k; ++m) acc = fma(S[(HALF + i) + m * LEAF_LD], Di[k + m * LEAF_LD], acc);
+      Lf[(HALF + i) + k * LEAF_LD] = acc;
+    }
+    __syncthreads();
+    // A22 -= L21 L21^T (lower)
+    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
+      const int i = e % HALF, j = e / HALF;
+      if (i >= n2 || j > i) continue;
+      double acc = 0.0;
+      for (int k = 0; k < HALF; ++k)
+        acc = fma(Lf[(HALF + i) + k * LEAF_LD], Lf[(HALF + j) + k * LEAF_LD], acc);
+      S[(HALF + i) + (HALF + j) * LEAF_LD] -= acc;
+    }
+    __syncthreads();
+    if (warp == 0) factor_inv_32(S, Lf, Di, HALF, n2, col0, info);
+    __syncthreads();
+    // P = L21 D11 : P(i,m) = sum_{k >= m} L21(i,k) D11(k,m), kept where A21 was
+    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
+      const int i = e % HALF, m = e / HALF;
+      if (i >= n2) continue;
+      double acc = 0.0;
+      for (int k = m; k < HALF; ++k) acc = fma(Lf[(HALF + i) + k * LEAF_LD], Di[k + m * LEAF_LD], acc);
+      S[(HALF + i) + m * LEAF_LD] = acc;
+    }
+    __syncthreads();
+    // D21 = -D22 P : D21(i,m) = -sum_{k <= i} D22(i,k) P(k,m)
+    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
+      const int i = e % HALF, m = e / HALF;
+      if (i >= n2) continue;
+      double acc = 0.0;
+      for (int k = 0; k <= i; ++k)
+        acc = fma(Di[(HALF + i) + (HALF + k) * LEAF_LD], S[(HALF + k) + m * LEAF_LD], acc);
+      Di[(HALF + i) + m * LEAF_LD] = -acc;
+    }
+    __syncthreads();
+  }
   for (int e = tid; e < n * n; e += blockDim.x) {
     const int i = e % n, j = e / n;
-    if (i >= j) A[(long)j * lda + i] = L[i + j * LEAF_LD];
-    Linv[(long)j * ldi + i] = W[i + j * LEAF_LD];
+    if (i >= j) A[(long)j * lda + i] = Lf[i + j * LEAF_LD];
+    Linv[(long)j * ldi + i] = Di[i + j * LEAF_LD];
   }
 }
 
@@ -419,13 +489,9 @@ moao_status potrf_inv_leaf(double* A, long lda, double* Linv, long ldi, int n, l
                            int* d_info, cudaStream_t s, long long* launches) {
   if (n <= 0) return MOAO_OK;
   if (n > LEAF) return set_error(MOAO_ERR_BAD_ARG, "potrf leaf: n > 64");
-  static bool configured = false;
-  const int smem = 2 * LEAF * LEAF_LD * (int)sizeof(double);
-  if (!configured) {
-    MOAO_CUDA_TRY(cudaFuncSetAttribute(potrf_inv_leaf_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};
+  const int smem = 3 * LEAF * LEAF_LD * (int)sizeof(double);
+  MOAO_CUDA_TRY(set_smem_limit(potrf_inv_leaf_kernel, smem, configured));
   potrf_inv_leaf_kernel<<<1, 256, smem, s>>>(A, lda, Linv, ldi, n, col0, d_info);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());

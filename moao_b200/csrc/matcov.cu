@@ -693,8 +693,8 @@ moao_status launch_impl(const DevGeometry& g, OutT* data, int nrows, int ncols, 
     }
     d.total_tiles = tiles;
     if (tiles == 0) continue;
-    MOAO_CUDA_TRY(cudaFuncSetAttribute(matcov_edge_kernel<OutT>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kESmem));
+    static std::atomic<unsigned long long> configured{0};
+    MOAO_CUDA_TRY(set_smem_limit(matcov_edge_kernel<OutT>, (int)kESmem, configured));
     matcov_edge_kernel<OutT><<<tiles, kEThreads, kESmem, s>>>(d, g, data);
     if (launches) ++*launches;
     MOAO_CUDA_TRY(cudaGetLastError());

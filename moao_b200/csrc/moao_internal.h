@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -27,6 +28,21 @@ moao_status set_error(moao_status s, const std::string& msg);
     moao_status _s = (expr);           \
     if (_s != MOAO_OK) return _s;      \
   } while (0)
+
+// Raises a kernel's dynamic shared-memory limit once per device (the attribute
+// belongs to the current device's copy of the kernel; devices past 63 set it on
+// every call).
+template <typename Kernel>
+cudaError_t set_smem_limit(Kernel kern, int bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load() & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
+}
 
 // ---------------------------------------------------------------------------
 // Geometry tables resident on the device (uploaded from a Tomo_struct).

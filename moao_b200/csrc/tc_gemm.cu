@@ -577,12 +577,8 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (num_sms <= 0) num_sms = 148;
   }
-  static bool configured = false;
-  if (!configured) {
-    MOAO_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)SMEM));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};
+  MOAO_CUDA_TRY(set_smem_limit(tc_gemm_kernel, (int)SMEM, configured));
   tc_gemm_kernel<<<(unsigned)std::min<long>(total, num_sms), THREADS, SMEM, s>>>(p);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
