@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--impl", default="moao", choices=["moao", "reference"])
     p.add_argument("--path", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--nb", type=int, default=0,
-                   help="panel width (0: 512 for the mixed path, 1024 for FP64, their fastest)")
+                   help="panel width (0: 1024, the fastest for both paths)")
     p.add_argument("--nb-fp64", type=int, default=1024, help="panel width of the FP64 comparison arm")
     p.add_argument("--config", default="elt", choices=["elt", "small"])
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -263,7 +263,7 @@ def serving_main(args):
         return f * 0.129 ** (-5.0 / 3.0), h, np.full(35, 25.0)
 
     def make_server(slots):
-        srv = Server(device=0, slots=slots, nb=args.nb or 512)
+        srv = Server(device=0, slots=slots, nb=args.nb or 1024)
         ids, infos = [], []
         for y in systems:
             sf, af = os.path.join(y["dir"], "sys-params.txt"), os.path.join(y["dir"], "prof-1-atmos-night0.txt")
@@ -338,7 +338,7 @@ def serving_main(args):
                        "at_rate_requests_per_s": sustained["rate_requests_per_s"]},
         "config": {"workload": (f"{n_req} requests, nmeas log-uniform 1000-48000 over grids "
                                 f"{nssps} (ELT geometry), 35-layer seeded profiles, R + Cvv + PSF each"),
-                   "slots": args.serve_slots, "path": "mixed", "panel_nb": args.nb or 512},
+                   "slots": args.serve_slots, "path": "mixed", "panel_nb": args.nb or 1024},
         "saturation_closed_loop": sat, "sweep": sweep,
         "baseline_sequential_fp64": base,
         "speedup_vs_sequential_fp64": sat["requests_per_s"] / base["requests_per_s"],
@@ -490,7 +490,7 @@ def main():
     torch.cuda.set_stream(stream)
     ctx = M.Context(dev)
     ctx.set_stream(stream.cuda_stream)
-    nb_main = args.nb or (512 if args.path == "mixed" else 1024)
+    nb_main = args.nb or 1024
     ctx.set_block(nb_main)
     t = M.Tomo(sf, af)
     nm, nts = t.getNMeas(), t.getNMeasTS()

@@ -116,7 +116,7 @@ moao_status moao_ctx_set_host_precision(moao_ctx* ctx, moao_prec prec);
 
 /* Number of kernels this library launched on the context since creation. */
 long long moao_ctx_launch_count(const moao_ctx* ctx);
-/* Panel width of the blocked factorisation (default 512; multiple of 64). */
+/* Panel width of the blocked factorisation (default 1024; multiple of 64). */
 moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
 
 /* Options of the mixed-precision reconstructor: bf16 slices of the factor in
@@ -348,7 +348,8 @@ moao_status moao_batch_reconstructors(moao_ctx* ctx, int count, moao_batch_item*
                                       moao_batch_opts* opts);
 /* Autotuner: for each nmeas size class (< 2k, 4k, 8k, 16k, 32k, larger) present
  * in the samples, the panel width (from nb_candidates, default 128, 256, 384,
- * 512) with the shortest measured single-instance build, then the stream count
+ * 512, 768, 1024; those above nmeas skipped) with the shortest measured
+ * single-instance build, then the stream count
  * (2, 4, 8) with the shortest batch of all samples; stored on the context. */
 moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samples,
                           moao_prec prec, const int* nb_candidates, int ncand);

@@ -420,9 +420,9 @@ moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samp
                           moao_prec prec, const int* nb_candidates, int ncand) {
   if (!ctx || count <= 0 || !samples || (ncand > 0 && !nb_candidates))
     return set_error(MOAO_ERR_BAD_ARG, "autotune: bad arguments");
-  static const int def[] = {128, 256, 384, 512};
+  static const int def[] = {128, 256, 384, 512, 768, 1024};
   const int* cand = ncand > 0 ? nb_candidates : def;
-  const int nc = ncand > 0 ? ncand : 4;
+  const int nc = ncand > 0 ? ncand : (int)(sizeof(def) / sizeof(def[0]));
   const int p = prec == MOAO_PREC_MIXED;
   std::vector<double> best_ms(kClasses, 1e300);
   std::vector<int> best_nb(kClasses, 0);

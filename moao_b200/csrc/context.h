@@ -49,7 +49,7 @@ struct moao_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   long long launches = 0;
-  int nb = 512;  // outer panel width of the blocked factorisation
+  int nb = 1024;  // outer panel width of the blocked factorisation
   moao_prec host_prec = MOAO_PREC_FP64;  // precision of moao_reconstructor_host
   bool keep_cmm = false;  // mixed path: leave Cmm as given (no factor written back)
   bool graph_mode = false;  // mixed path under stream capture: no host waits or reads

@@ -20,17 +20,30 @@
 namespace moao {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int BK = 16;
 constexpr int STAGES = 4;
-constexpr int NTHREADS = 256;
 constexpr int PAD_MN = 4;  // doubles of padding on m/n-contiguous rows
 constexpr int PAD_K = 4;   // doubles of padding on k-contiguous rows
-constexpr int LDA_S = BM + PAD_MN;  // As[k][m]
-constexpr int LDB_S = BN + PAD_MN;  // Bs[k][n]   (transB)
-constexpr int LDBT_S = BK + PAD_K;  // Bs[n][k]   (!transB)
-constexpr int A_STAGE = BK * LDA_S;
-constexpr int B_STAGE = (BK * LDB_S > BN * LDBT_S) ? BK * LDB_S : BN * LDBT_S;
-constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+
+// CTA tile BM x BN; each warp computes WM x 32 (warps: BM/WM along m, BN/32
+// along n). 128x128 (8 warps of 64x32) for large products; 64x64 (4 warps of
+// 32x32) when the large tiles would leave most SMs idle (the small products of
+// the diagonal-block recursion).
+template <int BM_, int BN_, int WM_>
+struct Tile {
+  static constexpr int BM = BM_, BN = BN_, WM = WM_;
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / 32;
+  static constexpr int NTHREADS = 32 * WARPS_M * WARPS_N;
+  static constexpr int MF = WM / 8;             // 8-row fragments per warp
+  static constexpr int LDA_S = BM + PAD_MN;     // As[k][m]
+  static constexpr int LDB_S = BN + PAD_MN;     // Bs[k][n]   (transB)
+  static constexpr int LDBT_S = BK + PAD_K;     // Bs[n][k]   (!transB)
+  static constexpr int A_STAGE = BK * LDA_S;
+  static constexpr int B_STAGE = (BK * LDB_S > BN * LDBT_S) ? BK * LDB_S : BN * LDBT_S;
+  static constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+};
+using TileL = Tile<128, 128, 64>;
+using TileS = Tile<64, 64, 32>;
 
 __device__ __forceinline__ void cp_async(double* smem, const double* gmem, int vec, int valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -81,41 +94,45 @@ struct KParams {
 };
 
 // Load one BK-slice of an MN-contiguous operand (A, or B when transB): the tile
-// rows r0..r0+127 of columns k0..k0+15 of a column-major rows x K matrix.
-template <int VEC>
+// rows r0..r0+R-1 of columns k0..k0+15 of a column-major rows x K matrix (R = BM
+// = BN; both tiles are square).
+template <class TL, int VEC>
 __device__ __forceinline__ void load_mn_tile(double* s, const double* g, long ld, long rows,
                                              long K, long r0, long k0) {
-  constexpr int CH = BM / VEC;           // chunks per k column
+  constexpr int CH = TL::BM / VEC;           // chunks per k column
   constexpr int TOTAL = CH * BK;
-  for (int c = threadIdx.x; c < TOTAL; c += NTHREADS) {
+  for (int c = threadIdx.x; c < TOTAL; c += TL::NTHREADS) {
     const int kk = c / CH, rr = (c % CH) * VEC;
     const long gr = r0 + rr, gk = k0 + kk;
     int valid = 0;
     if (gk < K && gr < rows) valid = (int)min((long)VEC, rows - gr);
     const double* src = valid ? g + gk * ld + gr : g;
-    cp_async(s + kk * LDA_S + rr, src, VEC, valid);
+    cp_async(s + kk * TL::LDA_S + rr, src, VEC, valid);
   }
 }
 
 // Load one BK-slice of a K-contiguous operand (B when !transB): rows k0..k0+15
-// of columns n0..n0+127 of a column-major K x N matrix, stored Bs[n][k].
-template <int VEC>
+// of columns n0..n0+BN-1 of a column-major K x N matrix, stored Bs[n][k].
+template <class TL, int VEC>
 __device__ __forceinline__ void load_k_tile(double* s, const double* g, long ld, long N,
                                             long K, long n0, long k0) {
   constexpr int CH = BK / VEC;
-  constexpr int TOTAL = CH * BN;
-  for (int c = threadIdx.x; c < TOTAL; c += NTHREADS) {
+  constexpr int TOTAL = CH * TL::BN;
+  for (int c = threadIdx.x; c < TOTAL; c += TL::NTHREADS) {
     const int nn = c / CH, kk = (c % CH) * VEC;
     const long gn = n0 + nn, gk = k0 + kk;
     int valid = 0;
     if (gn < N && gk < K) valid = (int)min((long)VEC, K - gk);
     const double* src = valid ? g + gn * ld + gk : g;
-    cp_async(s + nn * LDBT_S + kk, src, VEC, valid);
+    cp_async(s + nn * TL::LDBT_S + kk, src, VEC, valid);
   }
 }
 
-template <bool TRANSB, bool LOWERC, int VEC, bool MMA16>
-__global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) {
+template <class TL, bool TRANSB, bool LOWERC, int VEC, bool MMA16>
+__global__ void __launch_bounds__(TL::NTHREADS) gemm_f64_kernel(const KParams p) {
+  constexpr int BM = TL::BM, BN = TL::BN, NTHREADS = TL::NTHREADS, MF = TL::MF;
+  constexpr int LDA_S = TL::LDA_S, LDB_S = TL::LDB_S, LDBT_S = TL::LDBT_S;
+  constexpr int A_STAGE = TL::A_STAGE, B_STAGE = TL::B_STAGE;
   extern __shared__ __align__(16) double smem[];
   double* As = smem;
   double* Bs = smem + STAGES * A_STAGE;
@@ -133,22 +150,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
   const int ntiles = (ke > kb) ? (int)((ke - kb + BK - 1) / BK) : 0;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int wm = (warp % TL::WARPS_M) * TL::WM, wn = (warp / TL::WARPS_M) * 32;
   const int gid = lane >> 2, tig = lane & 3;
 
-  // acc[i][j][h]: k4 layout = 8 m-frags of 8 rows x 4 n-frags x 2;
-  // k16 layout = 4 m-frags of 16 rows x 4 n-frags x 4 (viewed through acc16).
-  double acc[8][4][2];
+  // acc[i][j][h]: k4 layout = MF m-frags of 8 rows x 4 n-frags x 2;
+  // k16 layout = MF/2 m-frags of 16 rows x 4 n-frags x 4.
+  double acc[MF][4][2];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < MF; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   auto issue = [&](int stage, int t) {
     const long k0 = kb + (long)t * BK;
-    load_mn_tile<VEC>(As + stage * A_STAGE, p.A, p.lda, p.M, p.K, m0, k0);
-    if (TRANSB) load_mn_tile<VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
-    else load_k_tile<VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
+    load_mn_tile<TL, VEC>(As + stage * A_STAGE, p.A, p.lda, p.M, p.K, m0, k0);
+    if (TRANSB) load_mn_tile<TL, VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
+    else load_k_tile<TL, VEC>(Bs + stage * B_STAGE, p.B, p.ldb, p.N, p.K, n0, k0);
   };
 
 #pragma unroll
@@ -198,7 +215,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
           bf[j][r] = TRANSB ? bs[k * LDB_S + n] : bs[n * LDBT_S + k];
         }
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < MF / 2; ++i) {
         double af[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r)
@@ -211,16 +228,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
     } else {
 #pragma unroll
       for (int k4 = 0; k4 < BK; k4 += 4) {
-        double a[8], b[4];
+        double a[MF], b[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) a[i] = as[(k4 + tig) * LDA_S + wm + i * 8 + gid];
+        for (int i = 0; i < MF; ++i) a[i] = as[(k4 + tig) * LDA_S + wm + i * 8 + gid];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           if (TRANSB) b[j] = bs[(k4 + tig) * LDB_S + wn + j * 8 + gid];
           else b[j] = bs[(wn + j * 8 + gid) * LDBT_S + k4 + tig];
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < MF; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
@@ -230,7 +247,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_f64_kernel(const KParams p) 
 
   // Epilogue: C = alpha * acc + beta * C (C is not read when beta == 0).
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < MF; ++i) {
     // k4: fragment i covers rows wm + 8 i; k16: acc[2q][j] and acc[2q+1][j] hold
     // the 4 values of m16 fragment q (rows wm + 16 q + gid and + 8).
     const long r = MMA16 ? m0 + wm + (i >> 1) * 16 + (i & 1) * 8 + gid : m0 + wm + i * 8 + gid;
@@ -260,21 +277,31 @@ bool use_mma16() {
   return v;
 }
 
-template <bool TRANSB, bool LOWERC, int VEC, bool MMA16>
+template <class TL, bool TRANSB, bool LOWERC, int VEC, bool MMA16>
 moao_status launch_gemm_t(const KParams& p, cudaStream_t s) {
   static std::atomic<unsigned long long> configured{0};
-  auto kern = gemm_f64_kernel<TRANSB, LOWERC, VEC, MMA16>;
-  MOAO_CUDA_TRY(set_smem_limit(kern, (int)SMEM_BYTES, configured));
-  dim3 grid((unsigned)((p.M + BM - 1) / BM), (unsigned)((p.N + BN - 1) / BN));
-  kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(p);
+  auto kern = gemm_f64_kernel<TL, TRANSB, LOWERC, VEC, MMA16>;
+  MOAO_CUDA_TRY(set_smem_limit(kern, (int)TL::SMEM_BYTES, configured));
+  dim3 grid((unsigned)((p.M + TL::BM - 1) / TL::BM), (unsigned)((p.N + TL::BN - 1) / TL::BN));
+  kern<<<grid, TL::NTHREADS, TL::SMEM_BYTES, s>>>(p);
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
 
+// Products whose 128x128 grid would fill fewer than two waves of the 148 SMs
+// take the 64x64 tiles (4x the CTAs).
+bool small_tiles(const KParams& p) {
+  const long tiles = ((p.M + 127) / 128) * ((p.N + 127) / 128);
+  return tiles < 2 * 148;
+}
+
 template <bool TRANSB, bool LOWERC, int VEC>
 moao_status launch_gemm(const KParams& p, cudaStream_t s) {
-  return use_mma16() ? launch_gemm_t<TRANSB, LOWERC, VEC, true>(p, s)
-                     : launch_gemm_t<TRANSB, LOWERC, VEC, false>(p, s);
+  if (small_tiles(p))
+    return use_mma16() ? launch_gemm_t<TileS, TRANSB, LOWERC, VEC, true>(p, s)
+                       : launch_gemm_t<TileS, TRANSB, LOWERC, VEC, false>(p, s);
+  return use_mma16() ? launch_gemm_t<TileL, TRANSB, LOWERC, VEC, true>(p, s)
+                     : launch_gemm_t<TileL, TRANSB, LOWERC, VEC, false>(p, s);
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }

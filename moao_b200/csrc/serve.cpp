@@ -113,7 +113,7 @@ size_t bytes_of(long a, long b) { return sizeof(double) * (size_t)std::max(a, 0L
 // of the chosen path, geometry and intersample state.
 size_t footprint(const moao_server* s, const System& sys, const moao_request& r) {
   const long n = sys.nmeas, m = sys.nmeasts, a = sys.nact;
-  const long nb = s->opt.nb > 0 ? s->opt.nb : 512;
+  const long nb = s->opt.nb > 0 ? s->opt.nb : 1024;
   size_t f = bytes_of(n, n) + bytes_of(m, n);
   if (r.prec == MOAO_PREC_MIXED) {
     const int nro = sys.tomo.sys.lgsCst > 0 ? 2 * sys.tomo.sys.nLgs : 0;
