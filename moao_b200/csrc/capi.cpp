@@ -386,6 +386,12 @@ void moao_ctx_destroy(moao_ctx* c) {
     cudaEventDestroy(p.b);
   }
   for (auto e : c->event_pool) cudaEventDestroy(e);
+  for (auto& e : c->la_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->aux) {
+    cudaStreamSynchronize(c->aux);
+    cudaStreamDestroy(c->aux);
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

@@ -72,6 +72,11 @@ struct moao_ctx {
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this
   int final_residual = 0;    // evaluate the residual once more after the last correction
   cudaEvent_t ev[8] = {};
+  // Mixed factorisation lookahead: the next diagonal block is factored on aux
+  // (created on first use) while the trailing update leaves kLookaheadSms SMs free.
+  bool lookahead = true;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t la_ev[2] = {};
   // kernel timing
   bool timing = false;
   std::map<std::string, moao::FamilyStats> stats;

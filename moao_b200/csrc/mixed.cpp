@@ -82,6 +82,7 @@ struct Maps {
 };
 
 constexpr long kYRows = 128;  // rows of the offset-indicator solve (one tile)
+constexpr int kLookaheadSms = 8;  // SMs left to the diagonal block during the lookahead
 
 
 // Products s_i * s_j of bf16 slices kept for a given slice count, smallest
@@ -102,8 +103,9 @@ Products products_for(int slices) {
 moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, const TcTensor* B,
                       int b_row0, int kb, int nk, const Products& pr, long M, long N, float* C,
                       long ldc, bool lower, int* err, double flops, const int* erow = nullptr,
-                      const int* ecol = nullptr) {
+                      const int* ecol = nullptr, int max_ctas = 0) {
   TcGemm g;
+  g.max_ctas = max_ctas;
   g.kind = A[0].kind;
   g.erow = erow;
   g.ecol = ecol;
@@ -406,13 +408,17 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_TRY(cvt_lower_minus_offsets(Cmm, ldCmm, A32, n, n, rid, off, s));
     // the ragged last diagonal block leaves K columns of its copies unused: zeros
     if (f16) MOAO_CUDA_TRY(cudaMemsetAsync(dr, 0, z.dsl, s));
-    for (long k0 = 0; k0 < n; k0 += nb) {
-      const long kb = std::min(nb, n - k0);
+    // Diagonal block at k0: FP64 factor and inverse (dinv), FP32 factor back into
+    // A32, fp16 copies of the inverse. Runs on stream st.
+    auto diag_block = [&](long k0, long kb, cudaStream_t st) -> moao_status {
+      cudaStream_t keep = ctx->stream;
+      ctx->stream = st;  // potrf_inv_block launches on the context's stream
       float* Akk = A32 + k0 + k0 * n;
-      MOAO_TRY(cvt_f32_to_f64(Akk, n, W1, kb, kb, kb, true, s));
-      MOAO_TRY(potrf_inv_block(ctx, W1, kb, dinv + k0, n, kb, k0, d_info, ctx->ws_w.as<double>()));
-      MOAO_TRY(cvt_f64_to_f32(W1, kb, Akk, n, kb, kb, true, s));
-      if (f16) {
+      moao_status r = cvt_f32_to_f64(Akk, n, W1, kb, kb, kb, true, st);
+      if (r == MOAO_OK)
+        r = potrf_inv_block(ctx, W1, kb, dinv + k0, n, kb, k0, d_info, ctx->ws_w.as<double>());
+      if (r == MOAO_OK) r = cvt_f64_to_f32(W1, kb, Akk, n, kb, kb, true, st);
+      if (r == MOAO_OK && f16) {
         // fp16 copies of the inverse diagonal block: its rows (for X Dinv^T) and its
         // columns (for X Dinv), each scaled by a power of two per row
         BfSlices br{}, bc{};
@@ -420,9 +426,29 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
           br.p[k] = dr + (size_t)k * n * nb + (size_t)k0 * nb;
           bc.p[k] = dcl + (size_t)k * n * nb + (size_t)k0 * nb;
         }
-        MOAO_TRY(scale_exponents(dinv + k0, n, kb, kb, kF16Bias, sc.edr + k0, sc.edc + k0, s));
-        MOAO_TRY(split_f16(dinv + k0, n, kb, kb, nsl, br, nb, sc.edr + k0, bc, nb, sc.edc + k0, s));
+        r = scale_exponents(dinv + k0, n, kb, kb, kF16Bias, sc.edr + k0, sc.edc + k0, st);
+        if (r == MOAO_OK)
+          r = split_f16(dinv + k0, n, kb, kb, nsl, br, nb, sc.edr + k0, bc, nb, sc.edc + k0, st);
       }
+      ctx->stream = keep;
+      return r;
+    };
+    // Lookahead (not under capture): once the trailing update has reached the next
+    // panel's columns, that panel's diagonal block is factored on the side stream
+    // while the rest of the update runs on kLookaheadSms fewer SMs.
+    const bool ahead = ctx->lookahead && !graph;
+    if (ahead && !ctx->aux) {
+      int lo = 0, hi = 0;
+      MOAO_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      MOAO_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->aux, cudaStreamNonBlocking, hi));
+      for (auto& e : ctx->la_ev)
+        MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    int nsm = 148;
+    MOAO_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+    MOAO_TRY(diag_block(0, std::min(nb, n), s));
+    for (long k0 = 0; k0 < n; k0 += nb) {
+      const long kb = std::min(nb, n - k0);
       const long rest = n - k0 - kb;
       if (rest <= 0) break;
       float* P = A32 + (k0 + kb) + k0 * n;
@@ -450,9 +476,28 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       } else {
         MOAO_TRY(split_bf16(W2, rest, rest, kb, nsl, rr, ldn, cc, ldn, s));
       }
-      MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k0 + kb), (int)k0, mp.lrB, (int)(k0 + kb), (int)k0,
-                         (int)(kb / 64), full, rest, rest, A32 + (k0 + kb) + (k0 + kb) * n, n,
-                         true, err, (double)rest * rest * kb, er, er));
+      const long k1 = k0 + kb, kb1 = std::min(nb, rest);
+      const int nk = (int)(kb / 64);
+      if (ahead && rest > kb1) {
+        // the next panel's columns first, then its diagonal block beside the rest
+        MOAO_TRY(tc_update(ctx, mp.lrA, (int)k1, (int)k0, mp.lrB, (int)k1, (int)k0, nk, full, rest,
+                           kb1, A32 + k1 + k1 * n, n, true, err,
+                           (double)(2 * rest - kb1) * kb1 * kb, er, er));
+        MOAO_CUDA_TRY(cudaEventRecord(ctx->la_ev[0], s));
+        MOAO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->la_ev[0], 0));
+        MOAO_TRY(diag_block(k1, kb1, ctx->aux));
+        MOAO_CUDA_TRY(cudaEventRecord(ctx->la_ev[1], ctx->aux));
+        const long r2 = rest - kb1;
+        MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k1 + kb1), (int)k0, mp.lrB, (int)(k1 + kb1), (int)k0,
+                           nk, full, r2, r2, A32 + (k1 + kb1) + (k1 + kb1) * n, n, true, err,
+                           (double)r2 * r2 * kb, er ? er + kb1 : nullptr, er ? er + kb1 : nullptr,
+                           nsm - kLookaheadSms));
+        MOAO_CUDA_TRY(cudaStreamWaitEvent(s, ctx->la_ev[1], 0));
+      } else {
+        MOAO_TRY(tc_update(ctx, mp.lrA, (int)k1, (int)k0, mp.lrB, (int)k1, (int)k0, nk, full, rest,
+                           rest, A32 + k1 + k1 * n, n, true, err, (double)rest * rest * kb, er, er));
+        MOAO_TRY(diag_block(k1, kb1, s));
+      }
     }
     if (!graph) {
       int info[2] = {0, 0};

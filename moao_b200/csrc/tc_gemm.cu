@@ -579,7 +579,8 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   }
   static std::atomic<unsigned long long> configured{0};
   MOAO_CUDA_TRY(set_smem_limit(tc_gemm_kernel, (int)SMEM, configured));
-  tc_gemm_kernel<<<(unsigned)std::min<long>(total, num_sms), THREADS, SMEM, s>>>(p);
+  const long ctas = std::min<long>(total, g.max_ctas > 0 ? std::min(g.max_ctas, num_sms) : num_sms);
+  tc_gemm_kernel<<<(unsigned)ctas, THREADS, SMEM, s>>>(p);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;

@@ -53,6 +53,7 @@ struct TcGemm {
   const int* ecol = nullptr;
   int shift = 0;
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
+  int max_ctas = 0;            // cap on the persistent grid (0: one CTA per SM)
 };
 
 // Describes a row-major (K-contiguous) device matrix for TMA. The output tile is
