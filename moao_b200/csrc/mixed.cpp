@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "context.h"
@@ -149,8 +150,11 @@ struct Scales {
 };
 constexpr int kF16Bias = 14;  // stored slices below 2^14 in magnitude (fp16 max 65504)
 
-// Slices of the m x kb solve block W2 (FP64) into xr for the tensor core.
-moao_status split_block(const Scales& sc, const double* W2, long m, long kb, int slices,
+// Slices of an m x kb solve block (column-major, leading dimension lds) into xr
+// for the tensor core: fp16 slices straight from the FP32 state, or bf16 slices
+// of an FP64 block.
+template <typename T>
+moao_status split_block(const Scales& sc, const T* src, long lds, long m, long kb, int slices,
                         const BfSlices& xr, long ldx, cudaStream_t s) {
   BfSlices none{};
   const long kpad = std::min(round_up(kb, 64), ldx);
@@ -158,19 +162,25 @@ moao_status split_block(const Scales& sc, const double* W2, long m, long kb, int
     for (int k = 0; k < slices; ++k)
       MOAO_CUDA_TRY(cudaMemset2DAsync(static_cast<uint16_t*>(xr.p[k]) + kb, ldx * sizeof(uint16_t),
                                       0, (kpad - kb) * sizeof(uint16_t), m, s));
-  if (!sc.f16) return split_bf16(W2, m, m, kb, slices, xr, ldx, none, 0, s);
-  MOAO_TRY(scale_exponents(W2, m, m, kb, kF16Bias, sc.ex, nullptr, s));
-  return split_f16(W2, m, m, kb, slices, xr, ldx, sc.ex, none, 0, nullptr, s);
+  if (!sc.f16) {
+    if constexpr (std::is_same<T, double>::value)
+      return split_bf16(src, lds, m, kb, slices, xr, ldx, none, 0, s);
+    else
+      return set_error(MOAO_ERR_UNSUPPORTED, "bf16 split of an FP32 block");
+  }
+  MOAO_TRY(scale_exponents(src, lds, m, kb, kF16Bias, sc.ex, nullptr, s));
+  return split_f16(src, lds, m, kb, slices, xr, ldx, sc.ex, none, 0, nullptr, s);
 }
 
-// fp16 format: C32 (m x kb, ldc) = W (m x kb, FP64) times the inverse diagonal
-// block starting at row k0, transposed (forward: Dinv^T, rows of the drB copy)
-// or not (backward: Dinv, rows of the dcB copy), on the tensor cores.
-moao_status block_product(moao_ctx* ctx, const Scales& sc, const TcTensor* A, const double* W,
-                          long m, long k0, long kb, const TcTensor* B, const int* eB,
+// fp16 format: C32 (m x kb, ldc) = W (m x kb, FP32, ldw; C32 itself is allowed)
+// times the inverse diagonal block starting at row k0, transposed (forward:
+// Dinv^T, rows of the drB copy) or not (backward: Dinv, rows of the dcB copy),
+// on the tensor cores.
+moao_status block_product(moao_ctx* ctx, const Scales& sc, const TcTensor* A, const float* W,
+                          long ldw, long m, long k0, long kb, const TcTensor* B, const int* eB,
                           const Products& pr, float* C32, long ldc, const BfSlices& xr, long ldx,
                           int slices, int* err) {
-  MOAO_TRY(split_block(sc, W, m, kb, slices, xr, ldx, ctx->stream));
+  MOAO_TRY(split_block(sc, W, ldw, m, kb, slices, xr, ldx, ctx->stream));
   TcGemm g;
   g.kind = A[0].kind;
   g.epi = kTcEpiF32;
@@ -212,18 +222,19 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
   for (int k = 0; k < slices; ++k) xr.p[k] = xs[k];
   for (long k0 = 0; k0 < n; k0 += nb) {
     const long kb = std::min(nb, n - k0);
-    MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
+    float* Tk = T32 + k0 * m;
     if (sc.f16) {
-      MOAO_TRY(block_product(ctx, sc, xA, W1, m, k0, kb, mp.drB, sc.edr, pr, T32 + k0 * m, m,
-                             xr, ldx, slices, err));
-      MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W2, m, m, kb, false, s));
+      MOAO_TRY(block_product(ctx, sc, xA, Tk, m, m, k0, kb, mp.drB, sc.edr, pr, Tk, m, xr, ldx,
+                             slices, err));
     } else {
+      MOAO_TRY(cvt_f32_to_f64(Tk, m, W1, m, m, kb, false, s));
       MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, true, 0.0, W2, m));
-      MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+      MOAO_TRY(cvt_f64_to_f32(W2, m, Tk, m, m, kb, false, s));
     }
     const long rest = n - k0 - kb;
     if (rest > 0) {
-      MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
+      if (sc.f16) MOAO_TRY(split_block(sc, (const float*)Tk, m, m, kb, slices, xr, ldx, s));
+      else MOAO_TRY(split_block(sc, (const double*)W2, m, m, kb, slices, xr, ldx, s));
       MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lrB, (int)(k0 + kb), (int)k0, (int)((kb + 63) / 64),
                          pr, m, rest, T32 + (k0 + kb) * m, m, false, err, 2.0 * m * rest * kb,
                          sc.f16 ? sc.ex : nullptr,
@@ -233,17 +244,18 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
   const long nblk = (n + nb - 1) / nb;
   for (long b = nblk - 1; b >= 0; --b) {
     const long k0 = b * nb, kb = std::min(nb, n - k0);
-    MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W1, m, m, kb, false, s));
+    float* Tk = T32 + k0 * m;
     if (sc.f16) {
-      MOAO_TRY(block_product(ctx, sc, xA, W1, m, k0, kb, mp.dcB, sc.edc, pr, T32 + k0 * m, m,
-                             xr, ldx, slices, err));
-      MOAO_TRY(cvt_f32_to_f64(T32 + k0 * m, m, W2, m, m, kb, false, s));
+      MOAO_TRY(block_product(ctx, sc, xA, Tk, m, m, k0, kb, mp.dcB, sc.edc, pr, Tk, m, xr, ldx,
+                             slices, err));
     } else {
+      MOAO_TRY(cvt_f32_to_f64(Tk, m, W1, m, m, kb, false, s));
       MOAO_TRY(gemm(ctx, m, kb, kb, 1.0, W1, m, dinv + k0, n, false, 0.0, W2, m));
-      MOAO_TRY(cvt_f64_to_f32(W2, m, T32 + k0 * m, m, m, kb, false, s));
+      MOAO_TRY(cvt_f64_to_f32(W2, m, Tk, m, m, kb, false, s));
     }
     if (k0 > 0) {
-      MOAO_TRY(split_block(sc, W2, m, kb, slices, xr, ldx, s));
+      if (sc.f16) MOAO_TRY(split_block(sc, (const float*)Tk, m, m, kb, slices, xr, ldx, s));
+      else MOAO_TRY(split_block(sc, (const double*)W2, m, m, kb, slices, xr, ldx, s));
       MOAO_TRY(tc_update(ctx, xA, 0, 0, mp.lcB, 0, (int)k0, (int)((kb + 63) / 64), pr, m, k0,
                          T32, m, false, err, 2.0 * m * k0 * kb, sc.f16 ? sc.ex : nullptr,
                          sc.f16 ? sc.ecf : nullptr));
@@ -452,13 +464,12 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       const long rest = n - k0 - kb;
       if (rest <= 0) break;
       float* P = A32 + (k0 + kb) + k0 * n;
-      MOAO_TRY(cvt_f32_to_f64(P, n, W1, rest, rest, kb, false, s));
       if (f16) {
-        // panel P <- P Dinv^T on the tensor cores, then its FP64 copy for the split
-        MOAO_TRY(block_product(ctx, sc, mp.pA, W1, rest, k0, kb, mp.drB, sc.edr, full, P, n, xsl,
+        // panel P <- P Dinv^T on the tensor cores, in place
+        MOAO_TRY(block_product(ctx, sc, mp.pA, P, n, rest, k0, kb, mp.drB, sc.edr, full, P, n, xsl,
                                ldx, nsl, err));
-        MOAO_TRY(cvt_f32_to_f64(P, n, W2, rest, rest, kb, false, s));
       } else {
+        MOAO_TRY(cvt_f32_to_f64(P, n, W1, rest, rest, kb, false, s));
         MOAO_TRY(gemm(ctx, rest, kb, kb, 1.0, W1, rest, dinv + k0, n, true, 0.0, W2, rest));
         MOAO_TRY(cvt_f64_to_f32(W2, rest, P, n, rest, kb, false, s));
       }
@@ -470,8 +481,8 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       const int* er = nullptr;
       if (f16) {
         int* erk = sc.erp + (k0 / nb) * n + (k0 + kb);  // rows k0+kb.. of panel k0/nb
-        MOAO_TRY(scale_exponents(W2, rest, rest, kb, kF16Bias, erk, sc.ecf + k0, s));
-        MOAO_TRY(split_f16(W2, rest, rest, kb, nsl, rr, ldn, erk, cc, ldn, sc.ecf + k0, s));
+        MOAO_TRY(scale_exponents((const float*)P, n, rest, kb, kF16Bias, erk, sc.ecf + k0, s));
+        MOAO_TRY(split_f16((const float*)P, n, rest, kb, nsl, rr, ldn, erk, cc, ldn, sc.ecf + k0, s));
         er = erk;
       } else {
         MOAO_TRY(split_bf16(W2, rest, rest, kb, nsl, rr, ldn, cc, ldn, s));

@@ -48,9 +48,14 @@ moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSl
 // m x n block: the smallest e with max |x| < 2^e, minus bias (null skips one).
 moao_status scale_exponents(const double* A, long lda, long m, long n, int bias, int* erow,
                             int* ecol, cudaStream_t st);
+moao_status scale_exponents(const float* A, long lda, long m, long n, int bias, int* erow,
+                            int* ecol, cudaStream_t st);
 // fp16 split of x * 2^-e into ns slices: row-major copy scaled by erow[r],
 // column-major copy by ecol[c] (either copy may be skipped with a null p[0]).
 moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
+                      cudaStream_t st);
+moao_status split_f16(const float* src, long lds, long m, long n, int ns, BfSlices rmaj,
                       long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
                       cudaStream_t st);
 // int8 slices of the rows of A (m x n, column-major): per-row exponents in e[m],

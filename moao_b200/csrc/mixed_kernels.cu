@@ -99,14 +99,22 @@ __device__ __forceinline__ int exponent_of(double mx) {
   return ilogb(mx) + 1;
 }
 
-// Row maxima of a column-major m x n block: 32 rows per block, 8 column strides.
-__global__ void row_exponent_kernel(const double* __restrict__ A, long lda, long m, long n,
+// 2^k for an exponent in the normal range (exact), ldexp otherwise.
+__device__ __forceinline__ double pow2i(int k) {
+  return (k >= -1022 && k <= 1023) ? __longlong_as_double((long long)(k + 1023) << 52)
+                                   : ldexp(1.0, k);
+}
+
+// Row maxima of a column-major m x n block (FP64 or FP32 values): 32 rows per
+// block, 8 column strides.
+template <typename T>
+__global__ void row_exponent_kernel(const T* __restrict__ A, long lda, long m, long n,
                                     int* __restrict__ e, int bias) {
   __shared__ double red[8][33];
   const long r = (long)blockIdx.x * 32 + threadIdx.x;
   double mx = 0;
   if (r < m)
-    for (long c = threadIdx.y; c < n; c += 8) mx = fmax(mx, fabs(A[c * lda + r]));
+    for (long c = threadIdx.y; c < n; c += 8) mx = fmax(mx, fabs((double)A[c * lda + r]));
   red[threadIdx.y][threadIdx.x] = mx;
   __syncthreads();
   if (threadIdx.y == 0 && r < m) {
@@ -116,12 +124,13 @@ __global__ void row_exponent_kernel(const double* __restrict__ A, long lda, long
 }
 
 // Column maxima of a column-major m x n block: one block per column.
-__global__ void col_exponent_kernel(const double* __restrict__ A, long lda, long m, long n,
+template <typename T>
+__global__ void col_exponent_kernel(const T* __restrict__ A, long lda, long m, long n,
                                     int* __restrict__ e, int bias) {
   __shared__ double red[32];
   const long c = blockIdx.x;
   double mx = 0;
-  for (long r = threadIdx.x; r < m; r += blockDim.x) mx = fmax(mx, fabs(A[c * lda + r]));
+  for (long r = threadIdx.x; r < m; r += blockDim.x) mx = fmax(mx, fabs((double)A[c * lda + r]));
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
   __syncthreads();
@@ -134,8 +143,10 @@ __global__ void col_exponent_kernel(const double* __restrict__ A, long lda, long
 // 32x32 tiles, 32x8 threads. fp16 slices of x * 2^-e: slice k = fp16 of what
 // the previous slices left (in FP64), e = erow[r] for the row-major copy and
 // ecol[c] for the column-major one, so either copy can be scaled back exactly
-// by a power of two per row of the operand it feeds.
-__global__ void split_f16_kernel(const double* __restrict__ src, long lds, long m, long n, int ns,
+// by a power of two per row of the operand it feeds. x is FP64 or FP32 (an
+// FP32 x is exact in FP64, so both give the same slices).
+template <typename T>
+__global__ void split_f16_kernel(const T* __restrict__ src, long lds, long m, long n, int ns,
                                  BfSlices rmaj, long ldr, const int* __restrict__ erow,
                                  BfSlices cmaj, long ldc, const int* __restrict__ ecol) {
   __shared__ __half t[kMaxBfSlices][32][34];
@@ -144,9 +155,9 @@ __global__ void split_f16_kernel(const double* __restrict__ src, long lds, long 
   for (int jj = ty; jj < 32; jj += 8) {
     const long r = r0 + tx, c = c0 + jj;
     double x = 0;
-    if (r < m && c < n) x = src[c * lds + r];
+    if (r < m && c < n) x = (double)src[c * lds + r];
     if (rmaj.p[0]) {
-      double rem = (r < m) ? ldexp(x, -erow[r]) : 0.0;
+      double rem = (r < m) ? x * pow2i(-erow[r]) : 0.0;
       for (int k = 0; k < ns; ++k) {
         const __half h = __double2half(rem);
         rem -= (double)__half2float(h);
@@ -154,7 +165,7 @@ __global__ void split_f16_kernel(const double* __restrict__ src, long lds, long 
       }
     }
     if (cmaj.p[0] && r < m && c < n) {
-      double rem = ldexp(x, -ecol[c]);
+      double rem = x * pow2i(-ecol[c]);
       for (int k = 0; k < ns; ++k) {
         const __half h = __double2half(rem);
         rem -= (double)__half2float(h);
@@ -581,39 +592,62 @@ moao_status split_bf16(const double* src, long lds, long m, long n, int ns, BfSl
   return MOAO_OK;
 }
 
-moao_status scale_exponents(const double* A, long lda, long m, long n, int bias, int* erow,
-                            int* ecol, cudaStream_t st) {
+template <typename T>
+moao_status scale_exponents_t(const T* A, long lda, long m, long n, int bias, int* erow,
+                              int* ecol, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   if (erow) {
-    row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, erow, bias);
+    row_exponent_kernel<T><<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, erow,
+                                                                              bias);
     ++tl_launches;
   }
   if (ecol) {
-    col_exponent_kernel<<<(unsigned)n, 256, 0, st>>>(A, lda, m, n, ecol, bias);
+    col_exponent_kernel<T><<<(unsigned)n, 256, 0, st>>>(A, lda, m, n, ecol, bias);
     ++tl_launches;
   }
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
 
-moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
-                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
-                      cudaStream_t st) {
+template <typename T>
+moao_status split_f16_t(const T* src, long lds, long m, long n, int ns, BfSlices rmaj, long ldr,
+                        const int* erow, BfSlices cmaj, long ldc, const int* ecol, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_f16: slices");
   if ((rmaj.p[0] && !erow) || (cmaj.p[0] && !ecol))
     return set_error(MOAO_ERR_BAD_ARG, "split_f16: exponents missing");
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
-  split_f16_kernel<<<grid, dim3(32, 8), 0, st>>>(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc, ecol);
+  split_f16_kernel<T><<<grid, dim3(32, 8), 0, st>>>(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc,
+                                                    ecol);
   ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }
 
+moao_status scale_exponents(const double* A, long lda, long m, long n, int bias, int* erow,
+                            int* ecol, cudaStream_t st) {
+  return scale_exponents_t(A, lda, m, n, bias, erow, ecol, st);
+}
+moao_status scale_exponents(const float* A, long lda, long m, long n, int bias, int* erow,
+                            int* ecol, cudaStream_t st) {
+  return scale_exponents_t(A, lda, m, n, bias, erow, ecol, st);
+}
+
+moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
+                      cudaStream_t st) {
+  return split_f16_t(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc, ecol, st);
+}
+moao_status split_f16(const float* src, long lds, long m, long n, int ns, BfSlices rmaj,
+                      long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
+                      cudaStream_t st) {
+  return split_f16_t(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc, ecol, st);
+}
+
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
                              int8_t* out, long ldo, cudaStream_t st) {
   if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
-  row_exponent_kernel<<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e, 0);
+  row_exponent_kernel<double><<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, e, 0);
   ++tl_launches;
   dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
   split_rows_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, m, n, e, ns, out, ldo, m * ldo);
