@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "mixed.h"
 
@@ -105,20 +106,34 @@ __device__ __forceinline__ double pow2i(int k) {
                                    : ldexp(1.0, k);
 }
 
+// 2^k in FP32 for an exponent in the normal range (exact), ldexpf otherwise.
+__device__ __forceinline__ float pow2f(int k) {
+  return (k >= -126 && k <= 127) ? __int_as_float((k + 127) << 23) : ldexpf(1.f, k);
+}
+
 // Row maxima of a column-major m x n block (FP64 or FP32 values): 32 rows per
-// block, 8 column strides.
+// block, blockDim.y (<= 32) column strides, 4 loads in flight per thread.
 template <typename T>
 __global__ void row_exponent_kernel(const T* __restrict__ A, long lda, long m, long n,
                                     int* __restrict__ e, int bias) {
-  __shared__ double red[8][33];
+  __shared__ double red[32][33];
+  const int ny = blockDim.y;
   const long r = (long)blockIdx.x * 32 + threadIdx.x;
   double mx = 0;
-  if (r < m)
-    for (long c = threadIdx.y; c < n; c += 8) mx = fmax(mx, fabs((double)A[c * lda + r]));
+  if (r < m) {
+    long c = threadIdx.y;
+    for (; c + 3 * ny < n; c += 4 * ny) {
+      const double a0 = fabs((double)A[c * lda + r]), a1 = fabs((double)A[(c + ny) * lda + r]);
+      const double a2 = fabs((double)A[(c + 2 * ny) * lda + r]);
+      const double a3 = fabs((double)A[(c + 3 * ny) * lda + r]);
+      mx = fmax(mx, fmax(fmax(a0, a1), fmax(a2, a3)));
+    }
+    for (; c < n; c += ny) mx = fmax(mx, fabs((double)A[c * lda + r]));
+  }
   red[threadIdx.y][threadIdx.x] = mx;
   __syncthreads();
   if (threadIdx.y == 0 && r < m) {
-    for (int k = 1; k < 8; ++k) mx = fmax(mx, red[k][threadIdx.x]);
+    for (int k = 1; k < ny; ++k) mx = fmax(mx, red[k][threadIdx.x]);
     e[r] = exponent_of(mx) - bias;
   }
 }
@@ -154,22 +169,46 @@ __global__ void split_f16_kernel(const T* __restrict__ src, long lds, long m, lo
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int jj = ty; jj < 32; jj += 8) {
     const long r = r0 + tx, c = c0 + jj;
-    double x = 0;
-    if (r < m && c < n) x = (double)src[c * lds + r];
-    if (rmaj.p[0]) {
-      double rem = (r < m) ? x * pow2i(-erow[r]) : 0.0;
-      for (int k = 0; k < ns; ++k) {
-        const __half h = __double2half(rem);
-        rem -= (double)__half2float(h);
-        t[k][tx][jj] = h;
+    if constexpr (std::is_same<T, float>::value) {
+      // FP32 source: x 2^-e and every remainder are exact in FP32 (a value minus
+      // its fp16 rounding fits the 24-bit significand), so the slices equal the
+      // FP64 computation's
+      float x = 0.f;
+      if (r < m && c < n) x = src[c * lds + r];
+      if (rmaj.p[0]) {
+        float rem = (r < m) ? x * pow2f(-erow[r]) : 0.f;
+        for (int k = 0; k < ns; ++k) {
+          const __half h = __float2half_rn(rem);
+          rem -= __half2float(h);
+          t[k][tx][jj] = h;
+        }
       }
-    }
-    if (cmaj.p[0] && r < m && c < n) {
-      double rem = x * pow2i(-ecol[c]);
-      for (int k = 0; k < ns; ++k) {
-        const __half h = __double2half(rem);
-        rem -= (double)__half2float(h);
-        static_cast<__half*>(cmaj.p[k])[c * ldc + r] = h;
+      if (cmaj.p[0] && r < m && c < n) {
+        float rem = x * pow2f(-ecol[c]);
+        for (int k = 0; k < ns; ++k) {
+          const __half h = __float2half_rn(rem);
+          rem -= __half2float(h);
+          static_cast<__half*>(cmaj.p[k])[c * ldc + r] = h;
+        }
+      }
+    } else {
+      double x = 0;
+      if (r < m && c < n) x = (double)src[c * lds + r];
+      if (rmaj.p[0]) {
+        double rem = (r < m) ? x * pow2i(-erow[r]) : 0.0;
+        for (int k = 0; k < ns; ++k) {
+          const __half h = __double2half(rem);
+          rem -= (double)__half2float(h);
+          t[k][tx][jj] = h;
+        }
+      }
+      if (cmaj.p[0] && r < m && c < n) {
+        double rem = x * pow2i(-ecol[c]);
+        for (int k = 0; k < ns; ++k) {
+          const __half h = __double2half(rem);
+          rem -= (double)__half2float(h);
+          static_cast<__half*>(cmaj.p[k])[c * ldc + r] = h;
+        }
       }
     }
   }
@@ -597,7 +636,7 @@ moao_status scale_exponents_t(const T* A, long lda, long m, long n, int bias, in
                               int* ecol, cudaStream_t st) {
   if (m <= 0 || n <= 0) return MOAO_OK;
   if (erow) {
-    row_exponent_kernel<T><<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(A, lda, m, n, erow,
+    row_exponent_kernel<T><<<(unsigned)((m + 31) / 32), dim3(32, 32), 0, st>>>(A, lda, m, n, erow,
                                                                               bias);
     ++tl_launches;
   }
