@@ -86,8 +86,17 @@ __device__ __forceinline__ double dphi_unit(double x) {
 // which keeps them inside the instruction cache (inlined, they stalled on
 // instruction fetch; ~8% slower). The shared-point kernel has one call site
 // and inlines it.
+// The two uncommon branches are separate functions, so that the series path,
+// the one most points take, issues none of their instructions (inlined, the
+// compiler predicates them into every evaluation).
+__device__ __noinline__ double dphi_tiny_s(double s) { return s > 0 ? dphi_unit(sqrt(s)) : 0.0; }
+__device__ __noinline__ double dphi_asym_y(double s, double y, double y3, double x) {
+  const double xi = y3;
+  return kK2 - kK3 * exp(-x) * (x * y * y) * (1.0 + xi * (kA1 + xi * (kA2 + xi * kA3)));
+}
+
 __device__ __forceinline__ double dphi_unit_s_inl(double s) {
-  if (!(s > 1e-30)) return s > 0 ? dphi_unit(sqrt(s)) : 0.0;
+  if (!(s > 1e-30)) return dphi_tiny_s(s);
   double y = (double)exp2f(__log2f((float)s) * (-1.0f / 6.0f));
 #pragma unroll
   for (int it = 0; it < 2; ++it) {
@@ -96,10 +105,7 @@ __device__ __forceinline__ double dphi_unit_s_inl(double s) {
   }
   const double y3 = y * y * y;
   const double x = s * y3;
-  if (x > kXlim) {
-    const double xi = y3;
-    return kK2 - kK3 * exp(-x) * (x * y * y) * (1.0 + xi * (kA1 + xi * (kA2 + xi * kA3)));
-  }
+  if (x > kXlim) return dphi_asym_y(s, y, y3, x);
   const double x53 = s * y;        // x^(5/3)
   const double z = 0.25 * s;       // (x/2)^2
   double pg = c_Gma[10];
