@@ -158,6 +158,10 @@ moao_status split_block(const Scales& sc, const T* src, long lds, long m, long k
                         const BfSlices& xr, long ldx, cudaStream_t s) {
   BfSlices none{};
   const long kpad = std::min(round_up(kb, 64), ldx);
+  if constexpr (std::is_same<T, float>::value) {
+    if (sc.f16 && kb <= 1024)  // exponents, slices and zero padding in one pass
+      return split_rows_f16(src, lds, m, kb, slices, xr, ldx, kpad, sc.ex, kF16Bias, s);
+  }
   if (kpad > kb)  // the tensor core reads K in steps of 64: padding columns must hold zeros
     for (int k = 0; k < slices; ++k)
       MOAO_CUDA_TRY(cudaMemset2DAsync(static_cast<uint16_t*>(xr.p[k]) + kb, ldx * sizeof(uint16_t),

@@ -58,6 +58,11 @@ moao_status split_f16(const double* src, long lds, long m, long n, int ns, BfSli
 moao_status split_f16(const float* src, long lds, long m, long n, int ns, BfSlices rmaj,
                       long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
                       cudaStream_t st);
+// Row exponents (erow[m], minus bias) and row-major fp16 slices (stride ldx) of
+// an FP32 column-major m x kb block in one pass, kb <= 1024; slice columns
+// kb..kpad-1 are zeroed.
+moao_status split_rows_f16(const float* src, long lds, long m, long kb, int ns, BfSlices out,
+                           long ldx, long kpad, int* erow, int bias, cudaStream_t st);
 // int8 slices of the rows of A (m x n, column-major): per-row exponents in e[m],
 // slice s at out + s*m*ldo, row-major with row stride ldo.
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <type_traits>
 
@@ -218,6 +219,56 @@ __global__ void split_f16_kernel(const T* __restrict__ src, long lds, long m, lo
     const long r = r0 + ii, c = c0 + tx;
     if (r < m && c < n)
       for (int k = 0; k < ns; ++k) static_cast<__half*>(rmaj.p[k])[r * ldr + c] = t[k][ii][tx];
+  }
+}
+
+// Row exponents and row-major fp16 slices of an FP32 column-major m x kb block in
+// one pass: a CTA stages 16 full rows (kb <= kSplitMaxCols) in shared memory,
+// takes their maxima, then writes each slice two columns per thread; columns
+// kb..kpad-1 of the slices get zeros (the tensor core reads K in steps of 64).
+// Same exponents and slices as row_exponent_kernel + split_f16_kernel.
+constexpr int kSplitRows = 16;
+constexpr int kSplitMaxCols = 1024;
+__global__ void __launch_bounds__(256) split_rows_f16_kernel(const float* __restrict__ src, long lds,
+                                                             long m, int kb, int ns, BfSlices out,
+                                                             long ldx, int kpad,
+                                                             int* __restrict__ erow, int bias) {
+  extern __shared__ float srow[];  // kSplitRows x (kb + 1)
+  __shared__ float red[16][kSplitRows + 1];
+  __shared__ float sscale[kSplitRows];
+  const int tid = threadIdx.x, tr = tid % kSplitRows, tc = tid / kSplitRows;
+  const long r0 = (long)blockIdx.x * kSplitRows, r = r0 + tr;
+  const int ld = kb + 1;
+  float mx = 0.f;
+  if (r < m)
+    for (int c = tc; c < kb; c += 16) {
+      const float v = src[(long)c * lds + r];
+      srow[tr * ld + c] = v;
+      mx = fmaxf(mx, fabsf(v));
+    }
+  red[tc][tr] = mx;
+  __syncthreads();
+  if (tc == 0) {
+    for (int k = 1; k < 16; ++k) mx = fmaxf(mx, red[k][tr]);
+    const int e = exponent_of((double)mx) - bias;
+    if (r < m) erow[r] = e;
+    sscale[tr] = pow2f(-e);
+  }
+  __syncthreads();
+  const int half = kpad / 2;
+  for (int idx = tid; idx < kSplitRows * half; idx += blockDim.x) {
+    const int rr = idx / half, c = 2 * (idx % half);
+    const long row = r0 + rr;
+    if (row >= m) continue;
+    float a = c < kb ? srow[rr * ld + c] * sscale[rr] : 0.f;
+    float b = c + 1 < kb ? srow[rr * ld + c + 1] * sscale[rr] : 0.f;
+    for (int k = 0; k < ns; ++k) {
+      const __half ha = __float2half_rn(a), hb = __float2half_rn(b);
+      a -= __half2float(ha);
+      b -= __half2float(hb);
+      *reinterpret_cast<__half2*>(static_cast<__half*>(out.p[k]) + row * ldx + c) =
+          __halves2half2(ha, hb);
+    }
   }
 }
 
@@ -681,6 +732,23 @@ moao_status split_f16(const float* src, long lds, long m, long n, int ns, BfSlic
                       long ldr, const int* erow, BfSlices cmaj, long ldc, const int* ecol,
                       cudaStream_t st) {
   return split_f16_t(src, lds, m, n, ns, rmaj, ldr, erow, cmaj, ldc, ecol, st);
+}
+
+moao_status split_rows_f16(const float* src, long lds, long m, long kb, int ns, BfSlices out,
+                           long ldx, long kpad, int* erow, int bias, cudaStream_t st) {
+  if (m <= 0 || kb <= 0) return MOAO_OK;
+  if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_rows_f16: slices");
+  if (kb > kSplitMaxCols || kpad < kb || kpad > ldx || (kpad & 1) || (ldx & 1))
+    return set_error(MOAO_ERR_BAD_ARG, "split_rows_f16: block shape");
+  static std::atomic<unsigned long long> configured{0};
+  const int smem = (int)(kSplitRows * (kSplitMaxCols + 1) * sizeof(float));
+  MOAO_CUDA_TRY(set_smem_limit(split_rows_f16_kernel, smem, configured));
+  const size_t dyn = (size_t)kSplitRows * (kb + 1) * sizeof(float);
+  split_rows_f16_kernel<<<(unsigned)((m + kSplitRows - 1) / kSplitRows), 256, dyn, st>>>(
+      src, lds, m, (int)kb, ns, out, ldx, (int)kpad, erow, bias);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
 }
 
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
