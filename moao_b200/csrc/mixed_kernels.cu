@@ -379,15 +379,26 @@ __global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long
     }
   }
   __syncthreads();
-  for (int jj = ty; jj < 32; jj += 8) {
-    const long j = j0 + jj, k = k0 + tx;
-    if (j >= n || k >= n) continue;
-    double v = ldexp(t[jj][tx], 6 - f[j]);
-    for (int s = 0; s < ns; ++s) {
-      const double qv = rint(v);
-      out[s * slice_stride + j * ldo + k] = (int8_t)qv;
-      v = (v - qv) * 128.0;
+  // 4 consecutive k per thread, one 32-bit store per slice (the row stride ldo is
+  // a multiple of 4; slice columns n..ldo-1 are never read, so a word that runs
+  // past n may hold zeros there)
+  const int tid = ty * 32 + tx;
+  const int jj = tid >> 3, kq = (tid & 7) * 4;
+  const long j = j0 + jj, k = k0 + kq;
+  if (j >= n || k >= n) return;
+  const double sc = pow2i(6 - f[j]);
+  double v[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = (k + i < n) ? t[jj][kq + i] * sc : 0.0;
+  for (int s = 0; s < ns; ++s) {
+    uint32_t w = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double qv = rint(v[i]);
+      w |= (uint32_t)(uint8_t)(int8_t)qv << (8 * i);
+      v[i] = (v[i] - qv) * 128.0;
     }
+    *reinterpret_cast<uint32_t*>(out + s * slice_stride + j * ldo + k) = w;
   }
 }
 
@@ -767,6 +778,8 @@ moao_status ozaki_split_sym(const double* A, long lda, long n, int ns, int* f,
                             unsigned long long* colmax, int8_t* out, long ldo, const int* rid,
                             const OffsetRanges& off, cudaStream_t st) {
   if (ns < 1 || ns > kMaxOzakiSlices) return set_error(MOAO_ERR_BAD_ARG, "ozaki: slices");
+  if ((ldo & 3) || (reinterpret_cast<uintptr_t>(out) & 3))
+    return set_error(MOAO_ERR_BAD_ARG, "ozaki: slice rows must be 4-byte aligned");
   MOAO_CUDA_TRY(cudaMemsetAsync(colmax, 0, n * sizeof(unsigned long long), st));
   const int* r = off.n ? rid : nullptr;
   const OffsetValues ov = values_of(off);
