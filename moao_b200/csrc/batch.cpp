@@ -213,16 +213,30 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     int k = -1;
     if (!load.empty()) k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
     const bool can_open = (int)load.size() < S && planned + f <= budget;
-    if (can_open && (k < 0 || load[k] > 0)) {
+    auto open_stream = [&]() {
       load.push_back(0.0);
       foot.push_back(0);
       per.emplace_back();
-      k = (int)load.size() - 1;
+      return (int)load.size() - 1;
+    };
+    if (can_open && (k < 0 || load[k] > 0)) {
+      k = open_stream();
+    } else if (k >= 0 && f > foot[k] && planned - foot[k] + f > budget) {
+      // the least-loaded stream cannot grow to this instance: the least-loaded
+      // one that holds it within the budget, else a new stream
+      k = -1;
+      double best = 0;
+      for (size_t j = 0; j < load.size(); ++j) {
+        const size_t grow = f > foot[j] ? f - foot[j] : 0;
+        if (planned + grow <= budget && (k < 0 || load[j] < best)) {
+          k = (int)j;
+          best = load[j];
+        }
+      }
+      if (k < 0 && can_open) k = open_stream();
     }
-    if (k < 0) return set_error(MOAO_ERR_OOM, "batch: the largest instance exceeds the device budget");
+    if (k < 0) return set_error(MOAO_ERR_OOM, "batch: an instance exceeds the device budget");
     if (f > foot[k]) {
-      if (planned - foot[k] + f > budget)
-        return set_error(MOAO_ERR_OOM, "batch: instances exceed the device budget");
       planned += f - foot[k];
       foot[k] = f;
     }
