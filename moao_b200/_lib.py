@@ -101,6 +101,7 @@ SIGNATURES = {
     "moao_ctx_set_offsets": (i32, [vp, i32, vp, vp, vp]),
     "moao_ctx_set_host_precision": (i32, [vp, i32]),
     "moao_ctx_set_factor_format": (i32, [vp, i32]),
+    "moao_ctx_set_lookahead": (i32, [vp, i32]),
     "moao_server_create": (i32, [C.POINTER(ServerOpts), C.POINTER(vp)]),
     "moao_server_add_system": (i32, [vp, C.c_char_p, C.c_char_p, C.c_long, vp, vp, vp, vp,
                                      C.POINTER(i32)]),

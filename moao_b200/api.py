@@ -156,6 +156,11 @@ class Context:
         code = {"bf16x3": 0, "f16x2": 1}[fmt]
         check(lib().moao_ctx_set_factor_format(self._h, code), "moao_ctx_set_factor_format")
 
+    def set_lookahead(self, on: bool):
+        """Mixed factorisation: factor the next diagonal block on a side stream
+        beside the trailing update (default on; results are the same)."""
+        check(lib().moao_ctx_set_lookahead(self._h, int(bool(on))), "moao_ctx_set_lookahead")
+
     def set_offsets(self, begin, end, value):
         """Block-constant offsets of Cmm for the mixed path (see moao_ctx_set_offsets);
         empty sequences clear them."""

@@ -521,6 +521,13 @@ moao_status moao_ctx_set_factor_format(moao_ctx* c, int format) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_lookahead(moao_ctx* c, int on) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->lookahead = on != 0;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_host_precision(moao_ctx* c, moao_prec prec) {
   if (!c || (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED))
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_precision: FP64 or MIXED");

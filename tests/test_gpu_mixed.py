@@ -144,3 +144,25 @@ def test_f16x2_factor_with_offsets(ctx, name):
     err = O.rel_fro(host(dT), R_ref)
     assert err <= 1e-5, err
     c2.close()
+
+
+def test_mixed_lookahead_gives_the_same_result(ctx):
+    """The lookahead only reorders work across two streams (the next diagonal
+    block beside the rest of the trailing update): R and the factor are
+    bit-identical with it on and off, on a system with several panels."""
+    import torch
+    nm, nts, Cmm, Ctm = case("elt16")
+    ctx.set_block(128)
+    outs = []
+    try:
+        for on in (True, False):
+            ctx.set_lookahead(on)
+            dC, dT = dev(Cmm), dev(Ctm)
+            M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=ctx)
+            ctx.synchronize()
+            outs.append((dC, dT))
+    finally:
+        ctx.set_lookahead(True)
+        ctx.set_block(256)
+    assert torch.equal(outs[0][1], outs[1][1])
+    assert torch.equal(outs[0][0], outs[1][0])
