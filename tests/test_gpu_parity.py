@@ -94,6 +94,33 @@ def test_matcov_symmetric_fill_and_tiles(ctx):
         assert_close(got, ref, 1e-11, f"tile type {typ} at {x0},{y0}")
 
 
+def test_matcov_tiles_through_shared_point_blocks(ctx):
+    """Tiles of the ELT-like system that cut through LGS x NGS and truth-sensor x
+    LGS blocks, which the shared-point kernel evaluates (edge-aligned WFS pairs
+    without an offset table): partial 4x4 / 8x8 cell tiles, the lower-triangle
+    mask, ld padding and untouched elements."""
+    t, g = tomo_and_geom("elt16")
+    nm, nts = g.nmeas, g.nmeasts
+    nlgs_rows = 2 * int(sum(g.t["Nsubap"][:g.nLgs]))  # slopes of the LGS
+    assert 0 < nlgs_rows < nm
+    cases = [(1, (nlgs_rows + 7, 13, 151, 173)),       # NGS rows x LGS columns
+             (1, (nlgs_rows - 40, nlgs_rows - 90, 97, 120)),  # across the LGS/NGS boundary
+             (3, (3, 29, nts - 10, 211)),               # truth sensor x LGS
+             (3, (11, nlgs_rows - 31, 60, 90))]         # truth sensor across LGS/NGS
+    for typ, (x0, y0, nr, nc) in cases:
+        ref = O.matcov(g, nr, nc, x0, y0, typ, nthreads=8)
+        buf = np.full((nr + 3, nc), 7.0, order="F")
+        M.matcov_tile(buf, nr, nc, x0, y0, nr + 3, t, typ, ctx=ctx)
+        got = buf[:nr]
+        if typ == 1:
+            gx = np.arange(nr)[:, None] + x0
+            gy = np.arange(nc)[None, :] + y0
+            assert np.all(got[gy > gx] == 7.0), "untouched upper elements were modified"
+            ref = np.where(gy > gx, 7.0, ref)
+        assert np.all(buf[nr:] == 7.0), "wrote outside the tile (ld padding)"
+        assert_close(got, ref, 1e-11, f"elt16 tile type {typ} at {x0},{y0}")
+
+
 def test_matcov_bad_type_raises(ctx):
     t, g = tomo_and_geom("small")
     buf = np.zeros((4, 4), order="F")
