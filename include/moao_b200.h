@@ -110,11 +110,11 @@ moao_status moao_ctx_set_offsets(moao_ctx* ctx, int nranges, const int* begin, c
  * the reference adds it to each such element). */
 moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* ctx, const moao_tomo* tomo);
 
-/* Lookahead in the mixed factorisation (default on): the next diagonal block is
- * factored on a side stream of the context while the trailing update runs on
- * all but 8 SMs. Same results either way; turn it off when other work should
- * have every SM. No reference counterpart. */
-moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int on);
+/* Lookahead in the mixed factorisation: the next diagonal block is factored on
+ * a side stream of the context while the trailing update leaves sms SMs to it
+ * (default 8; 0 turns the lookahead off, at most 64). Same results either way;
+ * turn it off when other work should have every SM. No reference counterpart. */
+moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int sms);
 
 /* Precision of moao_reconstructor_host (default MOAO_PREC_FP64, the
  * reference's behaviour). No reference counterpart. */

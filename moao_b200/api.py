@@ -156,10 +156,12 @@ class Context:
         code = {"bf16x3": 0, "f16x2": 1}[fmt]
         check(lib().moao_ctx_set_factor_format(self._h, code), "moao_ctx_set_factor_format")
 
-    def set_lookahead(self, on: bool):
+    def set_lookahead(self, sms=8):
         """Mixed factorisation: factor the next diagonal block on a side stream
-        beside the trailing update (default on; results are the same)."""
-        check(lib().moao_ctx_set_lookahead(self._h, int(bool(on))), "moao_ctx_set_lookahead")
+        beside the trailing update, which leaves it `sms` SMs (default 8;
+        0 or False turns the lookahead off; True means 8). Same results."""
+        n = 8 if sms is True else int(sms)
+        check(lib().moao_ctx_set_lookahead(self._h, n), "moao_ctx_set_lookahead")
 
     def set_offsets(self, begin, end, value):
         """Block-constant offsets of Cmm for the mixed path (see moao_ctx_set_offsets);

@@ -150,7 +150,7 @@ moao_status ensure_subs(moao_ctx* ctx, int S) {
   while ((int)v.size() < S) {
     moao_ctx* c = nullptr;
     MOAO_TRY(moao_ctx_create(ctx->device, &c));
-    c->lookahead = false;  // concurrent instances fill the SMs; no side stream in the capture
+    c->lookahead_sms = 0;  // concurrent instances fill the SMs; no side stream in the capture
     v.push_back(c);
   }
   return MOAO_OK;

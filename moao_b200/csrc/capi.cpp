@@ -521,10 +521,11 @@ moao_status moao_ctx_set_factor_format(moao_ctx* c, int format) {
   return MOAO_OK;
 }
 
-moao_status moao_ctx_set_lookahead(moao_ctx* c, int on) {
+moao_status moao_ctx_set_lookahead(moao_ctx* c, int sms) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead: null");
+  if (sms < 0 || sms > 64) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead: 0..64 SMs");
   std::lock_guard<std::mutex> lk(c->mu);
-  c->lookahead = on != 0;
+  c->lookahead_sms = sms;
   return MOAO_OK;
 }
 

@@ -73,8 +73,9 @@ struct moao_ctx {
   int final_residual = 0;    // evaluate the residual once more after the last correction
   cudaEvent_t ev[8] = {};
   // Mixed factorisation lookahead: the next diagonal block is factored on aux
-  // (created on first use) while the trailing update leaves kLookaheadSms SMs free.
-  bool lookahead = true;
+  // (created on first use) while the trailing update leaves this many SMs free
+  // (0: no lookahead).
+  int lookahead_sms = 8;
   cudaStream_t aux = nullptr;
   cudaEvent_t la_ev[2] = {};
   // kernel timing

@@ -83,7 +83,6 @@ struct Maps {
 };
 
 constexpr long kYRows = 128;  // rows of the offset-indicator solve (one tile)
-constexpr int kLookaheadSms = 8;  // SMs left to the diagonal block during the lookahead
 
 
 // Products s_i * s_j of bf16 slices kept for a given slice count, smallest
@@ -451,8 +450,8 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     };
     // Lookahead (not under capture): once the trailing update has reached the next
     // panel's columns, that panel's diagonal block is factored on the side stream
-    // while the rest of the update runs on kLookaheadSms fewer SMs.
-    const bool ahead = ctx->lookahead && !graph;
+    // while the rest of the update leaves ctx->lookahead_sms SMs to it.
+    const bool ahead = ctx->lookahead_sms > 0 && !graph;
     if (ahead && !ctx->aux) {
       int lo = 0, hi = 0;
       MOAO_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -506,7 +505,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
         MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k1 + kb1), (int)k0, mp.lrB, (int)(k1 + kb1), (int)k0,
                            nk, full, r2, r2, A32 + (k1 + kb1) + (k1 + kb1) * n, n, true, err,
                            (double)r2 * r2 * kb, er ? er + kb1 : nullptr, er ? er + kb1 : nullptr,
-                           nsm - kLookaheadSms));
+                           std::max(1, nsm - ctx->lookahead_sms)));
         MOAO_CUDA_TRY(cudaStreamWaitEvent(s, ctx->la_ev[1], 0));
       } else {
         MOAO_TRY(tc_update(ctx, mp.lrA, (int)k1, (int)k0, mp.lrB, (int)k1, (int)k0, nk, full, rest,
