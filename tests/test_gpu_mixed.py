@@ -166,3 +166,26 @@ def test_mixed_lookahead_gives_the_same_result(ctx):
         ctx.set_block(256)
     assert torch.equal(outs[0][1], outs[1][1])
     assert torch.equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("n,m,nb", [(1000, 77, 256), (1370, 130, 512)])
+def test_mixed_default_format_ragged_panels(ctx, n, m, nb):
+    """Default fp16x2 format on sizes that are not multiples of the panel width
+    or of 64: the last panel and the last solve blocks are ragged and their
+    fp16 slices carry zero K padding up to the next multiple of 64."""
+    rng = np.random.default_rng(n)
+    X = rng.standard_normal((n, n))
+    A = X @ X.T / n + np.eye(n)
+    B = rng.standard_normal((m, n))
+    R_ref = np.linalg.solve(A, B.T).T
+    ctx.set_block(nb)
+    ctx.set_mixed(final_residual=True)
+    try:
+        dC, dT = dev(A), dev(B)
+        rep = M.reconstructor(n, m, dC, n, dT, m, 1, prec="mixed", ctx=ctx)
+        ctx.synchronize()
+    finally:
+        ctx.set_mixed()
+        ctx.set_block(256)
+    err = O.rel_fro(host(dT), R_ref)
+    assert err <= 1e-5, (err, rep)
