@@ -127,8 +127,10 @@ moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
 
 /* Options of the mixed-precision reconstructor: bf16 slices of the factor in
  * the first solve (2: ~16 significant bits, 3 products; 3: ~24 bits, 6
- * products; default 3), bf16 slices of the factor in the correction solves
- * (2 or 3, at most bf16_slices; default 2), int8
+ * products; default 3; these two apply to MOAO_FACTOR_BF16X3), slices of the
+ * factor in the correction solves (1 to the format's slice count; 1 uses only
+ * the leading slice products; 0, the default, picks 1 for MOAO_FACTOR_F16X2
+ * and 2 for BF16X3: a correction needs ~1e-2 relative accuracy), int8
  * slices per operand of the refinement residual (2..6, default 5), refinement
  * corrections per target (0..8, default 1), residual tolerance that stops
  * refinement early (default 0) and whether to evaluate the residual again after

@@ -144,7 +144,7 @@ class Context:
         check(lib().moao_ctx_set_block(self._h, nb), "moao_ctx_set_block")
 
     def set_mixed(self, bf16_slices: int = 3, ozaki_slices: int = 5, max_refine: int = 1,
-                  tol: float = 0.0, final_residual: bool = False, corr_slices: int = 2):
+                  tol: float = 0.0, final_residual: bool = False, corr_slices: int = 0):
         """Options of the mixed-precision reconstructor (see moao_ctx_set_mixed)."""
         check(lib().moao_ctx_set_mixed(self._h, bf16_slices, corr_slices, ozaki_slices,
                                        max_refine, tol, int(final_residual)),

@@ -451,10 +451,10 @@ moao_status moao_ctx_reset_kernel_stats(moao_ctx* c) {
 
 moao_status moao_ctx_set_mixed(moao_ctx* c, int bf16_slices, int corr_slices, int ozaki_slices,
                                int max_refine, double tol, int final_residual) {
-  if (!c || bf16_slices < 2 || bf16_slices > 3 || corr_slices < 2 || corr_slices > bf16_slices ||
+  if (!c || bf16_slices < 2 || bf16_slices > 3 || corr_slices < 0 || corr_slices > bf16_slices ||
       ozaki_slices < 2 || ozaki_slices > 6 || max_refine < 0 || max_refine > 8 || tol < 0)
     return set_error(MOAO_ERR_BAD_ARG,
-                     "ctx_set_mixed: bf16 slices in [2, 3], correction slices in [2, bf16 slices], "
+                     "ctx_set_mixed: bf16 slices in [2, 3], correction slices in [0, bf16 slices], "
                      "int8 slices in [2, 6], max_refine in [0, 8]");
   std::lock_guard<std::mutex> lk(c->mu);
   c->bf16_slices = bf16_slices;

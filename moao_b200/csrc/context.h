@@ -66,7 +66,7 @@ struct moao_ctx {
   moao::OffsetRanges offsets;
   int bf16_slices = 3;       // bf16 slices of the factor (3: ~24 bits, 6 products)
   int factor_format = 1;     // MOAO_FACTOR_F16X2 (default) or MOAO_FACTOR_BF16X3
-  int corr_slices = 2;       // bf16 slices of the factor in the correction solves
+  int corr_slices = 0;       // factor slices in the correction solves (0: 1 for fp16x2, 2 for bf16x3)
   int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
   int max_refine = 1;        // refinement corrections per target
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this

@@ -4,8 +4,10 @@ Tolerance: relative Frobenius error of R <= 1e-5 against FP64 (the accuracy the
 mixed path is specified to), with the residual ||Ctm - R Cmm||_F / ||Ctm||_F
 reported by the library after the last refinement step. Defaults: three bf16
 slices of the factor (about 24 significant bits, six tensor-core products) in
-the factorisation and the first solve, one refinement step whose correction
-solve uses two slices, residual from 5 int8 slices per operand.
+the factorisation and the first solve (the tests that pin the bf16x3 format;
+the default fp16x2 keeps two fp16 slices, three products), one refinement step
+whose correction solve uses two bf16 slices (fp16x2: the leading slice product
+only), residual from 5 int8 slices per operand.
 """
 import numpy as np
 import pytest
