@@ -97,7 +97,12 @@ __device__ __noinline__ double dphi_asym_y(double s, double y, double y3, double
 
 __device__ __forceinline__ double dphi_unit_s_inl(double s) {
   if (!(s > 1e-30)) return dphi_tiny_s(s);
-  double y = (double)exp2f(__log2f((float)s) * (-1.0f / 6.0f));
+  // seed 2^(-log2(s)/6) from the PTX approximations (flush-to-zero forms: s is
+  // a normal float here, and so is the seed)
+  float l2, y0;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2) : "f"((float)s));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(l2 * (-1.0f / 6.0f)));
+  double y = (double)y0;
 #pragma unroll
   for (int it = 0; it < 2; ++it) {
     const double y2 = y * y;
