@@ -90,27 +90,32 @@ __device__ __forceinline__ double dphi_unit(double x) {
 // the one most points take, issues none of their instructions (inlined, the
 // compiler predicates them into every evaluation).
 __device__ __noinline__ double dphi_tiny_s(double s) { return s > 0 ? dphi_unit(sqrt(s)) : 0.0; }
-__device__ __noinline__ double dphi_asym_y(double s, double y, double y3, double x) {
-  const double xi = y3;
+__device__ __noinline__ double dphi_asym_y(double s, double y) {
+  const double xi = y * y * y;  // 1/x
+  const double x = s * xi;
   return kK2 - kK3 * exp(-x) * (x * y * y) * (1.0 + xi * (kA1 + xi * (kA2 + xi * kA3)));
 }
+
+// The branch is taken on s = x^2 against xlim^2, so the series path never forms
+// x (points within an ulp of the boundary may take either form, as they may in
+// the reference's own rounding of x).
+constexpr double kXlim2 = kXlim * kXlim;
 
 __device__ __forceinline__ double dphi_unit_s_inl(double s) {
   if (!(s > 1e-30)) return dphi_tiny_s(s);
   // seed 2^(-log2(s)/6) from the PTX approximations (flush-to-zero forms: s is
-  // a normal float here, and so is the seed)
+  // a normal float here, and so is the seed), then y <- y (7/6 - (s/6) y^6)
   float l2, y0;
   asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2) : "f"((float)s));
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(l2 * (-1.0f / 6.0f)));
   double y = (double)y0;
+  const double s6 = s * (1.0 / 6.0);
 #pragma unroll
   for (int it = 0; it < 2; ++it) {
     const double y2 = y * y;
-    y = y * fma(-s, y2 * y2 * y2, 7.0) * (1.0 / 6.0);
+    y = y * fma(-s6, y2 * y2 * y2, 7.0 / 6.0);
   }
-  const double y3 = y * y * y;
-  const double x = s * y3;
-  if (x > kXlim) return dphi_asym_y(s, y, y3, x);
+  if (s > kXlim2) return dphi_asym_y(s, y);
   const double x53 = s * y;        // x^(5/3)
   const double z = 0.25 * s;       // (x/2)^2
   double pg = c_Gma[10];
