@@ -145,7 +145,10 @@ class Context:
 
     def set_mixed(self, bf16_slices: int = 3, ozaki_slices: int = 5, max_refine: int = 1,
                   tol: float = 0.0, final_residual: bool = False, corr_slices: int = 0):
-        """Options of the mixed-precision reconstructor (see moao_ctx_set_mixed)."""
+        """Options of the mixed-precision reconstructor (see moao_ctx_set_mixed):
+        bf16 slices of the bf16x3 format, int8 slices of the refinement residual,
+        refinement corrections, stop tolerance, a last residual evaluation, and
+        the factor slices of the correction solves (0: 1 for fp16x2, 2 for bf16x3)."""
         check(lib().moao_ctx_set_mixed(self._h, bf16_slices, corr_slices, ozaki_slices,
                                        max_refine, tol, int(final_residual)),
               "moao_ctx_set_mixed")
