@@ -196,14 +196,17 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
  * without an allocation stalling in the driver, or an application whose memory
  * pool already owns all of the GPU.
  * Same contract as moao_reconstructor with MOAO_PREC_FP64 (device pointers, Cmm
- * becomes its lower factor, each target's Ctm becomes R), on the given
- * cudaStream_t (NULL = legacy default stream); returns after the stream has
- * finished the work. Limit: nmeas <= 2048 and nmeasts <= 2048; larger sizes
- * return MOAO_ERR_BAD_ARG. Scratch lives in one fixed 8 MiB device array that
- * every GPU loading the library holds until exit; all calls share it, so calls
- * that overlap on the GPU (other threads, other streams) race and must be
- * serialised by the caller. The first call on a device looks the array up
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * becomes its lower factor, each target's Ctm becomes R; nmeas 0 is a no-op and
+ * ngal 0 factors without solving), on the given cudaStream_t (NULL = legacy
+ * default stream), which must belong to the current device (otherwise
+ * MOAO_ERR_BAD_ARG); returns after the stream has finished the work. Limit:
+ * nmeas <= 2048 and nmeasts <= 2048; larger sizes return MOAO_ERR_BAD_ARG.
+ * Scratch lives in one fixed 8 MiB device array that every GPU loading the
+ * library holds until exit; all calls share it, so calls that overlap on the
+ * GPU (other threads, other streams) race and must be serialised by the
+ * caller. Each call looks the array's address up in the current CUDA context
+ * (cudaGetSymbolAddress, no allocation); the first call in a context loads the
+ * library's device code, so make that first call before any stream capture.
  * On a non-positive pivot, *info (if not NULL) receives the 1-based column and
  * MOAO_ERR_NOT_SPD is returned. */
 moao_status moao_reconstructor_noalloc(long nmeas, long nmeasts, double* d_Cmm, long ldCmm,

@@ -11,7 +11,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "context.h"
 #include "dense.h"
@@ -27,27 +26,19 @@ constexpr size_t kScratchDoubles = kDinvDoubles + kPanelDoubles + 32;  // + pivo
 // 8 MiB + 256 bytes of device memory per GPU, shared by every call.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array for the current device; looked up once
-// per device (the first call on a device does this).
-moao_status scratch_for_current_device(double** out) {
-  int dev = 0;
-  MOAO_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices)
-    return moao::set_error(MOAO_ERR_UNSUPPORTED, "reconstructor_noalloc: device index too large");
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return moao::set_error(MOAO_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
-                                                cudaGetErrorString(e));
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
+// Device address of the scratch array in the current context. A __device__
+// symbol's address belongs to the CUDA context that loaded the module, not to
+// the device: after cudaDeviceReset the module is loaded again, and a caller
+// driving its own driver-API context gets a different copy. So the address is
+// looked up on every call (a host-side table lookup once the module is loaded;
+// it allocates nothing). The first call in a context loads the module.
+moao_status scratch_for_current_context(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return moao::set_error(MOAO_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
+                                              cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return MOAO_OK;
 }
 
@@ -57,21 +48,31 @@ extern "C" moao_status moao_reconstructor_noalloc(long nmeas, long nmeasts, doub
                                                   long ldCmm, double* d_Ctm, long ldCtm, long ngal,
                                                   void* stream, int* info) {
   using namespace moao;
-  if (nmeas < 1 || nmeasts < 1 || nmeas > kNoAllocMaxN || nmeasts > kNoAllocMaxN)
+  if (nmeas < 0 || nmeasts < 0 || ngal < 0 || ldCmm < std::max(1L, nmeas) ||
+      ldCtm < std::max(1L, nmeasts) || (nmeas > 0 && (!d_Cmm || !d_Ctm)))
     return set_error(MOAO_ERR_BAD_ARG,
-                     "reconstructor_noalloc: nmeas and nmeasts must be in [1, 2048] (the size "
+                     "reconstructor_noalloc: bad sizes, pointers or leading dimensions");
+  if (nmeas > kNoAllocMaxN || nmeasts > kNoAllocMaxN)
+    return set_error(MOAO_ERR_BAD_ARG,
+                     "reconstructor_noalloc: nmeas and nmeasts must be at most 2048 (the size "
                      "of its fixed device scratch); use moao_reconstructor for larger systems");
-  if (ngal < 1 || !d_Cmm || !d_Ctm || ldCmm < nmeas || ldCtm < nmeasts)
-    return set_error(MOAO_ERR_BAD_ARG, "reconstructor_noalloc: bad pointers, ngal or leading dimensions");
   if (info) *info = 0;
+  if (nmeas == 0) return MOAO_OK;  // nothing to factor, as moao_reconstructor
+  int cur = 0, sdev = 0;
+  MOAO_CUDA_TRY(cudaGetDevice(&cur));
+  MOAO_CUDA_TRY(cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev));
+  if (sdev != cur)
+    return set_error(MOAO_ERR_BAD_ARG,
+                     "reconstructor_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                         " but the current device is " + std::to_string(cur));
   double* scratch = nullptr;
-  MOAO_TRY(scratch_for_current_device(&scratch));
+  MOAO_TRY(scratch_for_current_context(&scratch));
   double* dinv = scratch;                 // nmeas x 256, leading dimension nmeas
   double* W = scratch + kDinvDoubles;     // one panel
   int* d_info = reinterpret_cast<int*>(W + kPanelDoubles);
 
   moao_ctx c;  // host-side bookkeeping only; owns no device memory
-  MOAO_CUDA_TRY(cudaGetDevice(&c.device));
+  c.device = cur;
   c.stream = static_cast<cudaStream_t>(stream);
   c.nb = (int)kNoAllocNb;
   const long n = nmeas, nb = kNoAllocNb;
@@ -95,7 +96,7 @@ extern "C" moao_status moao_reconstructor_noalloc(long nmeas, long nmeasts, doub
   if (info) *info = h_info;
   if (h_info) return set_error(MOAO_ERR_NOT_SPD, "reconstructor_noalloc: non-positive pivot at column " +
                                                      std::to_string(h_info));
-  for (long g = 0; g < ngal; ++g) {
+  for (long g = 0; g < ngal && nmeasts > 0; ++g) {  // ngal 0: factor only
     double* B = d_Ctm + nmeas * nmeasts * g;
     const long m = nmeasts;
     for (long k0 = 0; k0 < n; k0 += nb) {  // X L^T = B

@@ -106,3 +106,24 @@ def test_configs_have_the_stated_sizes():
     for _ in range(20):
         s, a = P.config_random(rng)
         assert 20 <= s.nssp <= 50 and 3 <= s.nW <= 9 and 1 <= a.nLayer <= 20
+
+
+@pytest.mark.parametrize("name", systems.CHECK_SETS + ["elt"])
+def test_check_set_geometry_matches_reference_golden(built, name):
+    """The six reference check systems (parsed from the reference's own
+    parameter files) and the ELT-scale system: every geometry table equals the
+    reference's Tomo_struct on the original files (small tables whole, large
+    ones through seeded samples, sums and norms)."""
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    t = M.Tomo(*systems.files(name))
+    for k in ["sspSizeL", "L0diff", "cn2", "Nsubap", "Nssp", "noiseNGS", "alphaX", "alphaY",
+              "lgsExt", "lgsTheta", "mr"]:
+        assert np.array_equal(t.table(k), z[k]), k
+    for k in ["u", "v", "X", "Y", "noiseLGSxx", "noiseLGSyy", "noiseLGSxy"]:
+        v = t.table(k)
+        assert v.size == int(z[f"{k}_n"]), k
+        assert np.array_equal(v[z[f"{k}_idx"]], z[f"{k}_val"]), k
+        assert v.sum() == float(z[f"{k}_sum"]) and np.linalg.norm(v) == float(z[f"{k}_fro"]), k
+    nW, nLgs, nL, Nx, nm, nts = z["info"]
+    assert (t.info.nW, t.info.nLgs, t.info.nLayer, t.info.Nx) == (nW, nLgs, nL, Nx)
+    assert (t.getNMeas(), t.getNMeasTS()) == (nm, nts)

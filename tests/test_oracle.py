@@ -135,3 +135,17 @@ def test_compare_matrices_semantics():
     B = np.array([[1.1, 5.0], [2.0, 4.0]])
     maxerr, fro = O.compare_matrices(A, B)
     assert np.isclose(maxerr, 5.0) and np.isclose(fro, np.sqrt(0.01 + 25))
+
+
+@pytest.mark.parametrize("name", systems.CHECK_SETS + ["elt"])
+def test_oracle_matches_reference_tiles_of_check_sets(name):
+    """The C restatement reproduces, bit for bit, the reference's tiles of Cmm,
+    Ctm and Ctt for the six reference check systems and the ELT-scale system
+    (tests/golden/ref_*.npz, from the reference's compiled code)."""
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    g = _geom(name)
+    nt = z["tile_vals"].shape[1]
+    for (typ, r0, c0), want in zip(z["tile_spec"], z["tile_vals"]):
+        got = np.zeros((nt, nt), order="F")
+        O.matcov(g, nt, nt, int(r0), int(c0), int(typ), out=got)
+        assert np.array_equal(got, want), (name, typ, r0, c0)
