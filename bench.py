@@ -8,15 +8,21 @@ tiled Cholesky of Cmm and the two triangular solves giving R = Ctm Cmm^-1.
 
     python bench.py [--gpus N --steps K --warmup W] [--path fp64|mixed]
     python bench.py --impl reference ...     # the reference's CPU path
+    python bench.py --probe STAGE --nssp S   # one stage once (profiling captures)
 
 Printed on rank 0: one JSON line. ``value`` is whole-job builds/s with the
-system tables resident in HBM; ``e2e`` is the same metric through the public
-API with the geometry uploaded from host memory and R read back to pinned host
-memory every step. Multi-GPU runs are independent replicas (one reconstructor
-per GPU, no collective on the data path). The CPU baseline / reference arm runs
-the reference's own covariance code (oracle/_ref, compiled from the reference
-sources) and LAPACK through scipy's OpenBLAS on a bounded sample of the same
-workload, extrapolated by element and flop counts.
+system tables resident in HBM. ``e2e`` is the same metric through the
+reference-shaped host-buffer entry points of the C ABI (moao_matcov_tile_host
+for Cmm and Ctm, then moao_reconstructor_host), host<->device copies inside the
+timed region, from and into pinned host memory. Beside them: the error
+covariances Cee and Cvv and the PSF Strehl ratio of the mixed path against the
+FP64 path at ELT size, their stage times, and full builds of two systems the
+CPU finishes, timed on the reference's own CPU code and on the GPU. Multi-GPU
+runs are independent replicas (one reconstructor per GPU, no collective on the
+data path). The CPU baseline / reference arm runs the reference's own code
+(oracle/_ref, compiled from the reference sources: covariance generation, and
+LAPACK through scipy's OpenBLAS) on a bounded sample of the ELT workload,
+extrapolated by element and flop counts and marked as such.
 """
 from __future__ import annotations
 
@@ -59,6 +65,14 @@ def parse():
     p.add_argument("--serve-slots", type=int, default=3)
     p.add_argument("--no-compare", action="store_true",
                    help="mixed path: skip timing the FP64 path beside it")
+    p.add_argument("--no-cee", action="store_true", help="skip the Cee/Cvv/PSF stage at ELT size")
+    p.add_argument("--no-pairs", action="store_true",
+                   help="skip the measured CPU-vs-GPU full builds of the small systems")
+    p.add_argument("--e2e-steps", type=int, default=5, help="builds timed through the host path")
+    p.add_argument("--probe", default=None,
+                   choices=["matcov_ctm", "build_fp64", "build_mixed", "cee_fp64", "cee_mixed"],
+                   help="run one stage once on the ELT geometry at --nssp subapertures (for ncu)")
+    p.add_argument("--nssp", type=int, default=37, help="probe: subapertures across (64 = ELT)")
     return p.parse_args()
 
 
@@ -127,13 +141,19 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------- CPU
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
 def cpu_reference_sample(sf, af, nm, nts, budget_s=20.0):
-    """Times the reference's CPU path on a bounded sample; returns (builds/s, info)."""
+    """Times the reference's CPU path on a bounded sample of the build and
+    extrapolates it to the whole build; returns (builds/s, info)."""
     import numpy as np
     import scipy.linalg.blas as blas
     import scipy.linalg.lapack as lapack
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = _oracle()
 
     cores = os.cpu_count() or 1
     kind = "reference" if O.RefTomo.available() else "port"
@@ -163,7 +183,7 @@ def cpu_reference_sample(sf, af, nm, nts, budget_s=20.0):
     n = 4096
     while True:
         A = rng.standard_normal((n, n))
-        C = np.asfortranarray(A @ A.T + n * np.eye(n))
+        C = np.asfortranarray(A + A.T + 4.0 * n * np.eye(n))  # SPD: diagonally dominant
         T = np.asfortranarray(rng.standard_normal((max(n // 8, 1), n)))
         t0 = time.perf_counter()
         L, info = lapack.dpotrf(C, lower=1, clean=0, overwrite_a=1)
@@ -179,7 +199,7 @@ def cpu_reference_sample(sf, af, nm, nts, budget_s=20.0):
     t_lapack = (nm ** 3 / 3) / rate_potrf + (2 * nts * nm ** 2) / rate_trsm
     total = t_matcov + t_lapack
     info = {
-        "cores": cores, "kind": kind,
+        "cores": cores, "kind": kind, "extrapolated": True,
         "sample": (f"covariance: {rows} Ctm rows x {nm} columns through the reference's matcov_tile "
                    f"({'oracle/_ref' if kind == 'reference' else 'C port'}, {cores} threads), "
                    f"{el_time * 1e6:.2f} us/element scaled to {n_el:.3e} elements; LAPACK: "
@@ -189,6 +209,58 @@ def cpu_reference_sample(sf, af, nm, nts, budget_s=20.0):
         "seconds_per_build": total,
     }
     return 1.0 / total, info
+
+
+PAIR_SYSTEMS = ("small", "nx5120_nLayers10_wfs8_Nssp29")
+
+
+def pair_system(name):
+    """(label, sys file, atm file) of a system the CPU builds in full: the 8 m
+    small system, or a check system of the reference (datafile/check, parsed
+    into tests/golden/check_sets.json)."""
+    from moao_b200 import params as P
+    if name == "small":
+        sp, ap = P.config_small()
+        label = "8 m, 10x10, 3 LGS + 1 NGS + TS, 3 layers"
+    else:
+        with open(os.path.join(ROOT, "tests", "golden", "check_sets.json")) as f:
+            d = json.load(f)[name]
+        sp, ap = P.SysParams(**d["sys"]), P.AtmParams(**d["atm"])
+        label = (f"reference check system {name} ({sp.diam:g} m, {sp.nssp}x{sp.nssp}, {sp.nLgs} LGS + "
+                 f"{sp.nW - sp.nLgs - 1} NGS + TS, {ap.nLayer} layers)")
+    d = tempfile.mkdtemp(prefix="moao_pair_")
+    P.write_system(d, sp, ap)
+    return label, os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt")
+
+
+def cpu_full_build(sf, af):
+    """One full FP64 build on the host cores with the reference's own code:
+    matcov_tile of Cmm and Ctm (oracle/_ref, all cores on independent tiles),
+    then MOAO_LAPACK::reconstructor (oracle/_ref, scipy's OpenBLAS threads).
+    Returns (seconds, R, nmeas, nmeasts, cores)."""
+    O = _oracle()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    t = O.RefTomo(sf, af)
+    nm, nts = t.info.nmeas, t.info.nmeasts
+    t.setTarget(0)
+    Cmm = t.matcov_full(nm, nm, 1, nthreads=cores)
+    Ctm = t.matcov_full(nts, nm, 3, nthreads=cores)
+    if O.RefDense.available():
+        _, R = O.RefDense.reconstructor(Cmm, Ctm)
+    else:
+        _, R, _ = O.reconstructor(Cmm, Ctm)
+    return time.perf_counter() - t0, R, nm, nts, cores
+
+
+def cpu_reference_pairs():
+    """The reference's CPU path, full builds of the pair systems (seconds each)."""
+    out = []
+    for name in PAIR_SYSTEMS:
+        label, sf, af = pair_system(name)
+        sec, _, nm, nts, cores = cpu_full_build(sf, af)
+        out.append({"system": label, "nmeas": nm, "nmeasts": nts, "cpu_s": sec, "cores": cores})
+    return out
 
 
 # ----------------------------------------------------------------------------- GPU
@@ -211,6 +283,181 @@ def fp64_peak_tflops(torch):
     del a, b
     torch.cuda.empty_cache()
     return 2 * n ** 3 / best / 1e9
+
+
+def lower_panel_bytes(nrows, ncols, d, corner_only, w=512):
+    """Bytes moved by the host entry points' lower-part copies (the column-panel
+    copies of moao_matcov_tile_host / moao_reconstructor_host)."""
+    total = 0
+    for c0 in range(0, ncols, w):
+        c1 = min(ncols, c0 + w)
+        r0 = max(0, c0 - d)
+        if r0 >= nrows:
+            break
+        r1 = min(nrows, max(r0, c1 - d)) if corner_only else nrows
+        total += 8 * (r1 - r0) * (c1 - c0)
+    return total
+
+
+def gpu_build_device(M, torch, ctx, t, nm, nts, prec, rep_out=None, reps=5):
+    """Median device ms of full builds (matcov Cmm + Ctm, reconstructor) through
+    the device API, and the R of the last one (its solve report into rep_out)."""
+    Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
+    Ctm = torch.empty((nm, nts), dtype=torch.float64, device="cuda")
+    ms = []
+    for k in range(reps + 2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        rep = M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=prec, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        if k >= 2:
+            ms.append(e0.elapsed_time(e1))
+        if rep_out is not None:
+            rep_out.update(rep)
+    import numpy as np
+    R = Ctm.cpu().numpy().T.copy(order="F")
+    return float(np.median(ms)), R
+
+
+def gpu_build_host(M, t, nm, nts, prec, ctx, reps=3):
+    """Median wall ms of full builds through the host-buffer (drop-in) entry
+    points: moao_matcov_tile_host for Cmm and Ctm, moao_reconstructor_host."""
+    import numpy as np
+    Cmm = np.zeros((nm, nm), order="F")
+    Ctm = np.zeros((nts, nm), order="F")
+    ms = []
+    for k in range(reps + 1):
+        t0 = time.perf_counter()
+        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=prec, ctx=ctx)
+        if k >= 1:
+            ms.append(1000.0 * (time.perf_counter() - t0))
+    return float(np.median(ms))
+
+
+def measured_pairs(M, torch, ctx):
+    """Full builds of the pair systems on the reference's CPU code and on the
+    GPU (device API FP64 and mixed, and the drop-in host path FP64), with the
+    agreement of the GPU FP64 R with the CPU R."""
+    O = _oracle()
+    out = []
+    for name in PAIR_SYSTEMS:
+        label, sf, af = pair_system(name)
+        t = M.Tomo(sf, af)
+        t.setTarget(0)
+        nm, nts = t.getNMeas(), t.getNMeasTS()
+        ms64, R64 = gpu_build_device(M, torch, ctx, t, nm, nts, "fp64")
+        ctx.set_offsets_from_tomo(t)
+        ctx.set_accuracy(1e-5)  # ill-conditioned systems fall back to FP64
+        rep = {}
+        msmx, Rmx = gpu_build_device(M, torch, ctx, t, nm, nts, "mixed", rep)
+        ctx.set_accuracy(0)
+        ms_host = gpu_build_host(M, t, nm, nts, "fp64", ctx)
+        cpu_s, Rc, _, _, cores = cpu_full_build(sf, af)
+        out.append({
+            "system": label, "nmeas": nm, "nmeasts": nts,
+            "cpu_reference_s": cpu_s, "cpu_cores": cores,
+            "cpu_kind": "reference" if O.RefDense.available() else "reference matcov + oracle LAPACK",
+            "gpu_fp64_ms": ms64, "gpu_mixed_ms": msmx, "gpu_fp64_dropin_host_ms": ms_host,
+            "speedup_fp64": cpu_s * 1000.0 / ms64, "speedup_mixed": cpu_s * 1000.0 / msmx,
+            "speedup_fp64_dropin": cpu_s * 1000.0 / ms_host,
+            "rel_fro_R_gpu_fp64_vs_cpu": O.rel_fro(R64, Rc), "rel_fro_R_gpu_mixed_vs_cpu": O.rel_fro(Rmx, Rc),
+            "mixed_accuracy_target": 1e-5, "mixed_fell_back_to_fp64": bool(rep.get("fallback")),
+            "mixed_est_error": rep.get("est_error"),
+        })
+    ctx.set_offsets([], [], [])
+    return out
+
+
+def cee_stage(M, torch, ctx, t, nm, nts, Cmm, R_fp64, R_mixed):
+    """Cee, Cvv and the PSF at ELT size from the FP64 R through the FP64 chain
+    and from the mixed R through the mixed chain: stage times (second call of
+    each; CUDA events on the context stream) and the relative Frobenius errors
+    and Strehl-ratio difference of the mixed results against the FP64 ones."""
+    import numpy as np
+    from moao_b200 import inputs as I
+    x = I.intersample_inputs(t.info.nssp_ts, t.info.diam, t.info.obs)
+    nact = x.nact
+    Dx = torch.from_numpy(np.ascontiguousarray(I.make_dx(nact, nts).T)).cuda()
+    Ctm2 = torch.empty((nm, nts), dtype=torch.float64, device="cuda")
+    Ctt = torch.empty((nts, nts), dtype=torch.float64, device="cuda")
+    Cee = torch.empty((nts, nts), dtype=torch.float64, device="cuda")
+    Cvv = torch.empty((nact, nact), dtype=torch.float64, device="cuda")
+    Tmp = torch.empty((nts, nact), dtype=torch.float64, device="cuda")
+    res = {}
+    for prec, R in (("fp64", R_fp64), ("mixed", R_mixed)):
+        for k in range(2):  # the first call sizes the workspaces
+            M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+            M.matcov_tile(Ctm2, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+            M.matcov_tile(Ctt, nts, nts, 0, 0, nts, t, 4, ctx=ctx)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            M.Cee_Cvv(nm, nts, nact, Cmm, nm, Ctt, nts, Ctm2, nts, R, nts, Dx, nact, Cee, nts, Cvv,
+                      nact, Tmp, nact, prec=prec, ctx=ctx)
+            e1.record()
+            torch.cuda.synchronize()
+        res[prec] = (Cee.clone(), Cvv.clone(), e0.elapsed_time(e1))
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    isx = M.Intersample(nact * nact, x.np_, t.info.diam, x.idx, x.abs2fi, x.otf, ctx=ctx)
+    psf0 = isx.process(torch.zeros((nact, nact), dtype=torch.float64, device="cuda"))
+    peak0 = float(psf0.max())
+    strehl = lambda C, c: float(isx.process(c * C).max()) / peak0
+    # The seeded N(0, 1) Dx gives phase variances whose PSF is all halo (Strehl
+    # ~1e-5): both Cvv are scaled by the one factor that puts the FP64 Strehl at
+    # 0.5 (bisection in log c; Cvv is quadratic in Dx, so this is Dx scaled).
+    lo, hi = -40.0, 10.0
+    for _ in range(48):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if strehl(res["fp64"][1], 10.0 ** mid) > 0.5 else (lo, mid)
+    c = 10.0 ** (0.5 * (lo + hi))
+    s_raw = strehl(res["fp64"][1], 1.0)
+    s64 = strehl(res["fp64"][1], c)
+    smx = strehl(res["mixed"][1], c)
+    isx.close()
+    out = {"nact": nact, "ms_fp64_chain": res["fp64"][2], "ms_mixed_chain": res["mixed"][2],
+           "rel_fro_err_Cee_vs_fp64": rel(res["mixed"][0], res["fp64"][0]),
+           "rel_fro_err_Cvv_vs_fp64": rel(res["mixed"][1], res["fp64"][1]),
+           "strehl_fp64": s64, "strehl_mixed": smx, "strehl_delta": abs(smx - s64),
+           "strehl_cvv_scale": c, "strehl_fp64_unscaled_dx": s_raw,
+           "note": ("Cee/Cvv from the FP64 R by the FP64 chain against those from the mixed R by "
+                    "the mixed chain (int8 Ozaki products); Strehl = PSF peak / telescope-only peak, "
+                    "512^2 PSF on the truth direction, both Cvv scaled by strehl_cvv_scale so that the "
+                    "FP64 Strehl is 0.5")}
+    del Ctm2, Ctt, Cee, Cvv, Tmp, Dx, res
+    torch.cuda.empty_cache()
+    return out
+
+
+def e2e_dropin(M, torch, ctx, t, nm, nts, prec, steps, set_profile):
+    """Builds through the reference-shaped host-buffer entry points of the C
+    ABI (moao_matcov_tile_host of Cmm and Ctm, then moao_reconstructor_host),
+    host buffers in pinned memory, every copy inside the timed region."""
+    Cmm_h = torch.empty((nm, nm), dtype=torch.float64, pin_memory=True).numpy().T
+    Ctm_h = torch.empty((nm, nts), dtype=torch.float64, pin_memory=True).numpy().T
+
+    def one():
+        set_profile()
+        M.matcov_tile(Cmm_h, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm_h, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        M.reconstructor(nm, nts, Cmm_h, nm, Ctm_h, nts, 1, prec=prec, ctx=ctx)
+    one()  # sizes the host-path workspaces
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    R = Ctm_h.copy(order="F")
+    h2d = (lower_panel_bytes(nm, nm, 0, True) + lower_panel_bytes(nm, nm, 0, False) +
+           8 * nm * nts)
+    d2h = 2 * lower_panel_bytes(nm, nm, 0, False) + 2 * 8 * nm * nts
+    del Cmm_h, Ctm_h
+    return sec, h2d, d2h, R
 
 
 def read_traffic_ratio(name, key="dram_bytes_per_work"):
@@ -434,8 +681,60 @@ def batch_main(args):
     return 0
 
 
+def probe_main(args):
+    """One stage, once, on the ELT geometry scaled to args.nssp subapertures
+    across (35 layers; 64 gives the ELT system itself). For profiler captures:
+    the ncu commands in profiles/ run this."""
+    import numpy as np
+    import torch
+    import moao_b200 as M
+    from moao_b200 import params as P
+    from moao_b200 import inputs as I
+    sp, ap = P.config_elt() if args.nssp == 64 else P.config_scaled(args.nssp, 35)
+    d = tempfile.mkdtemp(prefix="moao_probe_")
+    P.write_system(d, sp, ap)
+    torch.cuda.set_device(0)
+    ctx = M.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ctx.set_block(args.nb or 1024)
+    t = M.Tomo(os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt"))
+    t.setTarget(0)
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    Ctm = torch.empty((nm, nts), dtype=torch.float64, device="cuda")
+    t0 = time.perf_counter()
+    if args.probe == "matcov_ctm":
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+    else:
+        prec = "mixed" if args.probe.endswith("mixed") else "fp64"
+        if prec == "mixed":
+            ctx.set_offsets_from_tomo(t)
+        Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
+        M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+        M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec=prec, ctx=ctx)
+        if args.probe.startswith("cee"):
+            nact = I.make_dm(t.info.nssp_ts, 0.2, t.info.obs).nactu
+            Dx = torch.from_numpy(np.ascontiguousarray(I.make_dx(nact, nts).T)).cuda()
+            Ctm2 = torch.empty((nm, nts), dtype=torch.float64, device="cuda")
+            Ctt = torch.empty((nts, nts), dtype=torch.float64, device="cuda")
+            Cee = torch.empty((nts, nts), dtype=torch.float64, device="cuda")
+            Cvv = torch.empty((nact, nact), dtype=torch.float64, device="cuda")
+            Tmp = torch.empty((nts, nact), dtype=torch.float64, device="cuda")
+            M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+            M.matcov_tile(Ctm2, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+            M.matcov_tile(Ctt, nts, nts, 0, 0, nts, t, 4, ctx=ctx)
+            M.Cee_Cvv(nm, nts, nact, Cmm, nm, Ctt, nts, Ctm2, nts, Ctm, nts, Dx, nact, Cee, nts,
+                      Cvv, nact, Tmp, nact, prec=prec, ctx=ctx)
+    torch.cuda.synchronize()
+    print(json.dumps({"probe": args.probe, "nssp": args.nssp, "nmeas": nm, "nmeasts": nts,
+                      "wall_s": time.perf_counter() - t0, "launches": ctx.launches}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.probe:
+        return probe_main(args)
     if args.serving:
         return serving_main(args)
     if args.batch:
@@ -448,25 +747,42 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        import moao_b200 as M
-        t = M.Tomo(sf, af)
-        nm, nts = t.getNMeas(), t.getNMeasTS()
-        vals = []
+        # sizes from the reference's own Tomo_struct (oracle/_ref): nothing of
+        # this repository's library is loaded on this arm
+        O = _oracle()
+        if O.RefTomo.available():
+            ri = O.RefTomo(sf, af).info
+            nm, nts = ri.nmeas, ri.nmeasts
+        else:
+            import moao_b200 as M
+            t = M.Tomo(sf, af)
+            nm, nts = t.getNMeas(), t.getNMeasTS()
+        vals, walls = [], []
         for i in range(args.warmup + args.steps):
-            v, info = cpu_reference_sample(sf, af, nm, nts, budget_s=8.0)
+            t0 = time.perf_counter()
+            v, info = cpu_reference_sample(sf, af, nm, nts, budget_s=3.0)
             if i >= args.warmup:
                 vals.append(v)
+                walls.append(time.perf_counter() - t0)
         value = statistics.median(vals)
+        pairs = None if args.no_pairs else cpu_reference_pairs()
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "extrapolated": True,
+            "sample_wall_s_per_step": statistics.median(walls),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded ELT-scale system)",
             "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer),
                        "path": "reference CPU (matcov_tile + LAPACK)", "parallelism": "host cores"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
-                             "sample": info["sample"]},
+                             "extrapolated": True, "sample": info["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "measured_full_builds": pairs,
+            "note": ("value: each step times a bounded sample of the ELT build (Ctm rows through the "
+                     "reference's matcov_tile, dpotrf/dtrsm at a reduced size) and extrapolates it to the "
+                     "whole build by element and flop counts; measured_full_builds: whole builds of two "
+                     "smaller systems, timed end to end"),
         }
         print(json.dumps(line), flush=True)
         return 0
@@ -559,7 +875,7 @@ def main():
 
     # The mixed path is reported beside the FP64 path of the same build: its
     # builds/s in this run and the relative Frobenius error of R between them.
-    rel_err, fp64_arm = None, None
+    rel_err, fp64_arm, cee = None, None, None
     if args.path == "mixed":
         R_mixed = Ctm.clone()
         ctx.set_block(args.nb_fp64)
@@ -574,27 +890,54 @@ def main():
                                        "p99": float(np.percentile(arm["per_step"], 99))},
                         "panel_nb": args.nb_fp64, "mixed_over_fp64": value / v64}
         rel_err = float(torch.linalg.norm(R_mixed - Ctm) / torch.linalg.norm(Ctm))
+        # ---- Cee, Cvv and the PSF from both R (Ctm holds the FP64 R now)
+        if not args.no_cee:
+            cee = cee_stage(M, torch, ctx, t, nm, nts, Cmm, Ctm, R_mixed)
         del R_mixed
+        torch.cuda.empty_cache()
+        ctx.set_block(nb_main)
 
-    # ---- e2e through the public API with host buffers
-    e2e = None
+    def set_profile():
+        t.set_profile(cn2_p, h_p, L0_p)
+
+    geom_bytes = 8 * (2 * atm.nLayer * (nm // 2 + nts // 2) + 5 * (nm // 2 + nts // 2) +
+                      sysp.nW * atm.nLayer + 3 * atm.nLayer + sysp.nW)
+    # ---- e2e through the drop-in host-buffer entry points of the C ABI
+    e2e, e2e_api = None, None
     if not args.no_e2e:
-        R_host = torch.empty((nm, nts), dtype=torch.float64, pin_memory=True)
-        cn2 = np.array(atm.cn2, dtype=np.float64)
-        h, L0 = np.array(atm.h), np.array(atm.L0)
-        geom_bytes = 8 * (2 * atm.nLayer * (nm // 2 + nts // 2) + 5 * (nm // 2 + nts // 2) +
-                          sysp.nW * atm.nLayer + 3 * atm.nLayer + sysp.nW)
+        del Cmm
+        torch.cuda.empty_cache()
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
+        ksteps = max(1, min(args.steps, args.e2e_steps))
+        sec, h2d, d2h, R_dropin = e2e_dropin(M, torch, ctx, t, nm, nts, args.path, ksteps,
+                                             set_profile)
+        e2e_s = max_over_ranks(sec, dist, "cuda")
+        e2e = {"value": world * ksteps / e2e_s, "unit": UNIT, "steps": ksteps,
+               "h2d_bytes_per_step": int(h2d + geom_bytes), "d2h_bytes_per_step": int(d2h),
+               "path": ("C ABI host-buffer entry points, as the reference's driver calls them: "
+                        "moao_matcov_tile_host (Cmm, Ctm) then moao_reconstructor_host; pinned host "
+                        "buffers; only the lower part of Cmm crosses PCIe"),
+               "rel_fro_R_vs_device_path": float(np.linalg.norm(R_dropin - Ctm.cpu().numpy().T) /
+                                                 np.linalg.norm(R_dropin)) if args.path == "fp64"
+               else None}
+        del R_dropin
+        Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
+        # the public device API with the profile set from host memory every step and
+        # R read back to pinned memory (the serving loop's flow)
+        R_host = torch.empty((nm, nts), dtype=torch.float64, pin_memory=True)
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for k in range(args.steps):
+        for k in range(ksteps):
             step(args.path)             # host profile -> geometry recomputed and re-uploaded
             R_host.copy_(Ctm, non_blocking=True)
             torch.cuda.synchronize()
-        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-        e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(geom_bytes), "d2h_bytes_per_step": int(nm * nts * 8)}
+        api_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        e2e_api = {"value": world * ksteps / api_s, "unit": UNIT, "steps": ksteps,
+                   "h2d_bytes_per_step": int(geom_bytes), "d2h_bytes_per_step": int(nm * nts * 8),
+                   "path": "device API: profile from host memory in, R out to pinned memory"}
+        del R_host
 
     # ---- roofline of the dominant kernel family (largest share of device time),
     # and of the largest tensor-core family beside it
@@ -618,17 +961,22 @@ def main():
                     "traffic": (ratio * s["work"] / s["launches"]) if ratio else None,
                     "launches": s["launches"], "share": share}
         if fam in ("tc_split", "tc_int8"):
-            bf16 = float(peaks.get("bf16_tflops", 1590.0))
+            # timed inside a seconds-long build: the sustained (power-capped) peak
+            bf16 = float(peaks.get("bf16_tflops_sustained", 1400.0))
             peak = bf16 * (2.0 if fam == "tc_int8" else 1.0)
             achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
             what = "int8" if fam == "tc_int8" else "fp16/bf16 split"
+            ratio = read_traffic_ratio("tc_gemm_int8_residual_nmeas15936.txt" if fam == "tc_int8"
+                                       else "tc_gemm_f16_trailing_nmeas15936.txt")
             return {"kernel": f"tc_gemm_kernel ({what} tcgen05, TMA, TMEM)", "bound": "tensor",
                     "achieved": round(achieved, 3), "peak": round(peak, 3),
                     "unit": "TFLOP/s" if fam == "tc_split" else "TOP/s",
                     "frac": round(achieved / peak, 4),
-                    "peak_source": (f"bf16_tflops (burst) {peak_src}" if fam == "tc_split" else
-                                    f"2 x bf16_tflops {peak_src} (the dense int8 rate is twice bf16)"),
-                    "traffic": None, "launches": s["launches"], "share": share}
+                    "peak_source": (f"bf16_tflops_sustained {peak_src}" if fam == "tc_split" else
+                                    f"2 x bf16_tflops_sustained {peak_src} (the dense int8 rate is "
+                                    "twice bf16)"),
+                    "traffic": (ratio * s["work"] / s["launches"]) if ratio else None,
+                    "launches": s["launches"], "share": share}
         if fam == "matcov":
             # HBM framing (bytes stored); the kernel itself is bound by its FP64 pipe
             hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -651,21 +999,40 @@ def main():
     def roofline_tc_kernel():
         """tc_gemm_kernel as one kernel: its fp16 launches (tc_split) and its int8
         launches (tc_int8) together, in bf16-equivalent flop (an int8 op counts
-        half, the dense int8 rate being twice bf16's) against the bf16 peak."""
+        half, the dense int8 rate being twice bf16's) against the sustained bf16
+        peak; beside it the FP64-equivalent rate: the build's algorithmic FP64
+        flop (POTRF nmeas^3/3, the two triangular solves 2 nmeasts nmeas^2, and per
+        refinement step the residual and the correction solve, 2 nmeasts nmeas^2
+        each) over the kernel's time."""
         a, b = stats["tc_split"], stats["tc_int8"]
         ms = a["ms"] + b["ms"]
         if ms <= 0:
             return None
-        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        bf16 = float(peaks.get("bf16_tflops_sustained", 1400.0))
         achieved = (a["work"] + 0.5 * b["work"]) / (ms / 1000.0) / 1e12
+        ra = read_traffic_ratio("tc_gemm_f16_trailing_nmeas15936.txt")
+        rb = read_traffic_ratio("tc_gemm_int8_residual_nmeas15936.txt")
+        traffic = None
+        if ra and rb:
+            traffic = (ra * a["work"] + rb * b["work"]) / max(1, a["launches"] + b["launches"])
+        refine = 1 if args.path == "mixed" else 0
+        fp64_flop = (nm ** 3 / 3.0 + 2.0 * nts * nm * nm * (1 + 2 * refine)) * args.steps
+        fp64_equiv = fp64_flop / (ms / 1000.0) / 1e12
         return {"kernel": "tc_gemm_kernel (tcgen05 kind::f16 fp16-split products and kind::i8 Ozaki "
                           "residual; TMA, TMEM)", "bound": "tensor",
                 "achieved": round(achieved, 3), "peak": round(bf16, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / bf16, 4),
-                "peak_source": f"bf16_tflops (burst) {peak_src}; int8 ops counted at half weight",
-                "traffic": None,
-                "traffic_note": ("per-launch DRAM traffic in profiles/: int8 residual launch 2.49 GB per "
-                                 "4.05e12 op (nmeas 15,936); the operands stay L2-resident at 84-89 % hit"),
+                "peak_source": (f"bf16_tflops_sustained {peak_src} (the kernel runs inside a "
+                                "seconds-long build); int8 ops counted at half weight"),
+                "fp64_equivalent_achieved": round(fp64_equiv, 3),
+                "frac_fp64_equivalent": round(fp64_equiv / bf16, 4),
+                "fp64_equivalent_note": ("algorithmic FP64 flop of the build over this kernel's time: "
+                                         "the split products multiply the tensor work (3 fp16 products "
+                                         "per update, 15 int8 slice pairs per residual)"),
+                "traffic": traffic,
+                "traffic_note": ("DRAM bytes per launch: each family's bytes per unit of work from its "
+                                 "ncu capture in profiles/ (nmeas 15,936) times the work of this run's "
+                                 "launches"),
                 "launches": a["launches"] + b["launches"], "share": round(ms / total_ms, 4),
                 "families": {"tc_split": roofline_of("tc_split"), "tc_int8": roofline_of("tc_int8")}}
 
@@ -700,11 +1067,17 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": e2e,
+        "e2e_device_api": e2e_api,
+        "cee_cvv_psf": cee,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(sf, af, nm, nts)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
-                                "sample": info["sample"]}
+                                "extrapolated": True, "sample": info["sample"]}
+    if rank == 0 and world == 1 and not args.no_pairs:
+        del Cmm, Ctm
+        torch.cuda.empty_cache()
+        line["measured_full_builds"] = measured_pairs(M, torch, ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

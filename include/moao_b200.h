@@ -116,8 +116,28 @@ moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* ctx, const moao_tomo* tomo)
  * turn it off when other work should have every SM. No reference counterpart. */
 moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int sms);
 
-/* Precision of moao_reconstructor_host (default MOAO_PREC_FP64, the
- * reference's behaviour). No reference counterpart. */
+/* Accuracy target of the mixed reconstructor (relative Frobenius error of R;
+ * 0, the default, turns the check off). With a target, the mixed path also
+ * evaluates the residual after its last correction and estimates the error of
+ * R as ||dR|| / ||R|| of that correction times the residual's reduction by it;
+ * if the estimate exceeds the target (refinement stalls on ill-conditioned
+ * systems), the FP64 path computes R from the untouched Cmm and Ctm instead,
+ * the report's fallback is 1 and the call still returns MOAO_OK (Cmm then holds
+ * the FP64 factor). The estimate is in the report's est_error. No reference
+ * counterpart. */
+moao_status moao_ctx_set_accuracy(moao_ctx* ctx, double target);
+
+/* Bound of every wait inside the tensor-core kernel of the mixed paths, in
+ * polls of its mbarrier (0 restores the default, 2^28: seconds). A wait that
+ * runs out ends the kernel early (its copies and tensor-core operations in
+ * flight drained, its tensor memory freed) and the call returns
+ * MOAO_ERR_TIMEOUT with its outputs undefined; the context stays usable. Applies
+ * to this context's own calls (not the batch engine's sub-contexts). No
+ * reference counterpart. */
+moao_status moao_ctx_set_wait_limit(moao_ctx* ctx, long long polls);
+
+/* Precision of moao_reconstructor_host and moao_cee_cvv_host (default
+ * MOAO_PREC_FP64, the reference's behaviour). No reference counterpart. */
 moao_status moao_ctx_set_host_precision(moao_ctx* ctx, moao_prec prec);
 
 /* Number of kernels this library launched on the context since creation. */
@@ -181,6 +201,10 @@ typedef struct {
   double ms_factor;      /* device time of the Cholesky factorisation         */
   double ms_solve;       /* device time of the two triangular solves           */
   double ms_refine;      /* device time of the refinement                      */
+  int fallback;          /* mixed path with an accuracy target: 1 when the     */
+                         /* estimate missed it and the FP64 path produced R    */
+  double est_error;      /* mixed path with an accuracy target: estimated      */
+                         /* relative Frobenius error of the mixed R            */
 } moao_solve_report;
 
 moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* d_Cmm,
@@ -225,6 +249,23 @@ moao_status moao_cee_cvv(moao_ctx* ctx, long nmeas, long nmeasts, long nact,
                          double* Cpm, long ldCpm, double* R, long ldR,
                          double* Dx, long ldDx, double* Cee, long ldCee,
                          double* Cvv, long ldCvv, double* Tmp, long ldTmp);
+/* Cee_Cvv in a chosen precision. MOAO_PREC_FP64 is moao_cee_cvv. MOAO_PREC_MIXED
+ * uses the reconstructor's residual E = Ctm - R Cmm: in exact arithmetic
+ * R Cmm R^T = Ctm R^T - E R^T, so Cee = Ctt - R Ctm^T - E R^T; the products
+ * R Ctm^T, R Cmm and E R^T run on the int8 tensor cores with the Ozaki
+ * splitting (exact int32 accumulation, FP64 sums; the context's int8 slice
+ * count, moao_ctx_set_mixed, and its declared offsets of Cmm apply), and
+ * Tmp = Dx Cee, Cvv = Tmp Dx^T in FP64. In-place contract of the mixed path: Cpm
+ * ends as R Cmm, Cpp (Ctt, lower triangle read) is left as given, Tmp holds
+ * Dx sym(Cee). The mixed path synchronises the context stream before it
+ * returns (it reads the kernels' error flag). No reference counterpart. */
+moao_status moao_cee_cvv_prec(moao_ctx* ctx, long nmeas, long nmeasts, long nact,
+                              double* Cmm, long ldCmm, double* Cpp, long ldCpp,
+                              double* Cpm, long ldCpm, double* R, long ldR,
+                              double* Dx, long ldDx, double* Cee, long ldCee,
+                              double* Cvv, long ldCvv, double* Tmp, long ldTmp,
+                              moao_prec prec);
+/* Host buffers; precision from moao_ctx_set_host_precision (default FP64). */
 moao_status moao_cee_cvv_host(moao_ctx* ctx, long nmeas, long nmeasts, long nact,
                               double* Cmm, long ldCmm, double* Cpp, long ldCpp,
                               double* Cpm, long ldCpm, double* R, long ldR,

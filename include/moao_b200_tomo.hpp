@@ -29,14 +29,26 @@ class SysParams {
   int RON = 0;
   T lgsCst = 0, spotWidth = 0, lgsAlt = 0, lgsDepth = 0;
   std::vector<T> targetX_as, targetY_as;
+  // Read from a legacy benchmark file (datafile/benchmark/*/sys-params.txt):
+  // its uniform noise variance replaces the photometric noise model.
+  int legacy = 0;
+  T noiseVar = 0;
 
   SysParams() = default;
   explicit SysParams(const std::string& sf) { read(sf); }
   // Positional reader of sys-params.txt: one comment line before every value
   // line (SysParams::getParams, common/tomo_struct/sysParams.cpp:166-204).
+  // A file of at most 24 value lines is read in the legacy benchmark layout
+  // instead (22 fields: diam, obs, nW, Nssp, gsAlt, type, nLgs, alphaX,
+  // alphaY, XPup, YPup, thetaML, thetaCam, sensibilite, tracking, pasDphi,
+  // ncpu, lgs_cst, noise_var, spot_width, lgs_alt, lgs_depth), the fields it
+  // lacks taking the reference constructor's defaults (one on-axis target).
   // Throws std::runtime_error on a missing file or a short vector.
   void read(const std::string& sf);
   void write(const std::string& sf) const;
+
+ private:
+  void read_current(const std::string& sf);
 };
 
 template <typename T>

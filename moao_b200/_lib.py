@@ -32,7 +32,8 @@ class TomoInfo(C.Structure):
 
 class SolveReport(C.Structure):
     _fields_ = [("info", i32), ("refine_steps", i32), ("refine_resid", C.c_double),
-                ("ms_factor", C.c_double), ("ms_solve", C.c_double), ("ms_refine", C.c_double)]
+                ("ms_factor", C.c_double), ("ms_solve", C.c_double), ("ms_refine", C.c_double),
+                ("fallback", i32), ("est_error", C.c_double)]
 
 
 class IsampleInfo(C.Structure):
@@ -100,6 +101,8 @@ SIGNATURES = {
     "moao_ctx_set_mixed": (i32, [vp, i32, i32, i32, i32, C.c_double, i32]),
     "moao_ctx_set_offsets": (i32, [vp, i32, vp, vp, vp]),
     "moao_ctx_set_host_precision": (i32, [vp, i32]),
+    "moao_ctx_set_wait_limit": (i32, [vp, C.c_longlong]),
+    "moao_ctx_set_accuracy": (i32, [vp, C.c_double]),
     "moao_ctx_set_factor_format": (i32, [vp, i32]),
     "moao_ctx_set_lookahead": (i32, [vp, i32]),
     "moao_server_create": (i32, [C.POINTER(ServerOpts), C.POINTER(vp)]),
@@ -133,6 +136,7 @@ SIGNATURES = {
     "moao_reconstructor_noalloc": (i32, [i64, i64, dp, i64, dp, i64, i64, vp, C.POINTER(i32)]),
     "moao_cee_cvv": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
     "moao_cee_cvv_host": (i32, [vp, i64, i64, i64] + [dp, i64] * 8),
+    "moao_cee_cvv_prec": (i32, [vp, i64, i64, i64] + [dp, i64] * 8 + [i32]),
     "moao_intersample_create": (i32, [vp, i64, i64, C.c_double, dp, dp, dp, C.POINTER(vp)]),
     "moao_intersample_get_info": (i32, [vp, C.POINTER(IsampleInfo)]),
     "moao_intersample_process": (i32, [vp, dp, dp]),

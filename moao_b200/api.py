@@ -182,6 +182,16 @@ class Context:
         check(lib().moao_ctx_set_offsets_from_tomo(self._h, tomo.handle),
               "moao_ctx_set_offsets_from_tomo")
 
+    def set_accuracy(self, target: float = 0.0):
+        """Accuracy target of the mixed reconstructor (0: off); a miss makes the
+        FP64 path compute R (report fallback = 1). See moao_ctx_set_accuracy."""
+        check(lib().moao_ctx_set_accuracy(self._h, float(target)), "moao_ctx_set_accuracy")
+
+    def set_wait_limit(self, polls: int = 0):
+        """Bound of the tensor-core kernel's waits in polls (0: the default);
+        see moao_ctx_set_wait_limit."""
+        check(lib().moao_ctx_set_wait_limit(self._h, int(polls)), "moao_ctx_set_wait_limit")
+
     def set_kernel_timing(self, enable: bool):
         check(lib().moao_ctx_set_kernel_timing(self._h, int(enable)), "moao_ctx_set_kernel_timing")
 
@@ -311,8 +321,9 @@ def reconstructor(nmeas: int, nmeasts: int, Cmm, ldCmm: int, Ctm, ldCtm: int, ng
             st = lib().moao_reconstructor(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
                                           PREC[prec], C.byref(rep))
     else:
-        if prec != "fp64":
-            raise ValueError("the host-buffer reconstructor runs the FP64 path")
+        # host buffers: the drop-in entry point, in the precision asked for
+        check(lib().moao_ctx_set_host_precision(ctx.handle, PREC[prec]),
+              "moao_ctx_set_host_precision")
         st = lib().moao_reconstructor_host(ctx.handle, nmeas, nmeasts, pc, ldCmm, pt, ldCtm, ngal,
                                            C.byref(rep))
     check(st, "reconstructor", column=rep.info) if st == 2 else check(st, "reconstructor")
@@ -320,9 +331,12 @@ def reconstructor(nmeas: int, nmeasts: int, Cmm, ldCmm: int, Ctm, ldCtm: int, ng
 
 
 def Cee_Cvv(nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx, ldDx, Cee,
-            ldCee, Cvv, ldCvv, Tmp, ldTmp, ctx: Optional[Context] = None):
+            ldCee, Cvv, ldCvv, Tmp, ldTmp, prec: str = "fp64", ctx: Optional[Context] = None):
     """Cee = Ctt - Ctm R^T - R Ctm^T + R Cmm R^T ; Cvv = Dx Cee Dx^T (Cpp and Cpm
-    are destroyed, Tmp is scratch), exactly the reference's in-place contract."""
+    are destroyed, Tmp is scratch), exactly the reference's in-place contract.
+    prec "mixed" (device buffers) evaluates Cee = Ctt - R Ctm^T - E R^T with the
+    residual E = Ctm - R Cmm on the int8 tensor cores (moao_cee_cvv_prec); Cpm
+    then ends as R Cmm and Cpp is left as given."""
     ctx = ctx or default_context()
     mats = [Cmm, Cpp, Cpm, R, Dx, Cee, Cvv, Tmp]
     names = ["Cmm", "Cpp", "Cpm", "R", "Dx", "Cee", "Cvv", "Tmp"]
@@ -331,9 +345,14 @@ def Cee_Cvv(nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx
     for m, n, ld in zip(mats, names, lds):
         args += [_ptr(m, n), ld]
     dev = _on_device(*mats)
-    f = lib().moao_cee_cvv if dev else lib().moao_cee_cvv_host
     with _TorchOrder(ctx, dev):
-        check(f(ctx.handle, nmeas, nmeasts, nact, *args), "Cee_Cvv")
+        if dev:
+            st = lib().moao_cee_cvv_prec(ctx.handle, nmeas, nmeasts, nact, *args, PREC[prec])
+        else:
+            check(lib().moao_ctx_set_host_precision(ctx.handle, PREC[prec]),
+                  "moao_ctx_set_host_precision")
+            st = lib().moao_cee_cvv_host(ctx.handle, nmeas, nmeasts, nact, *args)
+        check(st, "Cee_Cvv")
 
 
 class Intersample:

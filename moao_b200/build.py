@@ -26,14 +26,6 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
           "-I" + INCLUDE, "-I" + CSRC, "--expt-relaxed-constexpr"]
 
 
-def _cutlass_include():
-    for p in glob.glob(os.path.join(sys.prefix, "lib", "python3*", "site-packages", "flashinfer",
-                                    "data", "cutlass", "include")):
-        if os.path.isdir(p):
-            return p
-    return None
-
-
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
@@ -55,15 +47,12 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         raise RuntimeError(f"nvcc not found at {NVCC}")
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
-    cutlass = _cutlass_include()
     objs, cmds = [], []
     for src in _sources():
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
             flags = list(COMMON)
-            if cutlass:
-                flags.append("-I" + cutlass)
             if src.endswith(".cpp"):
                 cmd = [NVCC, "-x", "cu"] + ARCH + flags + ["-c", src, "-o", obj]
             else:

@@ -529,6 +529,22 @@ moao_status moao_ctx_set_lookahead(moao_ctx* c, int sms) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_accuracy(moao_ctx* c, double target) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_accuracy: null");
+  if (!(target >= 0.0)) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_accuracy: target >= 0");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->acc_target = target;
+  return MOAO_OK;
+}
+
+moao_status moao_ctx_set_wait_limit(moao_ctx* c, long long polls) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_wait_limit: null");
+  if (polls < 0) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_wait_limit: polls >= 0");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->wait_polls = (unsigned long long)polls;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_host_precision(moao_ctx* c, moao_prec prec) {
   if (!c || (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED))
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_precision: FP64 or MIXED");
@@ -560,6 +576,35 @@ moao_status moao_matcov_tile(moao_ctx* ctx, const moao_tomo* t, double* d_data, 
                        &ctx->launches);
 }
 
+namespace {
+
+// Copies, column panel by column panel (width w), the part of an nrows x ncols
+// column-major tile whose local row r and column c satisfy r >= c - d (d = the
+// tile's global row offset minus its global column offset): exactly the
+// elements a type-1 (lower) covariance tile writes and the lower factor
+// occupies. Each panel [c0, c1) is copied from its first such row down to the
+// last row, which includes, inside the panel, the elements above the boundary;
+// with corner_only only those first rows (the panel's diagonal block, where
+// the untouched elements lie) are copied.
+moao_status copy_lower_panels(double* dst, long ldd, const double* src, long lds, long nrows,
+                              long ncols, long d, bool corner_only, cudaMemcpyKind kind,
+                              cudaStream_t s) {
+  const long w = 512;
+  for (long c0 = 0; c0 < ncols; c0 += w) {
+    const long c1 = std::min(ncols, c0 + w);
+    const long r0 = std::max(0L, c0 - d);
+    if (r0 >= nrows) break;  // later panels start lower still
+    const long r1 = corner_only ? std::min(nrows, std::max(r0, c1 - d)) : nrows;
+    if (r1 <= r0) continue;
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(dst + c0 * ldd + r0, sizeof(double) * ldd,
+                                    src + c0 * lds + r0, sizeof(double) * lds,
+                                    sizeof(double) * (r1 - r0), c1 - c0, kind, s));
+  }
+  return MOAO_OK;
+}
+
+}  // namespace
+
 moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_data, int nrows,
                                   int ncols, int xoffset, int yoffset, int lda, int type_mat) {
   if (!ctx || !t || !h_data) return set_error(MOAO_ERR_BAD_ARG, "matcov_tile_host: null");
@@ -572,17 +617,26 @@ moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_d
   const size_t bytes = sizeof(double) * (size_t)nrows * ncols;
   MOAO_TRY(ctx->ws_tmp.ensure(bytes));
   double* d = ctx->ws_tmp.as<double>();
-  // Elements the reference leaves untouched (upper triangle of Cmm) must keep
-  // the caller's values, so the tile goes down and comes back.
-  MOAO_CUDA_TRY(cudaMemcpy2DAsync(d, sizeof(double) * nrows, h_data, sizeof(double) * lda,
-                                  sizeof(double) * nrows, ncols, cudaMemcpyHostToDevice,
-                                  ctx->stream));
-  MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, ctx->stream,
-                         &ctx->launches));
-  MOAO_CUDA_TRY(cudaMemcpy2DAsync(h_data, sizeof(double) * lda, d, sizeof(double) * nrows,
-                                  sizeof(double) * nrows, ncols, cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  cudaStream_t s = ctx->stream;
+  if (type_mat == 1) {
+    // A type-1 tile writes only elements on or below the global diagonal; the
+    // others keep the caller's values. Only the panels' diagonal blocks (where
+    // both kinds meet) go down, and only the written panels come back.
+    const long dd = (long)xoffset - yoffset;
+    MOAO_TRY(copy_lower_panels(d, nrows, h_data, lda, nrows, ncols, dd, true,
+                               cudaMemcpyHostToDevice, s));
+    MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, s,
+                           &ctx->launches));
+    MOAO_TRY(copy_lower_panels(h_data, lda, d, nrows, nrows, ncols, dd, false,
+                               cudaMemcpyDeviceToHost, s));
+  } else {
+    // every element of the tile is written (or the type is rejected)
+    MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, s,
+                           &ctx->launches));
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(h_data, sizeof(double) * lda, d, sizeof(double) * nrows,
+                                    sizeof(double) * nrows, ncols, cudaMemcpyDeviceToHost, s));
+  }
+  MOAO_CUDA_TRY(cudaStreamSynchronize(s));
   return MOAO_OK;
 }
 
@@ -593,35 +647,34 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
   if (!ctx || !Cmm || !Ctm) return set_error(MOAO_ERR_BAD_ARG, "reconstructor_host: null");
   if (nmeas <= 0 || nmeasts <= 0 || ngal <= 0 || ldCmm < nmeas || ldCtm < nmeasts)
     return set_error(MOAO_ERR_BAD_ARG, "reconstructor_host: bad sizes");
-  double *dC = nullptr, *dT = nullptr;
-  const size_t cb = sizeof(double) * (size_t)nmeas * nmeas;
   const size_t tspan = (size_t)nmeas * nmeasts * (ngal - 1) + (size_t)ldCtm * (nmeas - 1) + nmeasts;
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
-  if (cudaMalloc(&dC, cb) != cudaSuccess) return set_error(MOAO_ERR_OOM, "reconstructor_host: Cmm");
-  if (cudaMalloc(&dT, sizeof(double) * tspan) != cudaSuccess) {
-    cudaFree(dC);
-    return set_error(MOAO_ERR_OOM, "reconstructor_host: Ctm");
+  double *dC = nullptr, *dT = nullptr;
+  {
+    // device copies in the context's workspaces (kept for the next call)
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    MOAO_TRY(ctx->ws_tmp.ensure(sizeof(double) * (size_t)nmeas * nmeas));
+    MOAO_TRY(ctx->ws_host_t.ensure(sizeof(double) * tspan));
+    dC = ctx->ws_tmp.as<double>();
+    dT = ctx->ws_host_t.as<double>();
   }
-  moao_status st = MOAO_OK;
   cudaStream_t s = ctx->stream;
-  auto fail = [&](cudaError_t e) {
-    if (e != cudaSuccess) st = set_error(MOAO_ERR_CUDA, cudaGetErrorString(e));
-    return e != cudaSuccess;
-  };
-  if (!fail(cudaMemcpy2DAsync(dC, sizeof(double) * nmeas, Cmm, sizeof(double) * ldCmm,
-                              sizeof(double) * nmeas, nmeas, cudaMemcpyHostToDevice, s)) &&
-      !fail(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice, s))) {
-    st = moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, ctx->host_prec, rep);
-    // On a failed factorisation the reference has already overwritten Cmm
-    // (partially) and leaves Ctm alone; mirror that.
-    if (!fail(cudaMemcpy2DAsync(Cmm, sizeof(double) * ldCmm, dC, sizeof(double) * nmeas,
-                                sizeof(double) * nmeas, nmeas, cudaMemcpyDeviceToHost, s)) &&
-        st == MOAO_OK)
-      fail(cudaMemcpyAsync(Ctm, dT, sizeof(double) * tspan, cudaMemcpyDeviceToHost, s));
-    cudaStreamSynchronize(s);
-  }
-  cudaFree(dC);
-  cudaFree(dT);
+  // Only the lower triangle of Cmm is read and only its lower triangle becomes
+  // the factor: the column panels of the lower part go down and come back (the
+  // panels' diagonal blocks carry their upper elements unchanged both ways).
+  MOAO_TRY(copy_lower_panels(dC, nmeas, Cmm, ldCmm, nmeas, nmeas, 0, false,
+                             cudaMemcpyHostToDevice, s));
+  MOAO_CUDA_TRY(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice, s));
+  const moao_status st =
+      moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, ctx->host_prec, rep);
+  // On a failed factorisation the reference has already overwritten Cmm
+  // (partially) and leaves Ctm alone; mirror that.
+  if (st == MOAO_OK || st == MOAO_ERR_NOT_SPD)
+    MOAO_TRY(copy_lower_panels(Cmm, ldCmm, dC, nmeas, nmeas, nmeas, 0, false,
+                               cudaMemcpyDeviceToHost, s));
+  if (st == MOAO_OK)
+    MOAO_CUDA_TRY(cudaMemcpyAsync(Ctm, dT, sizeof(double) * tspan, cudaMemcpyDeviceToHost, s));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(s));
   return st;
 }
 
@@ -658,11 +711,11 @@ moao_status moao_cee_cvv_host(moao_ctx* ctx, long nmeas, long nmeasts, long nact
     }
   }
   if (st == MOAO_OK)
-    st = moao_cee_cvv(ctx, nmeas, nmeasts, nact, mats[0].d, std::max(1L, nmeas), mats[1].d,
-                      std::max(1L, nmeasts), mats[2].d, std::max(1L, nmeasts), mats[3].d,
-                      std::max(1L, nmeasts), mats[4].d, std::max(1L, nact), mats[5].d,
-                      std::max(1L, nmeasts), mats[6].d, std::max(1L, nact), mats[7].d,
-                      std::max(1L, nact));
+    st = moao_cee_cvv_prec(ctx, nmeas, nmeasts, nact, mats[0].d, std::max(1L, nmeas), mats[1].d,
+                           std::max(1L, nmeasts), mats[2].d, std::max(1L, nmeasts), mats[3].d,
+                           std::max(1L, nmeasts), mats[4].d, std::max(1L, nact), mats[5].d,
+                           std::max(1L, nmeasts), mats[6].d, std::max(1L, nact), mats[7].d,
+                           std::max(1L, nact), ctx->host_prec);
   if (st == MOAO_OK)
     for (auto& m : mats)
       if (m.out && m.m * m.n > 0 &&

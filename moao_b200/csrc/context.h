@@ -55,11 +55,13 @@ struct moao_ctx {
   bool graph_mode = false;  // mixed path under stream capture: no host waits or reads
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
-  moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp;
+  moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp, ws_host_t;
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
   moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv, mx_exps, mx_dsl;
+  // mixed Cee/Cvv chain: int8 slices of Ctm's rows (then of E's), their exponents
+  moao::DevBuf cx_qc, cx_ec;
   long mx_factored_n = -1;  // size of the factorisation held in mx_* (reuse across targets)
   // Block-constant offsets of Cmm known to the caller (moao_ctx_set_offsets):
   // the mixed path factors Cmm minus them and adds them back exactly.
@@ -71,6 +73,12 @@ struct moao_ctx {
   int max_refine = 1;        // refinement corrections per target
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this
   int final_residual = 0;    // evaluate the residual once more after the last correction
+  // polls of each bounded wait inside the tensor-core kernel (0: its default, 2^28);
+  // a wait that runs out makes the call return MOAO_ERR_TIMEOUT
+  unsigned long long wait_polls = 0;
+  // mixed reconstructor: estimated relative error of R above which the FP64
+  // path runs instead (0: no estimate, no fallback)
+  double acc_target = 0.0;
   cudaEvent_t ev[8] = {};
   // Mixed factorisation lookahead: the next diagonal block is factored on aux
   // (created on first use) while the trailing update leaves this many SMs free
@@ -91,10 +99,10 @@ struct moao_ctx {
 
   // Every workspace buffer of the context (not the geometry caches).
   std::vector<moao::DevBuf*> workspaces() {
-    return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
+    return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &ws_host_t, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
             &mx_w1, &mx_w2,   &mx_x,    &mx_r64, &mx_e64, &mx_qa,  &mx_qb,    &mx_ea,
             &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv, &mx_exps,
-            &mx_dsl};
+            &mx_dsl, &cx_qc, &cx_ec};
   }
   // Device bytes held by the workspaces and the geometry caches.
   size_t bytes_held() {
@@ -106,6 +114,8 @@ struct moao_ctx {
 };
 
 namespace moao {
+
+struct TcTensor;
 
 // Brackets the launches issued during its lifetime with events when the
 // context's kernel timing is on.
@@ -156,6 +166,19 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
 void release_batch_state(moao_ctx* ctx);
 // Writes the mixed factorisation's (FP32) factor into the lower triangle of Cmm.
 moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm);
+// C (FP64, M x N, ldc) += alpha * A B^T from int8 Ozaki slices of the rows of
+// A (ta[0..nsa), 128-row boxes) and of B (tb[0..nsb), 256-row boxes), K columns,
+// keeping the slice products p + q + 2 <= dmax (0-based p, q); erow / ecol are
+// the row exponents of A and B (see mixed.cpp). Accounted as family tc_int8.
+moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTensor* tb, int nsb,
+                       int dmax, long M, long N, long K, float alpha, double* C, long ldc,
+                       const int* erow, const int* ecol, int* err);
+// Cee and Cvv with the int8 tensor cores (cee_mixed.cpp); same arguments and
+// in-place contract as moao_cee_cvv except that Cpp is left as given.
+moao_status cee_cvv_mixed(moao_ctx* ctx, long nmeas, long nmeasts, long nact, const double* Cmm,
+                          long ldCmm, const double* Cpp, long ldCpp, double* Cpm, long ldCpm,
+                          const double* R, long ldR, const double* Dx, long ldDx, double* Cee,
+                          long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp);
 // R = B * L^-T * L^-1 in place on B (m x n, ldb) using the factor and dinv.
 moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, const double* dinv,
                             double* B, long ldb, long m);

@@ -94,7 +94,33 @@ struct KParams {
   double* C;
   long ldc;
   int triB;
+  // tile order (set by the launcher): bands of group_m row tiles; inside a band
+  // the column tiles in turn, the band's row tiles fastest
+  int tiles_m, tiles_n, group_m;
 };
+
+// Tile v of the launch in band order. Consecutive CTAs share one column strip
+// of B and the band's row strips of A stay in L2 while the band sweeps the
+// columns: the CTAs resident together touch group_m strips of A and a few of B
+// instead of every row strip of A (which, for a 1,024-wide panel of an
+// nmeas ~ 15k-48k factorisation, no longer fits in L2). For a lower C the sweep
+// of a band stops at the diagonal. Returns false past the last tile.
+template <int BM, int BN, bool LOWERC>
+__device__ __forceinline__ bool band_tile(const KParams& p, long v, long* m0, long* n0) {
+  for (int b0 = 0; b0 < p.tiles_m; b0 += p.group_m) {
+    const int rows = min(p.group_m, p.tiles_m - b0);
+    long cols = p.tiles_n;
+    if (LOWERC) cols = min((long)p.tiles_n, ((long)(b0 + rows) * BM - 1) / BN + 1);
+    const long cnt = rows * cols;
+    if (v < cnt) {
+      *m0 = (long)(b0 + (int)(v % rows)) * BM;
+      *n0 = (v / rows) * BN;
+      return true;
+    }
+    v -= cnt;
+  }
+  return false;
+}
 
 // Load one BK-slice of an MN-contiguous operand (A, or B when transB): the tile
 // rows r0..r0+R-1 of columns k0..k0+15 of a column-major rows x K matrix, stored
@@ -140,7 +166,8 @@ __global__ void __launch_bounds__(TL::NTHREADS) gemm_f64_kernel(const KParams p)
   double* As = smem;
   double* Bs = smem + STAGES * A_STAGE;
 
-  const long m0 = (long)blockIdx.x * BM, n0 = (long)blockIdx.y * BN;
+  long m0 = 0, n0 = 0;
+  if (!band_tile<BM, BN, LOWERC>(p, blockIdx.x, &m0, &n0)) return;
   if (LOWERC && m0 + BM <= n0) return;  // tile strictly above the diagonal
 
   // K range (tile aligned); a triangular B limits it.
@@ -286,8 +313,20 @@ moao_status launch_gemm_t(const KParams& p, cudaStream_t s) {
   static std::atomic<unsigned long long> configured{0};
   auto kern = gemm_f64_kernel<TL, TRANSB, LOWERC, VEC, MMA16>;
   MOAO_CUDA_TRY(set_smem_limit(kern, (int)TL::SMEM_BYTES, configured));
-  dim3 grid((unsigned)((p.M + TL::BM - 1) / TL::BM), (unsigned)((p.N + TL::BN - 1) / TL::BN));
-  kern<<<grid, TL::NTHREADS, TL::SMEM_BYTES, s>>>(p);
+  KParams q = p;
+  q.tiles_m = (int)((p.M + TL::BM - 1) / TL::BM);
+  q.tiles_n = (int)((p.N + TL::BN - 1) / TL::BN);
+  q.group_m = std::max(1, 4096 / TL::BM);  // bands of 4,096 rows
+  long total = 0;
+  for (int b0 = 0; b0 < q.tiles_m; b0 += q.group_m) {
+    const int rows = std::min(q.group_m, q.tiles_m - b0);
+    long cols = q.tiles_n;
+    if (LOWERC) cols = std::min((long)q.tiles_n, ((long)(b0 + rows) * TL::BM - 1) / TL::BN + 1);
+    total += rows * cols;
+  }
+  if (total <= 0) return MOAO_OK;
+  if (total > 0x7fffffffL) return set_error(MOAO_ERR_BAD_ARG, "gemm: too many tiles");
+  kern<<<(unsigned)total, TL::NTHREADS, TL::SMEM_BYTES, s>>>(q);
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
 }

@@ -61,6 +61,13 @@ __global__ void sumsq_kernel(const double* __restrict__ A, long lda, long m, lon
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
+// A (m x n, ld m) += B (m x n, ld m).
+__global__ void add_f64_kernel(double* __restrict__ A, const double* __restrict__ B, long total) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x)
+    A[e] += B[e];
+}
+
 moao_status sumsq(moao_ctx* ctx, const double* A, long lda, long m, long n, double* d_out,
                   double* h_out) {
   MOAO_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double), ctx->stream));
@@ -108,6 +115,7 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
                       const int* ecol = nullptr, int max_ctas = 0) {
   TcGemm g;
   g.max_ctas = max_ctas;
+  g.spin_limit = ctx->wait_polls;
   g.kind = A[0].kind;
   g.erow = erow;
   g.ecol = ecol;
@@ -187,6 +195,7 @@ moao_status block_product(moao_ctx* ctx, const Scales& sc, const TcTensor* A, co
                           int slices, int* err) {
   MOAO_TRY(split_block(sc, W, ldw, m, kb, slices, xr, ldx, ctx->stream));
   TcGemm g;
+  g.spin_limit = ctx->wait_polls;
   g.kind = A[0].kind;
   g.epi = kTcEpiF32;
   g.M = m;
@@ -270,6 +279,53 @@ moao_status mixed_solve(moao_ctx* ctx, long n, long m, float* T32, const double*
 }
 
 }  // namespace
+
+// C (FP64, M x N, ldc) += alpha * A B^T from int8 slices (Ozaki splitting):
+// ta[0..nsa) hold the slices of A's rows (128-row boxes), tb[0..nsb) those of
+// B's rows (256-row boxes), K columns each, slice s of a row with exponent e
+// holding digits of x * 2^(6 - e) * 128^s. The products of slices p and q
+// (0-based) with p + q + 2 <= dmax are accumulated exactly in int32 on the
+// tensor cores and added in FP64 scaled by 2^(erow[r] + ecol[c] - 12 -
+// 7 (p + q)): one launch per anti-diagonal p + q, split where the int32 sum
+// could overflow (|digit| <= 64, so 4096 K per product).
+moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTensor* tb, int nsb,
+                       int dmax, long M, long N, long K, float alpha, double* C, long ldc,
+                       const int* erow, const int* ecol, int* err) {
+  if (nsa < 1 || nsa > kMaxOzakiSlices || nsb < 1 || nsb > kMaxOzakiSlices)
+    return set_error(MOAO_ERR_BAD_ARG, "ozaki_gemm: slice counts");
+  const long pair_cap = std::min<long>(
+      kTcMaxSegs, std::max(1L, (long)(2147483647.0 / (4096.0 * (double)std::max(K, 1L)))));
+  for (int d = 2; d <= dmax; ++d) {
+    std::vector<std::pair<int, int>> pairs;
+    for (int p = 1; p <= nsa; ++p)
+      if (d - p >= 1 && d - p <= nsb) pairs.push_back({p - 1, d - p - 1});
+    for (size_t b0 = 0; b0 < pairs.size(); b0 += pair_cap) {
+      TcGemm g;
+      g.spin_limit = ctx->wait_polls;
+      g.kind = kTcI8;
+      g.epi = kTcEpiF64Scaled;
+      g.M = M;
+      g.N = N;
+      for (int i = 0; i < nsa; ++i) g.A[i] = &ta[i];
+      for (int i = 0; i < nsb; ++i) g.B[i] = &tb[i];
+      g.nA = nsa;
+      g.nB = nsb;
+      const size_t b1 = std::min(pairs.size(), b0 + (size_t)pair_cap);
+      for (size_t q = b0; q < b1; ++q)
+        g.seg[g.nseg++] = TcSegment{pairs[q].first, pairs[q].second, 0, 0, (int)((K + 127) / 128), 0};
+      g.alpha = alpha;
+      g.C = C;
+      g.ldc = ldc;
+      g.erow = erow;
+      g.ecol = ecol;
+      g.shift = -12 - 7 * (d - 2);
+      g.err = err;
+      KernelTimer kt(ctx, "tc_int8", 2.0 * M * (double)N * K * (double)(b1 - b0));
+      MOAO_TRY(tc_gemm(g, ctx->stream, &ctx->launches));
+    }
+  }
+  return MOAO_OK;
+}
 
 MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
   const long ldn = round_up(n, 64), ldq = round_up(n, 128);
@@ -569,37 +625,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
                                     m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
     MOAO_TRY(ozaki_split_rows(R64, m, m, n, ns, ea, qa, ldq, s));
-    const long pair_cap = std::max(1L, (long)(2147483647.0 / (4096.0 * (double)n)));
-    for (int d = 2; d <= ns + 1; ++d) {
-      std::vector<std::pair<int, int>> pairs;
-      for (int p = 1; p <= ns; ++p)
-        if (d - p >= 1 && d - p <= ns) pairs.push_back({p - 1, d - p - 1});
-      for (size_t b0 = 0; b0 < pairs.size(); b0 += pair_cap) {
-        TcGemm g;
-        g.kind = kTcI8;
-        g.epi = kTcEpiF64Scaled;
-        g.M = m;
-        g.N = n;
-        for (int i = 0; i < ns; ++i) {
-          g.A[i] = &ta[i];
-          g.B[i] = &tb[i];
-        }
-        g.nA = g.nB = ns;
-        const size_t b1 = std::min(pairs.size(), b0 + (size_t)pair_cap);
-        for (size_t q = b0; q < b1; ++q)
-          g.seg[g.nseg++] = TcSegment{pairs[q].first, pairs[q].second, 0, 0,
-                                      (int)((n + 127) / 128), 0};
-        g.alpha = -1.f;
-        g.C = E64;
-        g.ldc = m;
-        g.erow = ea;
-        g.ecol = fb;
-        g.shift = -12 - 7 * (d - 2);
-        g.err = err;
-        KernelTimer kt(ctx, "tc_int8", 2.0 * m * (double)n * n * (double)(b1 - b0));
-        MOAO_TRY(tc_gemm(g, s, &ctx->launches));
-      }
-    }
+    MOAO_TRY(ozaki_gemm(ctx, ta, ns, tb, ns, ns + 1, m, n, n, -1.f, E64, m, ea, fb, err));
     if (nro > 0) {  // the offsets' part of R Cmm
       MOAO_TRY(range_sums(R64, m, m, off, ZU, s));
       MOAO_TRY(subtract_offset_products(E64, m, m, n, ZU, rid, off, s));
@@ -610,21 +636,59 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
     }
     return MOAO_OK;
   };
+  // Accuracy guard (ctx->acc_target > 0, not under capture): the error of the
+  // returned R is estimated as ||dR|| / ||R|| of the last correction (the error
+  // of R before it) times the residual's reduction by that correction, which
+  // needs the residual once more at the end. A miss is reported in
+  // rep->fallback and R is not written: the caller runs the FP64 path.
+  const bool guard = ctx->acc_target > 0 && !graph;
+  double r_before = -1.0, dr2 = 0.0;
   int steps = 0;
   for (; steps < ctx->max_refine; ++steps) {
     MOAO_TRY(residual());
     if (!graph && rep->refine_resid <= ctx->refine_tol) break;
+    r_before = rep->refine_resid;
     MOAO_TRY(cvt_f64_to_f32(E64, m, T32, m, m, n, false, s));
     MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, corr, csl, err, sc));
-    if (nro > 0) {
+    if (guard) {
+      // the correction in FP64 in E64 (free until the next residual), its norm, R += it
+      if (nro > 0) {
+        MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
+        MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, E64, m, false, s));
+      } else {
+        MOAO_TRY(cvt_f32_to_f64(T32, m, E64, m, m, n, false, s));
+      }
+      MOAO_TRY(sumsq(ctx, E64, m, m, n, dnorm, &dr2));
+      add_f64_kernel<<<148 * 8, 256, 0, s>>>(R64, E64, m * n);
+      ++ctx->launches;
+      MOAO_CUDA_TRY(cudaGetLastError());
+    } else if (nro > 0) {
       MOAO_TRY(range_sums(T32, m, m, off, ZU, s));
       MOAO_TRY(woodbury_apply(T32, m, m, n, ZU, nro, Y2, R64, m, true, s));
     } else {
       MOAO_TRY(add_f32_to_f64(T32, m, R64, m, m, n, s));
     }
   }
-  if (ctx->final_residual && !graph) MOAO_TRY(residual());
+  if ((ctx->final_residual || guard) && !graph) MOAO_TRY(residual());
   rep->refine_steps = steps;
+  if (guard) {
+    double r2 = 0.0;
+    MOAO_TRY(sumsq(ctx, R64, m, m, n, dnorm, &r2));
+    double est;
+    if (r_before < 0)  // no correction ran (the first residual met the tolerance)
+      est = rep->refine_resid;
+    else
+      est = std::sqrt(dr2 / std::max(r2, 1e-300)) * (rep->refine_resid / std::max(r_before, 1e-300));
+    rep->est_error = std::max(rep->est_error, est);
+    if (!(est <= ctx->acc_target)) {
+      rep->fallback = 1;
+      int herr[2] = {0, 0};
+      MOAO_CUDA_TRY(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+      if (herr[0]) return set_error(MOAO_ERR_TIMEOUT, "tensor-core kernel: bounded wait expired");
+      return MOAO_OK;  // Ctm and Cmm untouched
+    }
+  }
   // ---- outputs: R in FP64, the FP32 factor into the lower triangle of Cmm
   MOAO_CUDA_TRY(cudaMemcpy2DAsync(Ctm, ldCtm * sizeof(double), R64, m * sizeof(double),
                                   m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));

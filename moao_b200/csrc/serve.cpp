@@ -198,13 +198,15 @@ moao_status run_request(moao_server* s, Slot& slot, Request& q, moao_solve_repor
     double* Tmp = slot.tmp.as<double>();
     MOAO_CUDA_TRY(cudaMemcpyAsync(slot.dx.as<double>(), sys.Dx.data(), bytes_of(a, m),
                                   cudaMemcpyHostToDevice, cs));
-    if (!mixed) MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), Cmm, (int)n, (int)n, 0, 0, (int)n, 1));
+    // the FP64 path (or a mixed request that fell back to it) left the factor in Cmm
+    if (!mixed || rep->fallback)
+      MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), Cmm, (int)n, (int)n, 0, 0, (int)n, 1));
     MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), Ctm2, (int)m, (int)n, 0, 0, (int)m, 3));
     MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), slot.ctt.as<double>(), (int)m, (int)m, 0, 0,
                               (int)m, 4));
-    MOAO_TRY(moao_cee_cvv(ctx, n, m, a, Cmm, n, slot.ctt.as<double>(), m, Ctm2, m, Ctm, m,
-                          slot.dx.as<double>(), a, slot.cee.as<double>(), m,
-                          slot.cvv.as<double>(), a, Tmp, a));
+    MOAO_TRY(moao_cee_cvv_prec(ctx, n, m, a, Cmm, n, slot.ctt.as<double>(), m, Ctm2, m, Ctm, m,
+                               slot.dx.as<double>(), a, slot.cee.as<double>(), m,
+                               slot.cvv.as<double>(), a, Tmp, a, q.r.prec));
     if (q.r.Cvv)
       MOAO_CUDA_TRY(cudaMemcpyAsync(q.r.Cvv, slot.cvv.as<double>(), bytes_of(a, a),
                                     cudaMemcpyDeviceToHost, cs));

@@ -114,6 +114,41 @@ moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, co
   return MOAO_OK;
 }
 
+// FP64 reconstructor: factor Cmm in place, then the solves of targets g0..ngal-1.
+moao_status reconstructor_fp64(moao_ctx* ctx, long nmeas, long nmeasts, double* d_Cmm, long ldCmm,
+                               double* d_Ctm, long ldCtm, long g0, long ngal,
+                               moao_solve_report* r) {
+  MOAO_TRY(ctx->ws_dinv.ensure(sizeof(double) * (size_t)nmeas * ctx->nb));
+  MOAO_TRY(ctx->ws_info.ensure(sizeof(int)));
+  int* d_info = ctx->ws_info.as<int>();
+  MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  MOAO_TRY(potrf_f64(ctx, d_Cmm, ldCmm, nmeas, ctx->ws_dinv.as<double>(), d_info));
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  int info = 0;
+  MOAO_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  r->info = info;
+  if (info != 0) {
+    // The reference prints and returns without solving (reconstructor.cpp:34-38).
+    return set_error(MOAO_ERR_NOT_SPD, "dpotrf: non-positive pivot at column " +
+                                           std::to_string(info));
+  }
+  for (long g = g0; g < ngal; ++g) {
+    double* Ctm_g = d_Ctm + nmeas * nmeasts * g;
+    MOAO_TRY(solve_right_f64(ctx, d_Cmm, ldCmm, nmeas, ctx->ws_dinv.as<double>(), Ctm_g, ldCtm,
+                             nmeasts));
+  }
+  cudaEventRecord(ctx->ev[2], ctx->stream);
+  MOAO_CUDA_TRY(cudaEventSynchronize(ctx->ev[2]));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+  r->ms_factor += ms;
+  cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+  r->ms_solve += ms;
+  return MOAO_OK;
+}
+
 }  // namespace moao
 
 using namespace moao;
@@ -134,54 +169,43 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
   std::memset(r, 0, sizeof(*r));
   if (nmeas == 0) return MOAO_OK;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   if (prec == MOAO_PREC_MIXED) {
-    MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
-    for (long g = 0; g < ngal; ++g) {
+    long g = 0;
+    for (; g < ngal; ++g) {
       // one factorisation serves every target: later targets reuse it
       MOAO_TRY(reconstructor_mixed(ctx, nmeas, nmeasts, d_Cmm, ldCmm,
                                    d_Ctm + nmeas * nmeasts * g, ldCtm, g > 0, r));
+      if (r->fallback) break;
+    }
+    if (r->fallback) {
+      // the mixed estimate missed the accuracy target: this and the remaining
+      // targets from the FP64 path (Cmm and their Ctm are still as given)
+      ctx->mx_factored_n = -1;
+      return reconstructor_fp64(ctx, nmeas, nmeasts, d_Cmm, ldCmm, d_Ctm, ldCtm, g, ngal, r);
     }
     if (!ctx->keep_cmm) MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
     MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return MOAO_OK;
   }
-  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
-  MOAO_TRY(ctx->ws_dinv.ensure(sizeof(double) * (size_t)nmeas * ctx->nb));
-  MOAO_TRY(ctx->ws_info.ensure(sizeof(int)));
-  int* d_info = ctx->ws_info.as<int>();
-  MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
-  cudaEventRecord(ctx->ev[0], ctx->stream);
-  MOAO_TRY(potrf_f64(ctx, d_Cmm, ldCmm, nmeas, ctx->ws_dinv.as<double>(), d_info));
-  cudaEventRecord(ctx->ev[1], ctx->stream);
-  int info = 0;
-  MOAO_CUDA_TRY(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  r->info = info;
-  if (info != 0) {
-    // The reference prints and returns without solving (reconstructor.cpp:34-38).
-    return set_error(MOAO_ERR_NOT_SPD, "dpotrf: non-positive pivot at column " +
-                                           std::to_string(info));
-  }
-  for (long g = 0; g < ngal; ++g) {
-    double* Ctm_g = d_Ctm + nmeas * nmeasts * g;
-    MOAO_TRY(solve_right_f64(ctx, d_Cmm, ldCmm, nmeas, ctx->ws_dinv.as<double>(), Ctm_g, ldCtm,
-                             nmeasts));
-  }
-  cudaEventRecord(ctx->ev[2], ctx->stream);
-  MOAO_CUDA_TRY(cudaEventSynchronize(ctx->ev[2]));
-  float ms = 0;
-  cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
-  r->ms_factor = ms;
-  cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
-  r->ms_solve = ms;
-  return MOAO_OK;
+  return reconstructor_fp64(ctx, nmeas, nmeasts, d_Cmm, ldCmm, d_Ctm, ldCtm, 0, ngal, r);
 }
 
 moao_status moao_cee_cvv(moao_ctx* ctx, long nmeas, long nmeasts, long nact, double* Cmm,
                          long ldCmm, double* Cpp, long ldCpp, double* Cpm, long ldCpm, double* R,
                          long ldR, double* Dx, long ldDx, double* Cee, long ldCee, double* Cvv,
                          long ldCvv, double* Tmp, long ldTmp) {
+  return moao_cee_cvv_prec(ctx, nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR,
+                           Dx, ldDx, Cee, ldCee, Cvv, ldCvv, Tmp, ldTmp, MOAO_PREC_FP64);
+}
+
+moao_status moao_cee_cvv_prec(moao_ctx* ctx, long nmeas, long nmeasts, long nact, double* Cmm,
+                              long ldCmm, double* Cpp, long ldCpp, double* Cpm, long ldCpm,
+                              double* R, long ldR, double* Dx, long ldDx, double* Cee, long ldCee,
+                              double* Cvv, long ldCvv, double* Tmp, long ldTmp, moao_prec prec) {
   if (!ctx) return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv: null context");
+  if (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED)
+    return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv: unknown precision");
   if (nmeas < 0 || nmeasts < 0 || nact < 0)
     return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv: negative size");
   if (ldCmm < std::max(1L, nmeas) || ldCpp < std::max(1L, nmeasts) ||
@@ -189,8 +213,14 @@ moao_status moao_cee_cvv(moao_ctx* ctx, long nmeas, long nmeasts, long nact, dou
       ldDx < std::max(1L, nact) || ldCee < std::max(1L, nmeasts) ||
       ldCvv < std::max(1L, nact) || ldTmp < std::max(1L, nact))
     return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv: leading dimension too small");
+  if ((nmeas > 0 && (!Cmm || !R)) || (nmeasts > 0 && (!Cpp || !Cpm || !Cee)) ||
+      (nact > 0 && (!Dx || !Cvv || !Tmp)))
+    return set_error(MOAO_ERR_BAD_ARG, "Cee_Cvv: null matrix pointer");
   std::lock_guard<std::mutex> lk(ctx->mu);
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  if (prec == MOAO_PREC_MIXED)
+    return cee_cvv_mixed(ctx, nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx,
+                         ldDx, Cee, ldCee, Cvv, ldCvv, Tmp, ldTmp);
   const long nm = nmeas, nt = nmeasts;
   // (1) Cpp <- Cpp - Cpm R^T - R Cpm^T  (syr2k, lower)
   MOAO_TRY(gemm(ctx, nt, nt, nm, -1.0, Cpm, ldCpm, R, ldR, true, 1.0, Cpp, ldCpp, true));

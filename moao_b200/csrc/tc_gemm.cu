@@ -49,7 +49,7 @@ constexpr int STAGE_C = 32 * 32 * 4;    // per epilogue warp: one 32x32 FP32 chu
 constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ +
                        EPI_WARPS * 32 * sizeof(float) /*per-warp column scales*/ +
                        (size_t)EPI_WARPS * STAGE_C /*per-warp C staging*/;
-constexpr unsigned long long kSpinLimit = 1ull << 28;
+constexpr unsigned long long kSpinLimit = 1ull << 28;  // default polls of a bounded wait
 
 struct __align__(64) TcParams {
   CUtensorMap mapA[kTcMaxMaps];
@@ -73,6 +73,7 @@ struct __align__(64) TcParams {
   int tiles_m, tiles_n;
   int total_tiles;         // tiles that intersect the written part of C
   int* err;
+  unsigned long long spin_limit;  // polls of a role's bounded wait before it gives up
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -104,9 +105,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; returns false (and records code) if the phase never completes.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-  for (unsigned long long i = 0; i < kSpinLimit; ++i) {
+// Bounded wait; returns false (and records code) if the phase does not
+// complete within limit polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                          unsigned long long limit) {
+  for (unsigned long long i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 1023) == 1023 && *(volatile int*)err) return false;  // another role gave up
   }
@@ -218,7 +221,8 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
   uint64_t* empty_bar = full_bar + STAGES;
   uint64_t* tfull_bar = empty_bar + STAGES;  // [2]
   uint64_t* tempty_bar = tfull_bar + 2;      // [2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
+  uint64_t* drain_bar = tempty_bar + 2;      // the issuer's last commit (every MMA done)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
   // per epilogue warp: 2^ecol of the 32 columns of its current chunk, and a
   // 32x32 FP32 staging chunk for the TMA reduce-add of C
   float* col_scale = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES + 256);
@@ -235,6 +239,7 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
       mbar_init(&tfull_bar[b], 1);
       mbar_init(&tempty_bar[b], EPI_WARPS);
     }
+    mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 2) {
@@ -263,7 +268,7 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
         for (int kb = 0; kb < sg.nk; ++kb, ++it) {
           const int st = it % STAGES;
           const uint32_t use = it / STAGES;
-          if (use > 0 && !mbar_wait(&empty_bar[st], (use - 1) & 1, p.err, 1)) {
+          if (use > 0 && !mbar_wait(&empty_bar[st], (use - 1) & 1, p.err, 1, p.spin_limit)) {
             ok = false;
             break;
           }
@@ -291,12 +296,12 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
     for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x, ++tc) {
       const int buf = tc & 1;
       const uint32_t use = tc >> 1;
-      if (use > 0 && !mbar_wait(&tempty_bar[buf], (use - 1) & 1, p.err, 4)) break;
+      if (use > 0 && !mbar_wait(&tempty_bar[buf], (use - 1) & 1, p.err, 4, p.spin_limit)) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const uint32_t acc = tmem + (uint32_t)(buf * ACC_COLS);
       for (int k = 0; k < kblocks; ++k, ++it) {
         const int st = it % STAGES;
-        if (!mbar_wait(&full_bar[st], (it / STAGES) & 1, p.err, 2)) {
+        if (!mbar_wait(&full_bar[st], (it / STAGES) & 1, p.err, 2, p.spin_limit)) {
           ok = false;
           break;
         }
@@ -312,7 +317,13 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
         }
         mma_commit(&empty_bar[st]);
       }
+      if (!ok) break;  // this tile's accumulator is incomplete: never hand it on
       mma_commit(&tfull_bar[buf]);
+    }
+    // Every MMA this thread issued has finished writing TMEM before the CTA
+    // frees it, also when a wait gave up in the middle of a tile.
+    mma_commit(drain_bar);
+    for (unsigned long long i = 0; i < kSpinLimit && !mbar_try_wait(drain_bar, 0); ++i) {
     }
   } else if (warp >= 4) {
     // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4).. and one
@@ -326,7 +337,7 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
       const int m0 = mt * TBM, n0 = nt * TBN;
       const int buf = tc & 1;
       // every lane waits; the warp leaves together if any lane gave up
-      const bool got = mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3);
+      const bool got = mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3, p.spin_limit);
       if (!__all_sync(0xffffffffu, got)) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const int r = m0 + q * 32 + lane;
@@ -540,6 +551,7 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   p.ecol = g.ecol;
   p.shift = g.shift;
   p.err = g.err;
+  p.spin_limit = g.spin_limit > 0 ? g.spin_limit : kSpinLimit;
   p.tiles_m = (int)((g.M + TBM - 1) / TBM);
   p.tiles_n = (int)((g.N + TBN - 1) / TBN);
   long total = 0;

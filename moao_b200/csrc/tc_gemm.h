@@ -54,6 +54,7 @@ struct TcGemm {
   int shift = 0;
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
   int max_ctas = 0;            // cap on the persistent grid (0: one CTA per SM)
+  unsigned long long spin_limit = 0;  // polls of each bounded wait (0: 2^28)
 };
 
 // Describes a row-major (K-contiguous) device matrix for TMA. The output tile is

@@ -84,8 +84,88 @@ T magnitude_from_flux(T qr, T F, T throughput, T d, T t, T bdw) {
 }  // namespace
 
 // ============================================================================
+// Value lines of a positional parameter file (one comment line before each).
+static long value_lines(const std::string& path) {
+  std::ifstream in(path);
+  if (!in.is_open()) throw std::runtime_error("Could not open file '" + path + "'!");
+  long n = 0;
+  std::string line;
+  while (std::getline(in, line)) ++n;
+  return n / 2;
+}
+
 template <typename T>
 void SysParams<T>::read(const std::string& sf) {
+  if (value_lines(sf) <= 24) {
+    // Legacy benchmark layout (datafile/benchmark/*/sys-params.txt of the
+    // reference, read by its PLASMA-era driver): 22 fields in another order
+    // and a uniform noise variance instead of the photometry. The fields it
+    // does not carry take the defaults of SysParams' constructor
+    // (common/tomo_struct/sysParams.cpp:53-104), one target on axis.
+    LineReader r(sf);
+    r.scalar(diam, "diam");
+    r.scalar(obs, "obs");
+    r.scalar(nW, "nW");
+    r.scalar(nssp, "Nssp");
+    r.vec(gsAlt, "gsAlt");
+    r.vec(gsType, "type");
+    r.scalar(nLgs, "nLgs");
+    r.vec(alphaX_as, "alphaX_as");
+    r.vec(alphaY_as, "alphaY_as");
+    r.vec(XPup, "XPup");
+    r.vec(YPup, "YPup");
+    r.vec(thetaML, "thetaML");
+    r.vec(thetaCam, "thetaCam");
+    r.vec(sensibilite, "sensibilite");
+    r.vec(tracking, "tracking");
+    r.scalar(pasDphi, "pasDphi");
+    r.scalar(ncpu, "ncpu");
+    r.scalar(lgsCst, "lgs_cst");
+    r.scalar(noiseVar, "noise_var");
+    r.scalar(spotWidth, "spot_width");
+    r.scalar(lgsAlt, "lgs_alt");
+    r.scalar(lgsDepth, "lgs_depth");
+    legacy = 1;
+    tFrame = 0.004;
+    nTarget = 1;
+    lgsFlux = 1.e7;
+    ngsPixSize = 0.3;
+    lgsPixSize = 1.0;
+    lambdaNGS = 6.5e-07;
+    lambdaLGS = 5.89e-07;
+    bdw_m = 3.3e-07;
+    throughNGS = 0.425;
+    throughLGS = 0.382;
+    throughAtm = 0.84;
+    RON = 3;
+    targetX_as.assign(1, 0);
+    targetY_as.assign(1, 0);
+    if (nW < 2 || nLgs < 0 || nLgs > nW - 1 || nssp < 1 || diam <= 0 || noiseVar < 0)
+      throw std::runtime_error("invalid system sizes in '" + sf + "'");
+    mrNGS.assign(nW - nLgs, 0.0);
+  } else {
+    read_current(sf);
+  }
+  nNgs = nW - nLgs - 1;
+  need(gsAlt, nW, "gsAlt");
+  need(gsType, nW, "type");
+  need(alphaX_as, nW, "alphaX_as");
+  need(alphaY_as, nW, "alphaY_as");
+  need(XPup, nW, "XPup");
+  need(YPup, nW, "YPup");
+  need(thetaML, nW, "thetaML");
+  need(thetaCam, nW, "thetaCam");
+  need(sensibilite, nW, "sensibilite");
+  need(tracking, 3, "tracking");
+  need(mrNGS, nW - nLgs, "mrNGS");
+  need(targetX_as, nTarget, "targetX_as");
+  need(targetY_as, nTarget, "targetY_as");
+}
+
+template <typename T>
+void SysParams<T>::read_current(const std::string& sf) {
+  legacy = 0;
+  noiseVar = 0;
   LineReader r(sf);
   r.scalar(diam, "diam");
   r.scalar(obs, "obs");
@@ -125,20 +205,6 @@ void SysParams<T>::read(const std::string& sf) {
   r.vec(targetY_as, "targetY_as");
   if (nW < 2 || nLgs < 0 || nLgs > nW - 1 || nssp < 1 || nTarget < 1 || diam <= 0)
     throw std::runtime_error("invalid system sizes in '" + sf + "'");
-  nNgs = nW - nLgs - 1;
-  need(gsAlt, nW, "gsAlt");
-  need(gsType, nW, "type");
-  need(alphaX_as, nW, "alphaX_as");
-  need(alphaY_as, nW, "alphaY_as");
-  need(XPup, nW, "XPup");
-  need(YPup, nW, "YPup");
-  need(thetaML, nW, "thetaML");
-  need(thetaCam, nW, "thetaCam");
-  need(sensibilite, nW, "sensibilite");
-  need(tracking, 3, "tracking");
-  need(mrNGS, nW - nLgs, "mrNGS");
-  need(targetX_as, nTarget, "targetX_as");
-  need(targetY_as, nTarget, "targetY_as");
 }
 
 template <typename T>
@@ -405,6 +471,28 @@ void Tomo_struct<T>::updateNoise() {
   noiseLGSxy.assign(Nx, 0);
   updateSeeing();
   int k = 0;
+  if (sys.legacy) {
+    // Legacy noise model of the benchmark files (the PLASMA-era covariance
+    // kernels of the reference, plasma/matcov_gpu/matcov_gpu_gb.cu:1265-1297):
+    // every NGS slope has variance noise_var; an LGS slope has noise_var across
+    // its spot elongation and noise_var (ext^2 + w^2) / w^2 along it (w the spot
+    // width, ext the elongation).
+    const T v = sys.noiseVar, w2 = sys.spotWidth * sys.spotWidth;
+    for (int i = 0; i < sys.nW; ++i) {
+      if (i < sys.nLgs) {
+        for (long j = 0; j < Nsubap[i]; ++j, ++k) {
+          const T longAxis = v * (lgsExt[k] * lgsExt[k] + w2) / w2;
+          const T c = std::cos(lgsTheta[k]), s = std::sin(lgsTheta[k]);
+          noiseLGSxx[k] = longAxis * c * c + v * s * s;
+          noiseLGSyy[k] = longAxis * s * s + v * c * c;
+          noiseLGSxy[k] = (longAxis - v) * s * c;
+        }
+      } else {
+        noiseNGS[i - sys.nLgs] = v;
+      }
+    }
+    return;
+  }
   for (int i = 0; i < sys.nW; ++i) {
     const T d = (sys.diam / Nssp[i]);
     const T F = flux<T>(qr, mr[i], throughput[i], d, sys.tFrame, bdw);

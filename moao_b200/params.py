@@ -168,6 +168,26 @@ def write_system(directory: str, sysp: SysParams, atm: AtmParams,
     return directory
 
 
+LEGACY_FIELDS = ["diam", "obs", "nW", "Nssp", "gsAlt", "type", "nLgs", "alphaX_as", "alphaY_as",
+                 "XPup", "YPup", "thetaML", "thetaCam", "sensibilite", "tracking", "pasDphi", "ncpu",
+                 "lgs_cst", "noise_var", "spot_width", "lgs_alt", "lgs_depth"]
+
+
+def write_legacy_sys(values, path: str) -> None:
+    """A sys-params.txt in the legacy benchmark layout (the 22 fields of
+    LEGACY_FIELDS in that order, one comment line before each value line), as
+    in the reference's datafile/benchmark directory."""
+    if len(values) != len(LEGACY_FIELDS):
+        raise ValueError("legacy layout: 22 value lines")
+    ints = {"nW", "Nssp", "type", "nLgs", "ncpu"}
+    vectors = {"gsAlt", "type", "alphaX_as", "alphaY_as", "XPup", "YPup", "thetaML", "thetaCam",
+               "sensibilite", "tracking"}
+    with open(path, "w") as f:
+        for name, v in zip(LEGACY_FIELDS, values):
+            v = [int(x) if name in ints else float(x) for x in v]
+            f.write(name + "\n" + _fmt(v if name in vectors else v[0]) + "\n")
+
+
 def _ring(n: int, radius: float):
     a = 2.0 * math.pi / n
     return ([radius * math.cos(i * a) for i in range(n)],

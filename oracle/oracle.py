@@ -19,10 +19,17 @@ does. Pieces:
 * ``intersample``     common/tomo_struct/intersample.cpp:74-170 in numpy; the
                       unnormalised FFTW r2c/c2r become numpy FFTs times N^2.
 * ``compare_matrices`` common/compute/check_utils.cpp:20-58.
+* ``RefDense``        the reference's own MOAO_LAPACK::reconstructor / Cee_Cvv and
+                      intersample_prepare/_init/_process/_free, compiled
+                      unchanged (oracle/_ref/libmoao_ref_dense.so) against
+                      oracle/shim/: CBLAS/LAPACKE from scipy's OpenBLAS, FFTW's
+                      2-D real transforms and cfitsio's image reads supplied by
+                      oracle/ref_dense_shim.cpp. tests/test_oracle.py pins
+                      ``reconstructor``, ``cee_cvv`` and ``intersample`` to it.
 
-The LAPACK steps have no golden vectors in the reference tree (its golden FITS
-files are not distributed with it); they are pinned by LAPACK's semantics and
-by the identities tested in tests/test_oracle.py.
+The reference tree has no golden vectors for the LAPACK and PSF steps (its
+golden FITS files are not distributed with it); those steps are pinned by
+running the reference's own code (RefDense) on the same inputs.
 """
 from __future__ import annotations
 
@@ -37,6 +44,7 @@ import scipy.linalg.lapack as lapack
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmoao_ref.so")
+REF_DENSE_LIB = os.path.join(HERE, "_ref", "libmoao_ref_dense.so")
 
 _TABLES = ["Nsubap", "Nssp", "u", "v", "sspSizeL", "L0diff", "cn2", "X", "Y", "noiseNGS",
            "noiseLGSxx", "noiseLGSyy", "noiseLGSxy"]
@@ -181,6 +189,71 @@ class RefTomo:
         self.lib().ref_matcov_tiled_mt(self.h, out.ctypes.data, nrows, ncols, nrows, type_mat, ts,
                                        nthreads)
         return out
+
+
+# ---------------------------------------------------------------- reference dense code
+class RefDense:
+    """The reference's lapack/compute and intersample code (oracle/_ref)."""
+    _lib = None
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(REF_DENSE_LIB)
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            L = C.CDLL(REF_DENSE_LIB)
+            L.ref_reconstructor.argtypes = [C.c_long, C.c_long, C.c_void_p, C.c_long, C.c_void_p,
+                                            C.c_long, C.c_long]
+            L.ref_cee_cvv.argtypes = [C.c_long] * 3 + [C.c_void_p, C.c_long] * 8
+            L.ref_intersample.argtypes = [C.c_long, C.c_long, C.c_double, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_long, C.c_void_p, C.c_void_p]
+            L.ref_intersample.restype = C.c_long
+            cls._lib = L
+        return cls._lib
+
+    @classmethod
+    def reconstructor(cls, Cmm, Ctm):
+        """(L, R): the reference's in-place potrf + two trsm on copies."""
+        L = np.array(Cmm, dtype=np.float64, order="F", copy=True)
+        R = np.array(Ctm, dtype=np.float64, order="F", copy=True)
+        nm, nts = L.shape[0], R.shape[0]
+        cls.lib().ref_reconstructor(nm, nts, L.ctypes.data, nm, R.ctypes.data, nts, 1)
+        return L, R
+
+    @classmethod
+    def cee_cvv(cls, Cmm, Ctt, Ctm, R, Dx):
+        """(Cee, Cvv, Cpp_after, Cpm_after, Tmp) from the reference's nine steps
+        (leading dimensions equal to the sizes, as the reference assumes)."""
+        f = lambda A: np.array(A, dtype=np.float64, order="F", copy=True)
+        Cmm, Cpp, Cpm, R, Dx = f(Cmm), f(Ctt), f(Ctm), f(R), f(Dx)
+        nm, nts, nact = Cmm.shape[0], Cpp.shape[0], Dx.shape[0]
+        Cee = np.zeros((nts, nts), order="F")
+        Cvv = np.zeros((nact, nact), order="F")
+        Tmp = np.zeros((nact, nts), order="F")
+        args = []
+        for A, ld in ((Cmm, nm), (Cpp, nts), (Cpm, nts), (R, nts), (Dx, nact), (Cee, nts),
+                      (Cvv, nact), (Tmp, nact)):
+            args += [A.ctypes.data, ld]
+        cls.lib().ref_cee_cvv(nm, nts, nact, *args)
+        return Cee, Cvv, Cpp, Cpm, Tmp
+
+    @classmethod
+    def intersample(cls, Cvv, idx, abs2fi, otf, np_, Dtel):
+        """PSF (N x N, flat C order like isample->dphi) from the reference's code."""
+        N = int(max(512, 8 * 2 ** int(np.log(np_) + 0.5)))
+        c = np.ascontiguousarray(np.asarray(Cvv, dtype=np.float64).flatten("F"))
+        ix = np.ascontiguousarray(idx, dtype=np.int64)
+        a = np.ascontiguousarray(np.asarray(abs2fi, dtype=np.float64).reshape(-1))
+        o = np.ascontiguousarray(np.asarray(otf, dtype=np.float64).reshape(-1))
+        assert a.size == N * N and o.size == N * N and ix.size == c.size
+        out = np.zeros(N * N)
+        got = cls.lib().ref_intersample(ix.size, np_, Dtel, ix.ctypes.data, a.ctypes.data,
+                                        o.ctypes.data, N, c.ctypes.data, out.ctypes.data)
+        if got != N:
+            raise ValueError("intersample: N differs from the tables' size")
+        return out.reshape(N, N)
 
 
 # ---------------------------------------------------------------- LAPACK steps

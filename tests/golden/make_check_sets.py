@@ -17,6 +17,13 @@
    truth sensor x LGS shared-point blocks, NGS x NGS, diagonal blocks, the x/y
    boundaries inside a WFS, the last rows).
 
+3. ``legacy_sets.json``: the ten legacy-layout system files of the reference's
+   ``datafile/benchmark`` directory (22 fields: diam, obs, nW, Nssp, gsAlt, type,
+   nLgs, alphaX, alphaY, XPup, YPup, thetaML, thetaCam, sensibilite, tracking,
+   pasDphi, ncpu, lgs_cst, noise_var, spot_width, lgs_alt, lgs_depth), value
+   lines as numbers. (The benchmark profiles are not kept: they declare 61
+   layers and list 60 altitudes, which the reference's reader rejects.)
+
     REF=/root/reference python tests/golden/make_check_sets.py
 """
 import json
@@ -103,7 +110,7 @@ def elt_extra(t):
         (3, 100, w(3, 0, 500)),                 # truth sensor x LGS (shared-point block)
         (3, ns + 50, w(1, 1, 2000)),            # truth sensor y x LGS y
         (3, 2000, w(6, 0, 400)),                # truth sensor x NGS
-        (3, ns - 24, w(7, 1, 2950) - 24),       # across boundaries
+        (3, ns - 24, w(7, 1, 2950) - 40),       # across boundaries, last WFS
     ]
 
 
@@ -123,6 +130,9 @@ def golden(name, t, extra=(), seed=7):
             np.linalg.norm(v)), np.array(v.size)
         out[f"{k}_idx"], out[f"{k}_val"] = sample_large(rng, v)
     spec = tiles_for(nm, nts, rng, list(extra))
+    for typ, r0, c0 in spec:  # every tile inside its matrix
+        nr, nc = {1: (nm, nm), 3: (nts, nm), 4: (nts, nts)}[typ]
+        assert 0 <= r0 <= nr - TILE and 0 <= c0 <= nc - TILE, (name, typ, r0, c0)
     vals = np.zeros((len(spec), TILE, TILE))
     t.setTarget(0)
     for i, (typ, r0, c0) in enumerate(spec):
@@ -152,6 +162,14 @@ def main():
         golden(s, t)
     with open(os.path.join(HERE, "check_sets.json"), "w") as f:
         json.dump(sets, f, indent=1)
+    legacy = {}
+    bdir = os.path.join(ref, "datafile", "benchmark")
+    for name in sorted(os.listdir(bdir)):
+        f = os.path.join(bdir, name, "sys-params.txt")
+        if os.path.exists(f):
+            legacy[name] = [[float(x) for x in v] for v in read_positional(f)]
+    with open(os.path.join(HERE, "legacy_sets.json"), "w") as f:
+        json.dump(legacy, f)
     # the seeded ELT-scale system of the benchmark
     sp, ap = P.config_elt()
     d = tempfile.mkdtemp(prefix="moao_elt_")

@@ -191,3 +191,63 @@ def test_mixed_default_format_ragged_panels(ctx, n, m, nb):
         ctx.set_block(256)
     err = O.rel_fro(host(dT), R_ref)
     assert err <= 1e-5, (err, rep)
+
+
+def test_wait_limit_times_out_then_context_recovers(ctx):
+    """A bound of one poll on the tensor-core kernel's waits makes them run out
+    (no GPU fault: the kernel drains its copies and MMAs, frees its tensor
+    memory and records the error); the call returns MOAO_ERR_TIMEOUT and the
+    same context then computes R normally."""
+    nm, nts, Cmm, Ctm = case("small")
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(M.MoaoError) as e:
+            M.reconstructor(nm, nts, dev(Cmm), nm, dev(Ctm), nts, 1, prec="mixed", ctx=ctx)
+        assert e.value.name == "MOAO_ERR_TIMEOUT"
+    finally:
+        ctx.set_wait_limit(0)
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    dT = dev(Ctm)
+    M.reconstructor(nm, nts, dev(Cmm), nm, dT, nts, 1, prec="mixed", ctx=ctx)
+    assert O.rel_fro(host(dT), R_ref) <= 1e-5
+
+
+def test_accuracy_target_falls_back_to_fp64_when_refinement_stalls(ctx):
+    """check2 (kappa ~ 2e7): one refinement leaves the mixed R near 1e-3; with
+    an accuracy target of 1e-5 the estimate misses it, the FP64 path computes
+    R and the factor, and the report says so. elt16 with declared offsets meets
+    the target and keeps the mixed result."""
+    import json
+    import os
+    nm, nts, Cmm, Ctm = case("check2")
+    L_ref, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    S = np.tril(Cmm) + np.tril(Cmm, -1).T
+    w = np.linalg.eigvalsh(S)
+    tol = max(1e-10, 50 * (w.max() / w.min()) * np.finfo(float).eps)
+    ctx.set_accuracy(1e-5)
+    try:
+        dC, dT = dev(Cmm), dev(Ctm)
+        rep = M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=ctx)
+        assert rep["fallback"] == 1 and rep["est_error"] > 1e-5, rep
+        assert O.rel_fro(host(dT), R_ref) <= tol
+        assert O.rel_fro(np.tril(host(dC)), np.tril(L_ref)) <= tol
+        est_bad = rep["est_error"]
+        sf, af = systems.files("elt16")
+        t = M.Tomo(sf, af)
+        ctx.set_offsets_from_tomo(t)
+        nm2, nts2, Cmm2, Ctm2 = case("elt16")
+        _, R2_ref, _ = O.reconstructor(Cmm2, Ctm2)
+        dT2 = dev(Ctm2)
+        rep2 = M.reconstructor(nm2, nts2, dev(Cmm2), nm2, dT2, nts2, 1, prec="mixed", ctx=ctx)
+        err2 = O.rel_fro(host(dT2), R2_ref)
+    finally:
+        ctx.set_accuracy(0)
+        ctx.set_offsets([], [], [])
+    path = os.environ.get("MOAO_PARITY_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"test": "accuracy_guard", "check2_est": est_bad,
+                                "elt16_est": rep2["est_error"], "elt16_actual": err2,
+                                "elt16_fallback": rep2["fallback"]}) + "\n")
+    assert rep2["fallback"] == 0 and 0 < rep2["est_error"] <= 1e-5, rep2
+    assert err2 <= 1e-5

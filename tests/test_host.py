@@ -127,3 +127,65 @@ def test_check_set_geometry_matches_reference_golden(built, name):
     nW, nLgs, nL, Nx, nm, nts = z["info"]
     assert (t.info.nW, t.info.nLgs, t.info.nLayer, t.info.Nx) == (nW, nLgs, nL, Nx)
     assert (t.getNMeas(), t.getNMeasTS()) == (nm, nts)
+
+
+@pytest.mark.parametrize("name", ["nx5120_wfs8_Nssp29", "nx10112_wfs8_Nssp41"])
+def test_legacy_benchmark_sys_file(built, name, tmp_path):
+    """A system file in the reference's legacy benchmark layout
+    (datafile/benchmark/*/sys-params.txt, tests/golden/legacy_sets.json) is
+    detected and read: its geometry equals the same system written in the
+    current layout, and its noise tables follow the legacy model (noise_var on
+    every NGS slope; across / along each LGS spot noise_var and
+    noise_var (ext^2 + w^2) / w^2)."""
+    import json
+    vals = json.load(open(os.path.join(GOLDEN, "legacy_sets.json")))[name]
+    f = dict(zip(P.LEGACY_FIELDS, vals))
+    sf = str(tmp_path / "legacy-sys-params.txt")
+    P.write_legacy_sys(vals, sf)
+    _, a = P.config_small()
+    af = str(tmp_path / "prof-1-atmos-night0.txt")
+    P.write_atm(a, af)
+    t = M.Tomo(sf, af)
+    nW, nLgs, nssp = int(f["nW"][0]), int(f["nLgs"][0]), int(f["Nssp"][0])
+    assert (t.info.nW, t.info.nLgs, t.info.nLayer) == (nW, nLgs, a.nLayer)
+    assert np.all(t.table("Nssp") == nssp)
+    # the same system in the current layout (photometric fields at their defaults)
+    s = P.SysParams(diam=f["diam"][0], obs=f["obs"][0], nW=nW, nLgs=nLgs, nTarget=1, nssp=nssp,
+                    gsAlt=f["gsAlt"], gsType=[int(x) for x in f["type"]], alphaX_as=f["alphaX_as"],
+                    alphaY_as=f["alphaY_as"], XPup=f["XPup"], YPup=f["YPup"], thetaML=f["thetaML"],
+                    thetaCam=f["thetaCam"], sensibilite=f["sensibilite"], tracking=f["tracking"],
+                    pasDphi=f["pasDphi"][0], ncpu=int(f["ncpu"][0]), mrNGS=[0.0] * (nW - nLgs),
+                    lgsCst=f["lgs_cst"][0], spotWidth=f["spot_width"][0], lgsAlt=f["lgs_alt"][0],
+                    lgsDepth=f["lgs_depth"][0])
+    sf2 = str(tmp_path / "sys-params.txt")
+    P.write_sys(s, sf2)
+    t2 = M.Tomo(sf2, af)
+    for k in ["u", "v", "X", "Y", "sspSizeL", "Nsubap", "lgsExt", "lgsTheta"]:
+        assert np.array_equal(t.table(k), t2.table(k)), k
+    assert t.getNMeas() == t2.getNMeas() and t.info.lgsCst == f["lgs_cst"][0]
+    v, w2 = f["noise_var"][0], f["spot_width"][0] ** 2
+    ext, th = t.table("lgsExt"), t.table("lgsTheta")
+    nl = int(np.sum(t.table("Nsubap")[:nLgs]))
+    L = v * (ext[:nl] ** 2 + w2) / w2
+    c, sn = np.cos(th[:nl]), np.sin(th[:nl])
+    assert np.allclose(t.table("noiseLGSxx")[:nl], L * c * c + v * sn * sn, rtol=1e-14, atol=0)
+    assert np.allclose(t.table("noiseLGSyy")[:nl], L * sn * sn + v * c * c, rtol=1e-14, atol=0)
+    assert np.allclose(t.table("noiseLGSxy")[:nl], (L - v) * sn * c, rtol=1e-13, atol=1e-18)
+    assert np.all(t.table("noiseNGS") == v)
+    # a current-layout file still takes the photometric model
+    assert not np.all(t2.table("noiseNGS") == v)
+
+
+def test_legacy_file_with_short_vectors_is_rejected(built, tmp_path):
+    """The eight wfs9 legacy files declare 10 WFS but list 9 guide-star
+    altitudes and types: rejected with MOAO_ERR_IO naming the short vector."""
+    import json
+    vals = json.load(open(os.path.join(GOLDEN, "legacy_sets.json")))["nx50184_wfs9_Nssp86"]
+    sf = str(tmp_path / "sys-params.txt")
+    P.write_legacy_sys(vals, sf)
+    _, a = P.config_small()
+    af = str(tmp_path / "prof-1-atmos-night0.txt")
+    P.write_atm(a, af)
+    with pytest.raises(M.MoaoError) as e:
+        M.Tomo(sf, af)
+    assert e.value.name == "MOAO_ERR_IO" and "gsAlt" in str(e.value)

@@ -149,3 +149,74 @@ def test_oracle_matches_reference_tiles_of_check_sets(name):
         got = np.zeros((nt, nt), order="F")
         O.matcov(g, nt, nt, int(r0), int(c0), int(typ), out=got)
         assert np.array_equal(got, want), (name, typ, r0, c0)
+
+
+needs_ref_dense = pytest.mark.skipif(not O.RefDense.available(),
+                                     reason="reference dense library not built here")
+
+
+def _dense_case(name):
+    g = _geom(name)
+    nm, nts = g.nmeas, g.nmeasts
+    Cmm = O.matcov(g, nm, nm, 0, 0, 1, nthreads=8)
+    Ctm = O.matcov(g, nts, nm, 0, 0, 3, nthreads=8)
+    Ctt = O.matcov(g, nts, nts, 0, 0, 4, nthreads=8)
+    return Cmm, Ctm, Ctt
+
+
+@needs_ref_dense
+@pytest.mark.parametrize("name", ["small", "check2"])
+def test_reconstructor_restatement_equals_reference_code(name):
+    """oracle.reconstructor against the reference's MOAO_LAPACK::reconstructor
+    (lapack/compute/reconstructor.cpp:32-58) run here on the same matrices."""
+    Cmm, Ctm, _ = _dense_case(name)
+    L, R, info = O.reconstructor(Cmm, Ctm)
+    L_ref, R_ref = O.RefDense.reconstructor(Cmm, Ctm)
+    assert info == 0
+    # the same OpenBLAS routines in the same order: bit-identical
+    assert np.array_equal(np.tril(L), np.tril(L_ref))
+    assert np.array_equal(R, R_ref)
+    assert np.array_equal(np.triu(L_ref, 1), np.triu(Cmm, 1)), "reference left the upper part"
+
+
+@needs_ref_dense
+@pytest.mark.parametrize("name", ["small", "check2"])
+def test_cee_cvv_restatement_equals_reference_code(name):
+    """oracle.cee_cvv (both geadd forms) against the reference's nine steps
+    (lapack/compute/cee_cvv.cpp:50-125) run here, including the in-place
+    results left in Cpp and Cpm."""
+    Cmm, Ctm, Ctt = _dense_case(name)
+    _, R, _ = O.reconstructor(Cmm, Ctm)
+    Dx = I.make_dx(100, Ctt.shape[0], seed=3)
+    ref = O.RefDense.cee_cvv(Cmm, Ctt, Ctm, R, Dx)
+    for literal in (True, False):
+        got = O.cee_cvv(Cmm, Ctt, Ctm, R, Dx, literal_geadd=literal)
+        Cee, Cvv, Cpp, Cpm, Tmp = got
+        # the literal geadd loop is bit-identical; the mirrored form equals it
+        # too (x + y and y + x round alike)
+        assert np.array_equal(Cee, ref[0])
+        assert np.array_equal(Cvv, ref[1])
+        assert np.array_equal(np.tril(Cpp), np.tril(ref[2]))
+        assert np.array_equal(Cpm, ref[3])
+        assert np.array_equal(Tmp, ref[4])
+
+
+@needs_ref_dense
+@pytest.mark.parametrize("nssp,diam,obs", [(10, 8.0, 0.14), (10, 39.0, 0.2), (29, 39.0, 0.2)])
+def test_intersample_restatement_equals_reference_code(nssp, diam, obs):
+    """oracle.intersample (numpy FFTs) against the reference's intersample
+    pipeline (common/tomo_struct/intersample.cpp:74-333) run here with the
+    FFTW transforms restated in oracle/ref_dense_shim.cpp."""
+    x = I.intersample_inputs(nssp, diam, obs)
+    rng = np.random.default_rng(4)
+    B = rng.standard_normal((x.nact, x.nact)) * 1e-3 / np.sqrt(x.nact)
+    Cvv = B @ B.T
+    got = O.intersample(Cvv, x.idx, x.abs2fi, x.otf, x.np_)
+    ref = O.RefDense.intersample(Cvv, x.idx, x.abs2fi, x.otf, x.np_, diam)
+    # measured: 1 ulp of the peak (numpy's FFT against the restated FFTW transforms)
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+    # a zero Cvv gives the telescope-only PSF in both
+    z = np.zeros_like(Cvv)
+    assert np.allclose(O.intersample(z, x.idx, x.abs2fi, x.otf, x.np_),
+                       O.RefDense.intersample(z, x.idx, x.abs2fi, x.otf, x.np_, diam),
+                       rtol=0, atol=1e-11 * np.max(np.abs(ref)))
