@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--serving", action="store_true",
                    help="serving-loop benchmark (Poisson arrivals, p50/p99) instead of the build loop")
-    p.add_argument("--serve-requests", type=int, default=24)
+    p.add_argument("--serve-requests", type=int, default=120)
     p.add_argument("--batch", action="store_true",
                    help="batched uneven instances in one graph launch instead of the build loop")
     p.add_argument("--batch-count", type=int, default=256)
@@ -499,8 +499,7 @@ def serving_main(args):
         sp, ap = P.config_elt() if nssp == 64 else P.config_scaled(nssp, 35)
         d = tempfile.mkdtemp(prefix=f"moao_serve_{nssp}_")
         P.write_system(d, sp, ap)
-        x = I.intersample_inputs(nssp, sp.diam, sp.obs)
-        systems.append(dict(nssp=nssp, dir=d, sys=sp, x=x))
+        systems.append(dict(nssp=nssp, dir=d, sys=sp))
     n_req = args.serve_requests
 
     def profile(r):
@@ -514,9 +513,11 @@ def serving_main(args):
         ids, infos = [], []
         for y in systems:
             sf, af = os.path.join(y["dir"], "sys-params.txt"), os.path.join(y["dir"], "prof-1-atmos-night0.txt")
-            nts = M.Tomo(sf, af).getNMeasTS()
-            Dx = I.make_dx(y["x"].nact, nts, seed=y["nssp"])
-            sid = srv.add_system(sf, af, Dx=Dx, idx=y["x"].idx, abs2fi=y["x"].abs2fi, otf=y["x"].otf)
+            tm = M.Tomo(sf, af)
+            # the PSF tables are synthesised by the library (C++/CUDA) for the truth sensor
+            nact, *_ = M.intersample_inputs(tm.info.nssp_ts, tm.info.diam, tm.info.obs, tables=False)
+            Dx = I.make_dx(nact, tm.getNMeasTS(), seed=y["nssp"])
+            sid = srv.add_system_synth(sf, af, Dx)
             ids.append(sid)
             infos.append(srv.system_info(sid))
         return srv, ids, infos

@@ -297,6 +297,22 @@ moao_status moao_intersample_get_info(const moao_isample* is, moao_isample_info*
 /* PSF (N x N, FFTW-unnormalised like the reference) from a DEVICE Cvv (nact^2,
  * column-major) into a DEVICE buffer d_psf of N*N doubles. */
 moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, double* d_psf);
+/* The three tables without files or the reference's Python tooling, for a truth
+ * sensor of nssp subapertures across on a telescope of diameter Dtel and
+ * central obscuration obs, DM influence coupling `coupling` (the tooling uses
+ * 0.2): the DM actuators (cython/pipeline/commande.py:57-79), idx
+ * (generate_file.py:57-76), abs2fi (generate_file.py:79-86) and the telescope
+ * OTF (intersample.pyx:151-200). *nact and *N receive the actuator count and
+ * the FFT support; idx (nact^2, 1-based, column-major pairs), abs2fi and otf_tel
+ * (N x N each) are filled where not NULL (host arrays). With all three NULL
+ * only the sizes are computed (ctx may then be NULL); the FFT tables run on
+ * the device (cuFFT). No reference counterpart: the reference reads FITS files. */
+moao_status moao_intersample_inputs(moao_ctx* ctx, long nssp, double Dtel, double obs,
+                                    double coupling, long* nact, long* N, long* idx,
+                                    double* abs2fi, double* otf_tel);
+/* moao_intersample_create with the tables of moao_intersample_inputs. */
+moao_status moao_intersample_create_synth(moao_ctx* ctx, long nssp, double Dtel, double obs,
+                                          double coupling, moao_isample** out);
 /* Same with host Cvv in and host PSF out. */
 moao_status moao_intersample_process_host(moao_isample* is, const double* Cvv, double* psf);
 void moao_intersample_destroy(moao_isample* is);
@@ -354,6 +370,14 @@ moao_status moao_server_create(const moao_server_opts* opts, moao_server** out);
 moao_status moao_server_add_system(moao_server* s, const char* sys_file, const char* atm_file,
                                    long nact, const double* Dx, const long* idx,
                                    const double* abs2fi, const double* otf_tel, int* system_id);
+/* The same with the PSF tables synthesised in C++/CUDA for the system's truth
+ * sensor (moao_intersample_inputs with the given DM coupling, 0.2 in the
+ * reference's tooling): no tables from the caller, no Python. nact must be the
+ * synthesised DM's actuator count (moao_intersample_inputs with NULL tables
+ * gives it without a GPU); Dx is nact x nmeasts. */
+moao_status moao_server_add_system_synth(moao_server* s, const char* sys_file,
+                                         const char* atm_file, long nact, const double* Dx,
+                                         double coupling, int* system_id);
 moao_status moao_server_system_info(moao_server* s, int system, long* nmeas, long* nmeasts,
                                     long* nact, long* psf_n);
 /* MOAO_ERR_OOM if the request alone exceeds the budget, MOAO_ERR_BUSY if the

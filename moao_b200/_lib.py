@@ -103,9 +103,14 @@ SIGNATURES = {
     "moao_ctx_set_host_precision": (i32, [vp, i32]),
     "moao_ctx_set_wait_limit": (i32, [vp, C.c_longlong]),
     "moao_ctx_set_accuracy": (i32, [vp, C.c_double]),
+    "moao_intersample_inputs": (i32, [vp, i64, C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,
+                                      vp]),
+    "moao_intersample_create_synth": (i32, [vp, i64, C.c_double, C.c_double, C.c_double, vp]),
     "moao_ctx_set_factor_format": (i32, [vp, i32]),
     "moao_ctx_set_lookahead": (i32, [vp, i32]),
     "moao_server_create": (i32, [C.POINTER(ServerOpts), C.POINTER(vp)]),
+    "moao_server_add_system_synth": (i32, [vp, C.c_char_p, C.c_char_p, C.c_long, vp, C.c_double,
+                                           C.POINTER(i32)]),
     "moao_server_add_system": (i32, [vp, C.c_char_p, C.c_char_p, C.c_long, vp, vp, vp, vp,
                                      C.POINTER(i32)]),
     "moao_server_system_info": (i32, [vp, i32, C.POINTER(C.c_long), C.POINTER(C.c_long),

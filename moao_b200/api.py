@@ -355,6 +355,28 @@ def Cee_Cvv(nmeas, nmeasts, nact, Cmm, ldCmm, Cpp, ldCpp, Cpm, ldCpm, R, ldR, Dx
         check(st, "Cee_Cvv")
 
 
+def intersample_inputs(nssp: int, Dtel: float, obs: float, coupling: float = 0.2,
+                       tables: bool = True, ctx: Optional[Context] = None):
+    """The intersample tables without files or Python tooling (moao_intersample_inputs):
+    returns (nact, N, idx, abs2fi, otf_tel); idx is exact host work, abs2fi and
+    otf_tel are computed on the device (None when tables is False)."""
+    na, N = C.c_long(), C.c_long()
+    check(lib().moao_intersample_inputs(None, nssp, Dtel, obs, coupling, C.byref(na), C.byref(N),
+                                        None, None, None), "moao_intersample_inputs")
+    idx = np.zeros(na.value * na.value, dtype=np.int64)
+    a = o = None
+    if tables:
+        ctx = ctx or default_context()
+        a = np.zeros((N.value, N.value))
+        o = np.zeros((N.value, N.value))
+    check(lib().moao_intersample_inputs(ctx.handle if tables else None, nssp, Dtel, obs, coupling,
+                                        C.byref(na), C.byref(N), idx.ctypes.data,
+                                        a.ctypes.data if tables else None,
+                                        o.ctypes.data if tables else None),
+          "moao_intersample_inputs")
+    return na.value, N.value, idx, a, o
+
+
 class Intersample:
     """PSF from Cvv; the three input tables (idx, abs2fi, otf_tel) are given as
     arrays instead of the reference's idx.fits / abs2fi.fits / otftel.fits."""

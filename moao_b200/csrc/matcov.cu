@@ -84,8 +84,8 @@ __device__ __forceinline__ double dphi_unit(double x) {
 // range) the direct form is used. The per-pair kernels call the non-inlined
 // copy below: their 9 or 16 stencil points per layer then share one body,
 // which keeps them inside the instruction cache (inlined, they stalled on
-// instruction fetch; ~8% slower). The shared-point kernel has one call site
-// and inlines it.
+// instruction fetch; ~8% slower). The shared-point kernel inlines it at its
+// four call sites (two evaluations per loop iteration, two loops).
 // The two uncommon branches are separate functions, so that the series path,
 // the one most points take, issues none of their instructions (inlined, the
 // compiler predicates them into every evaluation).
@@ -445,25 +445,27 @@ __global__ void __launch_bounds__(kEThreads, 3)
       sq[k] = t2 * (dv * dv);
     }
     __syncthreads();
-    // 2. points: 4 x 1,440, each covariance a whole number of warps
-    for (int p = tid; p < 4 * kEKind; p += kEThreads) {
-      const int kind = p / kEKind, f = p - kind * kEKind;
-      int r, cc, dst;
-      double sr, sc;
-      if (kind == 0) {         // XX 45 x 32
-        r = f >> 5; cc = f & 31; dst = r * 36 + cc;
-        sr = sq[kESqXXr + r]; sc = sq[kESqXXc + cc];
-      } else if (kind == 1) {  // YY 45 x 32
-        r = f >> 5; cc = f & 31; dst = kEOffYY + r * 36 + cc;
-        sr = sq[kESqYYr + r]; sc = sq[kESqYYc + cc];
-      } else if (kind == 2) {  // XY 40 x 36
-        r = f / 36; cc = f - r * 36; dst = kEOffXY + r * 36 + cc;
-        sr = sq[kESqXYr + r]; sc = sq[kESqXYc + cc];
-      } else {                 // YX 36 x 40
-        r = f / 40; cc = f - r * 40; dst = kEOffYX + r * 44 + cc;
-        sr = sq[kESqYXr + r]; sc = sq[kESqYXc + cc];
+    // 2. points: 4 x 1,440, two independent evaluations per iteration (twice the
+    // FP64 chains in flight) with the table indices stepped, not divided out
+    {
+      // XX and YY (45 x 32 each, row stride 36): column tid % 32, rows tid / 32 + 8 k
+      const int cc = tid & 31;
+      const double scx = sq[kESqXXc + cc], scy = sq[kESqYYc + cc];
+      for (int r = tid >> 5; r < 45; r += kEThreads / 32) {
+        const double vx = dphi_unit_s_inl(sq[kESqXXr + r] + scx);
+        const double vy = dphi_unit_s_inl(sq[kESqYYr + r] + scy);
+        pts[r * 36 + cc] = vx;
+        pts[kEOffYY + r * 36 + cc] = vy;
       }
-      pts[dst] = dphi_unit_s_inl(sr + sc);
+      // XY (40 x 36, stride 36) and YX (36 x 40, stride 44) by flat index
+      for (int f = tid; f < kEKind; f += kEThreads) {
+        const int r1 = f / 36, c1 = f - 36 * r1;
+        const int r2 = f / 40, c2 = f - 40 * r2;
+        const double v1 = dphi_unit_s_inl(sq[kESqXYr + r1] + sq[kESqXYc + c1]);
+        const double v2 = dphi_unit_s_inl(sq[kESqYXr + r2] + sq[kESqYXc + c2]);
+        pts[kEOffXY + r1 * 36 + c1] = v1;
+        pts[kEOffYX + r2 * 44 + c2] = v2;
+      }
     }
     __syncthreads();
     // 3. the reference's stencils (cov_XX/YY/XY/YX, matcov_kernels.cpp:147-193), in its

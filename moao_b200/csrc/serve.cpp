@@ -393,6 +393,42 @@ moao_status moao_server_add_system(moao_server* s, const char* sys_file, const c
   return MOAO_OK;
 }
 
+moao_status moao_server_add_system_synth(moao_server* s, const char* sys_file,
+                                         const char* atm_file, long nact, const double* Dx,
+                                         double coupling, int* system_id) {
+  if (!s || !sys_file || !atm_file || !system_id || !Dx || nact <= 0)
+    return set_error(MOAO_ERR_BAD_ARG, "server_add_system_synth: null or nact <= 0");
+  Tomo_struct<double> t;
+  try {
+    t = Tomo_struct<double>(sys_file, atm_file);
+  } catch (const std::exception& ex) {
+    return set_error(MOAO_ERR_IO, ex.what());
+  }
+  const long nssp = t.Nssp[t.sys.nW - 1];
+  long na = 0, N = 0;
+  MOAO_TRY(moao_intersample_inputs(nullptr, nssp, t.sys.diam, t.sys.obs, coupling, &na, &N,
+                                   nullptr, nullptr, nullptr));
+  if (na != nact)
+    return set_error(MOAO_ERR_BAD_ARG, "server_add_system_synth: the truth sensor's DM has " +
+                                           std::to_string(na) + " actuators, Dx has " +
+                                           std::to_string(nact) + " rows");
+  std::vector<long> idx((size_t)na * na);
+  std::vector<double> a((size_t)N * N), o((size_t)N * N);
+  if (s->opt.dry_run) {
+    MOAO_TRY(moao_intersample_inputs(nullptr, nssp, t.sys.diam, t.sys.obs, coupling, &na, &N,
+                                     idx.data(), nullptr, nullptr));
+  } else {
+    moao_ctx* ctx = nullptr;
+    MOAO_TRY(moao_ctx_create(s->opt.device, &ctx));
+    const moao_status st = moao_intersample_inputs(ctx, nssp, t.sys.diam, t.sys.obs, coupling, &na,
+                                                   &N, idx.data(), a.data(), o.data());
+    moao_ctx_destroy(ctx);
+    MOAO_TRY(st);
+  }
+  return moao_server_add_system(s, sys_file, atm_file, nact, Dx, idx.data(), a.data(), o.data(),
+                                system_id);
+}
+
 moao_status moao_server_system_info(moao_server* s, int system, long* nmeas, long* nmeasts,
                                     long* nact, long* psf_n) {
   if (!s) return set_error(MOAO_ERR_BAD_ARG, "server_system_info: null");

@@ -70,6 +70,17 @@ class Server:
                                            dxp, ip, ap, op, C.byref(sid)), "moao_server_add_system")
         return int(sid.value)
 
+    def add_system_synth(self, sys_file: str, atm_file: str, Dx, coupling: float = 0.2) -> int:
+        """Registers a system whose PSF tables the library synthesises itself for
+        the truth sensor (moao_server_add_system_synth); Dx is nact x nmeasts with
+        nact the synthesised DM's actuator count (moao_b200.intersample_inputs)."""
+        Dx = np.asfortranarray(Dx, dtype=np.float64)
+        sid = C.c_int()
+        check(lib().moao_server_add_system_synth(self._h, sys_file.encode(), atm_file.encode(),
+                                                 Dx.shape[0], Dx.ctypes.data, coupling,
+                                                 C.byref(sid)), "moao_server_add_system_synth")
+        return int(sid.value)
+
     def system_info(self, system: int) -> dict:
         v = [C.c_long() for _ in range(4)]
         check(lib().moao_server_system_info(self._h, system, *[C.byref(x) for x in v]),

@@ -1,7 +1,10 @@
 """The reference's C++ entry points (include/moao_b200_compat.hpp): a driver
 written against that interface alone (tests/drivers/lapack_driver.cpp, the call
 sequence of the reference's lapack driver) compiles and links against the
-library; on a GPU its outputs equal the Python API's."""
+library; on a GPU its outputs equal the Python API's. The reference's own
+driver, lapack/moao_lapack.cpp, compiled unchanged against the library through
+include/moao_b200_dropin (oracle/_ref/moao_lapack_dropin, built by
+`make -C oracle ref`), runs on the GPU and writes the same PSF."""
 import os
 import shutil
 import subprocess
@@ -16,6 +19,7 @@ from moao_b200.fits import read_fits, write_fits
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBDIR = os.path.join(ROOT, "moao_b200")
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "moao_lapack_dropin")
 
 
 def build_driver(tmp_path):
@@ -62,23 +66,10 @@ def write_inputs(d, sysp, nts):
     return x, Dx
 
 
-@pytest.mark.gpu
-def test_driver_matches_python_api(tmp_path, built, ctx):
-    sysp, atm = P.config_small()
-    d = str(tmp_path / "sys")
-    out = str(tmp_path / "out")
-    os.makedirs(out)
-    sf, af = os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt")
-    os.makedirs(d)
-    P.write_system(d, sysp, atm)
-    t = M.Tomo(sf, af)
+def python_sequence(t, sysp, x, Dx, ctx):
+    """The reference driver's first refine step and first observation through
+    the Python API (host buffers): R, Cee, Cvv and the PSF of target 0."""
     nm, nts = t.getNMeas(), t.getNMeasTS()
-    x, Dx = write_inputs(d, sysp, nts)
-    exe = build_driver(tmp_path)
-    r = subprocess.run([exe, d, af, out], capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stdout + r.stderr
-
-    # the same sequence through the Python API (host buffers)
     Cmm = np.zeros((nm, nm), order="F")
     M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
     t.setTarget(0)
@@ -100,6 +91,29 @@ def test_driver_matches_python_api(tmp_path, built, ctx):
     isx = M.Intersample(nact * nact, x.np_, sysp.diam, x.idx, x.abs2fi, x.otf, ctx=ctx)
     psf = isx.process(Cvv.copy(order="F"))
     isx.close()
+    return R, Cee, Cvv, psf
+
+
+def small_system(tmp_path):
+    sysp, atm = P.config_small()
+    d = str(tmp_path / "sys")
+    os.makedirs(d)
+    sf, af = os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt")
+    P.write_system(d, sysp, atm)
+    t = M.Tomo(sf, af)
+    x, Dx = write_inputs(d, sysp, t.getNMeasTS())
+    return sysp, d, af, t, x, Dx
+
+
+@pytest.mark.gpu
+def test_driver_matches_python_api(tmp_path, built, ctx):
+    sysp, d, af, t, x, Dx = small_system(tmp_path)
+    out = str(tmp_path / "out")
+    os.makedirs(out)
+    exe = build_driver(tmp_path)
+    r = subprocess.run([exe, d, af, out], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    R, Cee, Cvv, psf = python_sequence(t, sysp, x, Dx, ctx)
 
     def same(name, want):
         got = read_fits(os.path.join(out, name))
@@ -110,3 +124,32 @@ def test_driver_matches_python_api(tmp_path, built, ctx):
     same("Cee_g0.fits", Cee.T)
     same("Cvv_g0.fits", Cvv.T)
     same("psf_g0.fits", psf)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.environ.get("MOAO_REFERENCE", "/root/reference")),
+                    reason="the reference tree is not on this machine")
+def test_reference_driver_built_unchanged(built):
+    """Where the reference tree is present, `make -C oracle ref` compiles the
+    reference's own lapack/moao_lapack.cpp unchanged against this library; the
+    binary starts and parses its command line (no GPU needed for that)."""
+    assert os.path.exists(DROPIN), "run `make -C oracle ref REF=<reference tree>`"
+    r = subprocess.run([DROPIN], capture_output=True, text=True, timeout=60)
+    assert "sys_path" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="reference driver not built")
+def test_reference_driver_runs_unchanged_on_the_library(tmp_path, built, ctx):
+    """The reference's lapack driver, unchanged, linked against this library:
+    one refine step and one observation of the 8 m system; its PSF file equals
+    the Python API's result of the same sequence."""
+    sysp, d, af, t, x, Dx = small_system(tmp_path)
+    out = str(tmp_path / "run")
+    os.makedirs(out)
+    r = subprocess.run([DROPIN, f"--sys_path={d}", f"--atm_path={d}", "--maxobs=1",
+                        "--maxrefine=1"], capture_output=True, text=True, timeout=600, cwd=out)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    R, Cee, Cvv, psf = python_sequence(t, sysp, x, Dx, ctx)
+    got = read_fits(os.path.join(out, "psf_oloop0_iloop0_gal0.fits"))
+    err = np.max(np.abs(got - psf)) / np.max(np.abs(psf))
+    assert err <= 1e-12, err

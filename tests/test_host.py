@@ -189,3 +189,15 @@ def test_legacy_file_with_short_vectors_is_rejected(built, tmp_path):
     with pytest.raises(M.MoaoError) as e:
         M.Tomo(sf, af)
     assert e.value.name == "MOAO_ERR_IO" and "gsAlt" in str(e.value)
+
+
+@pytest.mark.parametrize("nssp,diam,obs", [(10, 8.0, 0.14), (29, 39.0, 0.2), (64, 39.0, 0.28)])
+def test_dm_and_idx_synthesis_matches_tooling(built, nssp, diam, obs):
+    """moao_intersample_inputs (C++, no Python tooling) gives the actuator count,
+    FFT support and idx of the reference tooling's formulas (restated in
+    moao_b200.inputs) exactly; host-only, no GPU."""
+    from moao_b200 import inputs as I
+    na, N, idx, _, _ = M.intersample_inputs(nssp, diam, obs, tables=False)
+    x = I.intersample_inputs(nssp, diam, obs)
+    assert na == x.nact and N == x.fourier.N
+    assert np.array_equal(idx, x.idx)

@@ -111,3 +111,19 @@ def test_cancel_and_error_contract(built):
             srv.submit(sid, *PROF)
         assert e.value.name == "MOAO_ERR_OOM"
         assert srv.stats()["rejected"] == 1
+
+
+def test_system_with_synthesised_psf_tables(built):
+    """A system registered with moao_server_add_system_synth carries PSF tables
+    built by the library for its truth sensor; Dx must have the synthesised DM's
+    actuator count (dry run: idx synthesised, no GPU)."""
+    t = M.Tomo(*systems.files("small"))
+    na, N, _, _, _ = M.intersample_inputs(t.info.nssp_ts, t.info.diam, t.info.obs, tables=False)
+    Dx = np.zeros((na, t.getNMeasTS()), order="F")
+    with Server(slots=1, hbm_budget_gb=100.0, dry_run=True) as srv:
+        sid = srv.add_system_synth(*systems.files("small"), Dx)
+        info = srv.system_info(sid)
+        assert info["nact"] == na and info["psf_n"] == N
+        with pytest.raises(M.MoaoError) as e:
+            srv.add_system_synth(*systems.files("small"), Dx[:-1])
+        assert e.value.name == "MOAO_ERR_BAD_ARG" and str(na) in str(e.value)
