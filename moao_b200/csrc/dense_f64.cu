@@ -350,141 +350,114 @@ moao_status launch_gemm(const KParams& p, cudaStream_t s) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // ---------------------------------------------------------------------------
-// Leaf factorisation of a diagonal block (n <= 64), fused with the inversion of
-// the resulting triangular factor, as one more level of the block recursion
-// inside one CTA:
-//   L11, D11 = L11^-1      one warp, 32 x 32 in registers (factor_inv_32)
-//   L21 = A21 D11^T        all threads
-//   A22 -= L21 L21^T       all threads (lower)
-//   L22, D22               one warp
-//   D21 = -D22 (L21 D11)   all threads
-// In factor_inv_32 lane l holds row l. Cholesky step j: d = A(j,j) from lane
-// j, r = 1/sqrt(d), L(l,j) = A(l,j) r, then A(l,k) -= L(l,j) L(k,j) for k > j
-// with L(k,j) shuffled from lane k. Inverse (right-looking forward
-// substitution, the row reusing the factor's registers): step i, lane i turns
-// its row into row i of L^-1 (times r_i = 1/L(i,i)), and every lane l > i
-// subtracts L(l,i) times that row, shuffled from lane i.
+// Leaf factorisation of a diagonal block (n <= 64) fused with the inversion of
+// its triangular factor, one CTA of 256 threads. Every thread owns up to nine
+// elements of the 64 x 64 lower triangle (element e = t + 256 s of the
+// row-packed triangle) and keeps them in registers through both phases:
+//   factor (right-looking, step j = 0..63): the owners of column j publish it
+//     (unscaled) to shared memory; after one barrier every thread takes
+//     d = A(j,j), r = 1/sqrt(d), writes L(i,j) = A(i,j) r (L(j,j) = d r) for
+//     its column-j elements and applies A(i,k) -= (A(i,j) r)(A(k,j) r) to
+//     its elements with k > j (column j is never written during step j);
+//   inverse (X = L^-1 by rows, step i = 0..63, B = I): the owners of row i
+//     finish X(i,c) = B(i,c) / L(i,i) and publish the row; after one barrier
+//     every thread applies B(r,c) -= L(r,i) X(i,c) to its elements with r > i.
+// The published column/row alternates between two buffers, so one barrier per
+// step suffices: a thread can only overwrite a buffer after every thread has
+// passed the next step's barrier, i.e. finished reading it. A non-positive
+// pivot is reported (first failing global column, 1-based, into *info) and
+// replaced by 1 so the kernel finishes without NaNs; rows and columns beyond n
+// are an identity block.
 // ---------------------------------------------------------------------------
 constexpr int LEAF = 64;
 constexpr int LEAF_LD = LEAF + 1;
-constexpr int HALF = 32;
+constexpr int LEAF_THREADS = 256;
+constexpr int LEAF_TRI = LEAF * (LEAF + 1) / 2;                          // 2,080
+constexpr int LEAF_OWN = (LEAF_TRI + LEAF_THREADS - 1) / LEAF_THREADS;  // 9
 
-// Factor and invert the nn x nn (nn <= 32) lower block at (o, o) of S into
-// the same place of Lo (factor) and Do (inverse). One full warp.
-__device__ __noinline__ void factor_inv_32(const double* S, double* Lo, double* Do, int o, int nn,
-                                           long col0, int* info) {
-  const int l = threadIdx.x & 31;
-  double a[HALF];
+__global__ void __launch_bounds__(LEAF_THREADS, 1) potrf_inv_leaf_kernel(double* A, long lda,
+                                                                         double* Linv, long ldi,
+                                                                         int n, long col0,
+                                                                         int* info) {
+  extern __shared__ __align__(16) double leaf_smem[];
+  double* Lf = leaf_smem;                     // the factor, column-major, ld LEAF_LD
+  double* Xs = leaf_smem + LEAF * LEAF_LD;    // the input block, then the inverse
+  double* buf = leaf_smem + 2 * LEAF * LEAF_LD;  // [2][LEAF]: published column / row
+  double* rinv = buf + 2 * LEAF;              // 1 / L(j,j)
+  const int tid = threadIdx.x;
+  for (int e = tid; e < LEAF * LEAF; e += LEAF_THREADS) {
+    const int i = e % LEAF, j = e / LEAF;
+    Xs[i + j * LEAF_LD] = (i < n && j < n) ? (i >= j ? A[(long)j * lda + i] : 0.0)
+                                           : (i == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  double a[LEAF_OWN];
+  int ri[LEAF_OWN], ci[LEAF_OWN];  // row >= column of each owned element; -1 past the triangle
 #pragma unroll
-  for (int k = 0; k < HALF; ++k)
-    a[k] = (l < nn && k <= l) ? S[(o + l) + (o + k) * LEAF_LD] : (k == l ? 1.0 : 0.0);
-  bool reported = false;
-  double r_own = 1.0;
+  for (int s = 0; s < LEAF_OWN; ++s) {
+    const int e = tid + LEAF_THREADS * s;
+    if (e < LEAF_TRI) {
+      int i = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);  // row of the packed index
+      while (i * (i + 1) / 2 > e) --i;
+      while ((i + 1) * (i + 2) / 2 <= e) ++i;
+      ri[s] = i;
+      ci[s] = e - i * (i + 1) / 2;
+      a[s] = Xs[ri[s] + ci[s] * LEAF_LD];
+    } else {
+      ri[s] = ci[s] = -1;
+      a[s] = 0.0;
+    }
+  }
+  // ---- factor
+  for (int j = 0; j < LEAF; ++j) {
+    double* cj = buf + (j & 1) * LEAF;
 #pragma unroll
-  for (int j = 0; j < HALF; ++j) {
-    double d = __shfl_sync(0xffffffffu, a[j], j);
+    for (int s = 0; s < LEAF_OWN; ++s)
+      if (ci[s] == j) cj[ri[s]] = a[s];
+    __syncthreads();
+    double d = cj[j];
     if (!(d > 0.0)) {
-      // keep going without NaNs; info reports the first such column
-      if (l == 0 && !reported && j < nn) {
-        reported = true;
-        atomicCAS(info, 0, (int)(col0 + o + j + 1));
-      }
+      if (tid == 0 && j < n) atomicCAS(info, 0, (int)(col0 + j + 1));
       d = 1.0;
     }
     const double r = rsqrt(d);
-    const double lj = (l == j ? d : a[j]) * r;
-    a[j] = lj;
-    if (l == j) r_own = r;
 #pragma unroll
-    for (int k = j + 1; k < HALF; ++k) a[k] = fma(-lj, __shfl_sync(0xffffffffu, lj, k), a[k]);
-  }
-  if (l < nn) {
-#pragma unroll
-    for (int k = 0; k < HALF; ++k)
-      if (k <= l && k < nn) Lo[(o + l) + (o + k) * LEAF_LD] = a[k];
-  }
-#pragma unroll
-  for (int i = 0; i < HALF; ++i) {
-    const double lli = a[i];
-#pragma unroll
-    for (int c = 0; c <= i; ++c) {
-      const double wc = __shfl_sync(0xffffffffu, c == i ? r_own : a[c] * r_own, i);
-      if (l == i) a[c] = wc;
-      else if (l > i) a[c] = c == i ? -lli * wc : fma(-lli, wc, a[c]);
+    for (int s = 0; s < LEAF_OWN; ++s) {
+      if (ci[s] == j) {
+        Lf[ri[s] + j * LEAF_LD] = (ri[s] == j ? d : a[s]) * r;
+      } else if (ci[s] > j) {
+        const double li = cj[ri[s]] * r, lk = cj[ci[s]] * r;
+        a[s] = fma(-li, lk, a[s]);
+      }
     }
-  }
-  if (l < nn) {
-#pragma unroll
-    for (int k = 0; k < HALF; ++k)
-      if (k <= l && k < nn) Do[(o + l) + (o + k) * LEAF_LD] = a[k];
-  }
-}
-
-__global__ void __launch_bounds__(256, 1) potrf_inv_leaf_kernel(double* A, long lda, double* Linv,
-                                                                long ldi, int n, long col0,
-                                                                int* info) {
-  extern __shared__ __align__(16) double leaf_smem[];
-  double* S = leaf_smem;                       // input lower, later L21 D11
-  double* Lf = leaf_smem + LEAF * LEAF_LD;     // factor
-  double* Di = leaf_smem + 2 * LEAF * LEAF_LD; // inverse
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  for (int e = tid; e < LEAF * LEAF; e += blockDim.x) {
-    const int i = e % LEAF, j = e / LEAF;
-    S[i + j * LEAF_LD] = (i < n && j < n && i >= j) ? A[(long)j * lda + i] : 0.0;
-    Lf[i + j * LEAF_LD] = 0.0;
-    Di[i + j * LEAF_LD] = 0.0;
+    if (tid == 0) rinv[j] = r;
   }
   __syncthreads();
-  const int n1 = n < HALF ? n : HALF, n2 = n - n1;
-  if (warp == 0) factor_inv_32(S, Lf, Di, 0, n1, col0, info);
-  __syncthreads();
-  if (n2 > 0) {
-    // L21 = A21 D11^T : L21(i,k) = sum_{m <= k} A21(i,m) D11(k,m)
-    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
-      const int i = e % HALF, k = e / HALF;
-      if (i >= n2) continue;
-      double acc = 0.0;
-      for (int m = 0; m <= k; ++m) acc = fma(S[(HALF + i) + m * LEAF_LD], Di[k + m * LEAF_LD], acc);
-      Lf[(HALF + i) + k * LEAF_LD] = acc;
-    }
+  // ---- inverse of the factor, by rows
+#pragma unroll
+  for (int s = 0; s < LEAF_OWN; ++s) a[s] = (ri[s] >= 0 && ri[s] == ci[s]) ? 1.0 : 0.0;
+  for (int i = 0; i < LEAF; ++i) {
+    double* xi = buf + (i & 1) * LEAF;
+    const double ri_inv = rinv[i];
+#pragma unroll
+    for (int s = 0; s < LEAF_OWN; ++s)
+      if (ri[s] == i) {
+        a[s] *= ri_inv;
+        xi[ci[s]] = a[s];
+      }
     __syncthreads();
-    // A22 -= L21 L21^T (lower)
-    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
-      const int i = e % HALF, j = e / HALF;
-      if (i >= n2 || j > i) continue;
-      double acc = 0.0;
-      for (int k = 0; k < HALF; ++k)
-        acc = fma(Lf[(HALF + i) + k * LEAF_LD], Lf[(HALF + j) + k * LEAF_LD], acc);
-      S[(HALF + i) + (HALF + j) * LEAF_LD] -= acc;
-    }
-    __syncthreads();
-    if (warp == 0) factor_inv_32(S, Lf, Di, HALF, n2, col0, info);
-    __syncthreads();
-    // P = L21 D11 : P(i,m) = sum_{k >= m} L21(i,k) D11(k,m), kept where A21 was
-    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
-      const int i = e % HALF, m = e / HALF;
-      if (i >= n2) continue;
-      double acc = 0.0;
-      for (int k = m; k < HALF; ++k) acc = fma(Lf[(HALF + i) + k * LEAF_LD], Di[k + m * LEAF_LD], acc);
-      S[(HALF + i) + m * LEAF_LD] = acc;
-    }
-    __syncthreads();
-    // D21 = -D22 P : D21(i,m) = -sum_{k <= i} D22(i,k) P(k,m)
-    for (int e = tid; e < HALF * HALF; e += blockDim.x) {
-      const int i = e % HALF, m = e / HALF;
-      if (i >= n2) continue;
-      double acc = 0.0;
-      for (int k = 0; k <= i; ++k)
-        acc = fma(Di[(HALF + i) + (HALF + k) * LEAF_LD], S[(HALF + k) + m * LEAF_LD], acc);
-      Di[(HALF + i) + m * LEAF_LD] = -acc;
-    }
-    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < LEAF_OWN; ++s)
+      if (ri[s] > i && ci[s] <= i) a[s] = fma(-Lf[ri[s] + i * LEAF_LD], xi[ci[s]], a[s]);
   }
-  for (int e = tid; e < n * n; e += blockDim.x) {
+#pragma unroll
+  for (int s = 0; s < LEAF_OWN; ++s)
+    if (ri[s] >= 0) Xs[ri[s] + ci[s] * LEAF_LD] = a[s];
+  __syncthreads();
+  for (int e = tid; e < n * n; e += LEAF_THREADS) {
     const int i = e % n, j = e / n;
     if (i >= j) A[(long)j * lda + i] = Lf[i + j * LEAF_LD];
-    Linv[(long)j * ldi + i] = Di[i + j * LEAF_LD];
+    Linv[(long)j * ldi + i] = i >= j ? Xs[i + j * LEAF_LD] : 0.0;
   }
 }
 
@@ -560,9 +533,9 @@ moao_status potrf_inv_leaf(double* A, long lda, double* Linv, long ldi, int n, l
   if (n <= 0) return MOAO_OK;
   if (n > LEAF) return set_error(MOAO_ERR_BAD_ARG, "potrf leaf: n > 64");
   static std::atomic<unsigned long long> configured{0};
-  const int smem = 3 * LEAF * LEAF_LD * (int)sizeof(double);
+  const int smem = (2 * LEAF * LEAF_LD + 3 * LEAF) * (int)sizeof(double);
   MOAO_CUDA_TRY(set_smem_limit(potrf_inv_leaf_kernel, smem, configured));
-  potrf_inv_leaf_kernel<<<1, 256, smem, s>>>(A, lda, Linv, ldi, n, col0, d_info);
+  potrf_inv_leaf_kernel<<<1, LEAF_THREADS, smem, s>>>(A, lda, Linv, ldi, n, col0, d_info);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
