@@ -392,6 +392,11 @@ void moao_ctx_destroy(moao_ctx* c) {
     cudaStreamSynchronize(c->aux);
     cudaStreamDestroy(c->aux);
   }
+  if (c->copy) {
+    cudaStreamSynchronize(c->copy);
+    cudaStreamDestroy(c->copy);
+  }
+  for (auto e : c->copy_ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -618,25 +623,59 @@ moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_d
   MOAO_TRY(ctx->ws_tmp.ensure(bytes));
   double* d = ctx->ws_tmp.as<double>();
   cudaStream_t s = ctx->stream;
-  if (type_mat == 1) {
-    // A type-1 tile writes only elements on or below the global diagonal; the
-    // others keep the caller's values. Only the panels' diagonal blocks (where
-    // both kinds meet) go down, and only the written panels come back.
-    const long dd = (long)xoffset - yoffset;
-    MOAO_TRY(copy_lower_panels(d, nrows, h_data, lda, nrows, ncols, dd, true,
-                               cudaMemcpyHostToDevice, s));
-    MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, s,
+  if (type_mat != 1 && type_mat != 2 && type_mat != 3 && type_mat != 4 && type_mat != 5)
+    return set_error(MOAO_ERR_BAD_ARG, "matcov_tile_host: unknown type_mat " +
+                                           std::to_string(type_mat));
+  // Column blocks at the WFS boundaries of the columns (types 1 and 3 have WFS
+  // slopes as columns and write only inside their own columns; a block holds both
+  // slope axes of its WFS, so no pair's stencils are evaluated twice): block b is
+  // generated on the context stream while block b - 1 is copied back on the copy
+  // stream. Type 5 mirrors into other columns and stays one block.
+  std::vector<long> cuts{0};
+  if (type_mat == 1 || type_mat == 3) {
+    long b = 0;
+    const Tomo_struct<double>& tt = t->t;
+    for (int w = 0; w + 1 < tt.sys.nW; ++w) {
+      b += 2 * tt.Nsubap[w];
+      const long c = b - yoffset;
+      if (c > 0 && c < ncols) cuts.push_back(c);
+    }
+  }
+  cuts.push_back(ncols);
+  if (!ctx->copy) MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  while (ctx->copy_ev.size() < cuts.size()) {
+    cudaEvent_t e;
+    MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->copy_ev.push_back(e);
+  }
+  const long dd = (long)xoffset - yoffset;
+  for (size_t k = 0; k + 1 < cuts.size(); ++k) {
+    const long c0 = cuts[k], w = cuts[k + 1] - c0;
+    double* dk = d + c0 * nrows;
+    double* hk = h_data + c0 * (long)lda;
+    if (type_mat == 1) {
+      // A type-1 tile writes only elements on or below the global diagonal; the
+      // others keep the caller's values. Only the panels' diagonal blocks (where
+      // both kinds meet) go down, and only the written panels come back.
+      MOAO_TRY(copy_lower_panels(dk, nrows, hk, lda, nrows, w, dd - c0, true,
+                                 cudaMemcpyHostToDevice, s));
+    }
+    MOAO_TRY(launch_matcov(*g, dk, nrows, (int)w, xoffset, yoffset + (int)c0, nrows, type_mat, s,
                            &ctx->launches));
-    MOAO_TRY(copy_lower_panels(h_data, lda, d, nrows, nrows, ncols, dd, false,
-                               cudaMemcpyDeviceToHost, s));
-  } else {
-    // every element of the tile is written (or the type is rejected)
-    MOAO_TRY(launch_matcov(*g, d, nrows, ncols, xoffset, yoffset, nrows, type_mat, s,
-                           &ctx->launches));
-    MOAO_CUDA_TRY(cudaMemcpy2DAsync(h_data, sizeof(double) * lda, d, sizeof(double) * nrows,
-                                    sizeof(double) * nrows, ncols, cudaMemcpyDeviceToHost, s));
+    MOAO_CUDA_TRY(cudaEventRecord(ctx->copy_ev[k], s));
+    MOAO_CUDA_TRY(cudaStreamWaitEvent(ctx->copy, ctx->copy_ev[k], 0));
+    if (type_mat == 1) {
+      MOAO_TRY(copy_lower_panels(hk, lda, dk, nrows, nrows, w, dd - c0, false,
+                                 cudaMemcpyDeviceToHost, ctx->copy));
+    } else {
+      // every element of the block is written
+      MOAO_CUDA_TRY(cudaMemcpy2DAsync(hk, sizeof(double) * lda, dk, sizeof(double) * nrows,
+                                      sizeof(double) * nrows, w, cudaMemcpyDeviceToHost,
+                                      ctx->copy));
+    }
   }
   MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->copy));
   return MOAO_OK;
 }
 
@@ -659,22 +698,40 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
     dT = ctx->ws_host_t.as<double>();
   }
   cudaStream_t s = ctx->stream;
+  if (!ctx->copy) MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  if (!ctx->inputs_ready)
+    MOAO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->inputs_ready, cudaEventDisableTiming));
   // Only the lower triangle of Cmm is read and only its lower triangle becomes
   // the factor: the column panels of the lower part go down and come back (the
   // panels' diagonal blocks carry their upper elements unchanged both ways).
+  // Ctm goes down on the copy stream while the factorisation runs (the solves
+  // wait for it), and the factor comes back on the copy stream while the solves
+  // run.
   MOAO_TRY(copy_lower_panels(dC, nmeas, Cmm, ldCmm, nmeas, nmeas, 0, false,
                              cudaMemcpyHostToDevice, s));
-  MOAO_CUDA_TRY(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice, s));
+  MOAO_CUDA_TRY(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice,
+                                ctx->copy));
+  MOAO_CUDA_TRY(cudaEventRecord(ctx->inputs_ready, ctx->copy));
+  ctx->wait_inputs = true;
+  ctx->host_factor = Cmm;
+  ctx->host_factor_ld = ldCmm;
   const moao_status st =
       moao_reconstructor(ctx, nmeas, nmeasts, dC, nmeas, dT, ldCtm, ngal, ctx->host_prec, rep);
+  const bool factor_sent = ctx->factor_done;
+  ctx->wait_inputs = false;
+  ctx->host_factor = nullptr;
+  ctx->factor_done = false;
+  // the stream must not run ahead of Ctm's copy on any path (errors included)
+  MOAO_CUDA_TRY(cudaStreamWaitEvent(s, ctx->inputs_ready, 0));
   // On a failed factorisation the reference has already overwritten Cmm
   // (partially) and leaves Ctm alone; mirror that.
-  if (st == MOAO_OK || st == MOAO_ERR_NOT_SPD)
+  if ((st == MOAO_OK || st == MOAO_ERR_NOT_SPD) && !factor_sent)
     MOAO_TRY(copy_lower_panels(Cmm, ldCmm, dC, nmeas, nmeas, nmeas, 0, false,
                                cudaMemcpyDeviceToHost, s));
   if (st == MOAO_OK)
     MOAO_CUDA_TRY(cudaMemcpyAsync(Ctm, dT, sizeof(double) * tspan, cudaMemcpyDeviceToHost, s));
   MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->copy));
   return st;
 }
 

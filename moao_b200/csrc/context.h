@@ -86,6 +86,18 @@ struct moao_ctx {
   int lookahead_sms = 8;
   cudaStream_t aux = nullptr;
   cudaEvent_t la_ev[2] = {};
+  // host-buffer entry points: device-to-host copies of finished column blocks
+  // on a second stream while the next block is computed (created on first use)
+  cudaStream_t copy = nullptr;
+  std::vector<cudaEvent_t> copy_ev;
+  // moao_reconstructor_host: Ctm arrives on the copy stream (the solves wait for
+  // inputs_ready), and the finished factor leaves for host_factor on the copy
+  // stream while the solves run; factor_done says it has been written to Cmm
+  bool wait_inputs = false;
+  cudaEvent_t inputs_ready = nullptr;
+  double* host_factor = nullptr;
+  long host_factor_ld = 0;
+  bool factor_done = false;
   // kernel timing
   bool timing = false;
   std::map<std::string, moao::FamilyStats> stats;
@@ -166,6 +178,11 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
 void release_batch_state(moao_ctx* ctx);
 // Writes the mixed factorisation's (FP32) factor into the lower triangle of Cmm.
 moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm);
+// The host-buffer path's overlap hooks: the stream waits for inputs that arrive on
+// the copy stream, and the finished lower factor in Cmm (ld n) goes back to the
+// host on the copy stream while the solves run.
+moao_status await_inputs(moao_ctx* ctx);
+moao_status factor_to_host(moao_ctx* ctx, const double* Cmm, long ldCmm, long n);
 // C (FP64, M x N, ldc) += alpha * A B^T from int8 Ozaki slices of the rows of
 // A (ta[0..nsa), 128-row boxes) and of B (tb[0..nsb), 256-row boxes), K columns,
 // keeping the slice products p + q + 2 <= dmax (0-based p, q); erow / ecol are

@@ -599,9 +599,18 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
       MOAO_TRY(mul_small_left(Sinv, nro, Y32, kYRows, n, Y2, s));
     }
     ctx->mx_factored_n = n;
+    // Cmm is not read after its int8 slices: a host-buffer caller without an
+    // accuracy target (whose fallback would need Cmm) gets the factor now, its
+    // copy back overlapping the solves
+    if (ctx->host_factor && !(ctx->acc_target > 0) && !ctx->keep_cmm && !graph) {
+      MOAO_TRY(cvt_f32_to_f64(A32, n, Cmm, ldCmm, n, n, true, s));
+      MOAO_TRY(factor_to_host(ctx, Cmm, ldCmm, n));
+      ctx->factor_done = true;
+    }
   }
   if (!graph) cudaEventRecord(ev[4], s);
   // ---- solve
+  MOAO_TRY(await_inputs(ctx));
   MOAO_TRY(cvt_f64_to_f32(Ctm, ldCtm, T32, m, m, n, false, s));
   MOAO_TRY(mixed_solve(ctx, n, m, T32, dinv, mp.xA, mp, W1, W2, xs, ldx, full, nsl, err, sc));
   if (nro > 0) {

@@ -114,6 +114,36 @@ moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, co
   return MOAO_OK;
 }
 
+moao_status await_inputs(moao_ctx* ctx) {
+  if (ctx->wait_inputs) {
+    MOAO_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->inputs_ready, 0));
+    ctx->wait_inputs = false;
+  }
+  return MOAO_OK;
+}
+
+// Column panels of the lower part of the n x n factor (device ld ldCmm) into the
+// host buffer (ld host_factor_ld), on the copy stream after the context stream's
+// work so far.
+moao_status factor_to_host(moao_ctx* ctx, const double* Cmm, long ldCmm, long n) {
+  if (ctx->copy_ev.empty()) {
+    cudaEvent_t e;
+    MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->copy_ev.push_back(e);
+  }
+  MOAO_CUDA_TRY(cudaEventRecord(ctx->copy_ev[0], ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamWaitEvent(ctx->copy, ctx->copy_ev[0], 0));
+  const long w = 512;
+  for (long c0 = 0; c0 < n; c0 += w) {
+    const long c1 = std::min(n, c0 + w);
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(ctx->host_factor + c0 * ctx->host_factor_ld + c0,
+                                    sizeof(double) * ctx->host_factor_ld, Cmm + c0 * ldCmm + c0,
+                                    sizeof(double) * ldCmm, sizeof(double) * (n - c0), c1 - c0,
+                                    cudaMemcpyDeviceToHost, ctx->copy));
+  }
+  return MOAO_OK;
+}
+
 // FP64 reconstructor: factor Cmm in place, then the solves of targets g0..ngal-1.
 moao_status reconstructor_fp64(moao_ctx* ctx, long nmeas, long nmeasts, double* d_Cmm, long ldCmm,
                                double* d_Ctm, long ldCtm, long g0, long ngal,
@@ -134,6 +164,11 @@ moao_status reconstructor_fp64(moao_ctx* ctx, long nmeas, long nmeasts, double* 
     return set_error(MOAO_ERR_NOT_SPD, "dpotrf: non-positive pivot at column " +
                                            std::to_string(info));
   }
+  if (ctx->host_factor) {  // the factor is final: back to the host beside the solves
+    MOAO_TRY(factor_to_host(ctx, d_Cmm, ldCmm, nmeas));
+    ctx->factor_done = true;
+  }
+  MOAO_TRY(await_inputs(ctx));
   for (long g = g0; g < ngal; ++g) {
     double* Ctm_g = d_Ctm + nmeas * nmeasts * g;
     MOAO_TRY(solve_right_f64(ctx, d_Cmm, ldCmm, nmeas, ctx->ws_dinv.as<double>(), Ctm_g, ldCtm,
@@ -170,6 +205,7 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
   if (nmeas == 0) return MOAO_OK;
   std::lock_guard<std::mutex> lk(ctx->mu);
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  ctx->factor_done = false;
   if (prec == MOAO_PREC_MIXED) {
     long g = 0;
     for (; g < ngal; ++g) {
@@ -184,7 +220,8 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
       ctx->mx_factored_n = -1;
       return reconstructor_fp64(ctx, nmeas, nmeasts, d_Cmm, ldCmm, d_Ctm, ldCtm, g, ngal, r);
     }
-    if (!ctx->keep_cmm) MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
+    if (!ctx->keep_cmm && !ctx->factor_done) MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));
+    if (ctx->factor_done) ctx->mx_factored_n = -1;  // A32 no longer matches what finish_mixed leaves
     MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return MOAO_OK;
   }

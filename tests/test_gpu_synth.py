@@ -2,7 +2,10 @@
 moao_intersample_create_synth) against the reference tooling's formulas
 (moao_b200.inputs, numpy): abs2fi and the telescope OTF within 1e-12 of their
 maxima (cuFFT against numpy's FFT, rounding only), idx exact, and a PSF from a
-synthesised intersample object equal to one built from the numpy tables."""
+synthesised intersample object within 1e-6 of one built from the numpy tables:
+the PSF's exponent multiplies the structure function by 2 (2 pi / lambda)^2 /
+(N dactupix)^2 (~1e8 at N = 512), which turns rounding-level differences of
+the tables into ~1e-7 of the PSF (measured 1.5e-7 at 10x10)."""
 import numpy as np
 import pytest
 
@@ -39,4 +42,4 @@ def test_psf_from_synthesised_object(ctx):
     check(lib().moao_intersample_process_host(h, Cvv.copy(order="F").ctypes.data, got.ctypes.data),
           "moao_intersample_process_host")
     lib().moao_intersample_destroy(h)
-    assert np.max(np.abs(got - want)) <= 1e-11 * np.max(np.abs(want))
+    assert np.max(np.abs(got - want)) <= 1e-6 * np.max(np.abs(want))
