@@ -55,7 +55,11 @@ constexpr int kErrSlices = 3;  // int8 slices of E's rows
 moao_status cee_cvv_mixed(moao_ctx* ctx, long nm, long nt, long nact, const double* Cmm,
                           long ldCmm, const double* Cpp, long ldCpp, double* Cpm, long ldCpm,
                           const double* R, long ldR, const double* Dx, long ldDx, double* Cee,
-                          long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp) {
+                          long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp,
+                          bool from_refinement) {
+  const bool use_state = from_refinement && ctx->rstate_valid && ctx->rstate_n == nm &&
+                         ctx->rstate_m == nt;
+  if (!use_state) ctx->rstate_valid = false;  // this call overwrites the state's buffers
   const long long h0 = helper_launches();
   cudaStream_t s = ctx->stream;
   const int ns = ctx->ozaki_slices;
@@ -104,30 +108,34 @@ moao_status cee_cvv_mixed(moao_ctx* ctx, long nm, long nt, long nact, const doub
     }
     for (int i = 0; i < kErrSlices; ++i)
       MOAO_TRY(make_tc_map(&taE[i], qc + (size_t)i * nt * ldq, kTcI8, nt, nm, ldq));
-    // slices of R's rows and of Ctm's rows
-    MOAO_TRY(ozaki_split_rows(R, ldR, nt, nm, ns, ea, qa, ldq, s));
+    // slices of R's rows (or the refinement's R_k) and of Ctm's rows
+    if (!use_state) MOAO_TRY(ozaki_split_rows(R, ldR, nt, nm, ns, ea, qa, ldq, s));
     MOAO_TRY(ozaki_split_rows(Cpm, ldCpm, nt, nm, ns, ec, qc, ldq, s));
     // Cee = sym(tril(Ctt)) - R Ctm^T
     MOAO_TRY(sym_from_lower(Cpp, ldCpp, Cee, ldCee, nt, s, &ctx->launches));
     MOAO_TRY(ozaki_gemm(ctx, taR, ns, tbC, ns, ns + 1, nt, nt, nm, -1.f, Cee, ldCee, ea, ec, err));
-    // E = Ctm - R sym(Cmm)
-    MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, nt * sizeof(double), Cpm, ldCpm * sizeof(double),
-                                    nt * sizeof(double), nm, cudaMemcpyDeviceToDevice, s));
-    MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, nm, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
-                             ldq, rid, off, s));
-    MOAO_TRY(ozaki_gemm(ctx, taR, ns, tbS, ns, ns + 1, nt, nm, nm, -1.f, E64, nt, ea, fb, err));
-    if (nro > 0) {  // the offsets' part of R Cmm
-      MOAO_TRY(range_sums(R, ldR, nt, off, RU, s));
-      MOAO_TRY(subtract_offset_products(E64, nt, nt, nm, RU, rid, off, s));
+    if (!use_state) {
+      // E = Ctm - R sym(Cmm) (the refinement state holds it for R_k)
+      MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, nt * sizeof(double), Cpm, ldCpm * sizeof(double),
+                                      nt * sizeof(double), nm, cudaMemcpyDeviceToDevice, s));
+      MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, nm, ns, fb, ctx->mx_colmax.as<unsigned long long>(),
+                               qb, ldq, rid, off, s));
+      MOAO_TRY(ozaki_gemm(ctx, taR, ns, tbS, ns, ns + 1, nt, nm, nm, -1.f, E64, nt, ea, fb, err));
+      if (nro > 0) {  // the offsets' part of R Cmm
+        MOAO_TRY(range_sums(R, ldR, nt, off, RU, s));
+        MOAO_TRY(subtract_offset_products(E64, nt, nt, nm, RU, rid, off, s));
+      }
     }
     // Cee -= E R^T (Ctm's slices are no longer needed: E's go in their place)
     MOAO_TRY(ozaki_split_rows(E64, nt, nt, nm, kErrSlices, ee, qc, ldq, s));
     MOAO_TRY(ozaki_gemm(ctx, taE, kErrSlices, tbR, ns, kErrSlices + 1, nt, nt, nm, -1.f, Cee,
                         ldCee, ee, ea, err));
-    // Cpm <- R Cmm = Ctm - E
-    sub_inplace_kernel<<<148 * 8, 256, 0, s>>>(Cpm, ldCpm, E64, nt, nt, nm);
-    ++ctx->launches;
-    MOAO_CUDA_TRY(cudaGetLastError());
+    if (!use_state) {
+      // Cpm <- R Cmm = Ctm - E
+      sub_inplace_kernel<<<148 * 8, 256, 0, s>>>(Cpm, ldCpm, E64, nt, nt, nm);
+      ++ctx->launches;
+      MOAO_CUDA_TRY(cudaGetLastError());
+    }
   } else if (nt > 0) {
     MOAO_TRY(sym_from_lower(Cpp, ldCpp, Cee, ldCee, nt, s, &ctx->launches));
   }

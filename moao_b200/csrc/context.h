@@ -98,6 +98,11 @@ struct moao_ctx {
   double* host_factor = nullptr;
   long host_factor_ld = 0;
   bool factor_done = false;
+  // After a mixed reconstructor whose refinement evaluated a residual, mx_qa /
+  // mx_ea hold the int8 slices of an R_k and mx_e64 its residual E_k = Ctm - R_k Cmm
+  // (nmeas rstate_n, nmeasts rstate_m): what a Cee from the refinement needs.
+  bool rstate_valid = false;
+  long rstate_n = 0, rstate_m = 0;
   // kernel timing
   bool timing = false;
   std::map<std::string, moao::FamilyStats> stats;
@@ -191,11 +196,16 @@ moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTenso
                        int dmax, long M, long N, long K, float alpha, double* C, long ldc,
                        const int* erow, const int* ecol, int* err);
 // Cee and Cvv with the int8 tensor cores (cee_mixed.cpp); same arguments and
-// in-place contract as moao_cee_cvv except that Cpp is left as given.
+// in-place contract as moao_cee_cvv except that Cpp is left as given. With
+// from_refinement and a matching refinement state on the context, Cee is
+// evaluated at that state's R_k and E_k (Cmm and R are then not read, Cpm is left
+// as given): Cee is stationary in R, so this differs from Cee at the final R by
+// second order in R_k's error.
 moao_status cee_cvv_mixed(moao_ctx* ctx, long nmeas, long nmeasts, long nact, const double* Cmm,
                           long ldCmm, const double* Cpp, long ldCpp, double* Cpm, long ldCpm,
                           const double* R, long ldR, const double* Dx, long ldDx, double* Cee,
-                          long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp);
+                          long ldCee, double* Cvv, long ldCvv, double* Tmp, long ldTmp,
+                          bool from_refinement = false);
 // R = B * L^-T * L^-1 in place on B (m x n, ldb) using the factor and dinv.
 moao_status solve_right_f64(moao_ctx* ctx, const double* L, long ldl, long n, const double* dinv,
                             double* B, long ldb, long m);

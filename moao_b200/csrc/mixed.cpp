@@ -629,7 +629,10 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   double* dnorm = ctx->mx_norm.as<double>();
   double ctm2 = 0, e2 = 0;
   if (!graph) MOAO_TRY(sumsq(ctx, Ctm, ldCtm, m, n, dnorm, &ctm2));
+  ctx->rstate_valid = false;
+  bool ran_residual = false;
   auto residual = [&]() -> moao_status {
+    ran_residual = true;
     // E = Ctm - R sym(Cmm) from the int8 slice products
     MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
                                     m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
@@ -702,6 +705,11 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   MOAO_CUDA_TRY(cudaMemcpy2DAsync(Ctm, ldCtm * sizeof(double), R64, m * sizeof(double),
                                   m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
   if (graph) return MOAO_OK;
+  // (slices of R_k, E_k) is a consistent pair: the guard's correction wrote into
+  // E64 only before its final residual
+  ctx->rstate_valid = ran_residual;
+  ctx->rstate_n = n;
+  ctx->rstate_m = m;
   cudaEventRecord(ev[6], s);
   int herr[2] = {0, 0};
   MOAO_CUDA_TRY(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));

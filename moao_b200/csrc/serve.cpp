@@ -204,9 +204,17 @@ moao_status run_request(moao_server* s, Slot& slot, Request& q, moao_solve_repor
     MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), Ctm2, (int)m, (int)n, 0, 0, (int)m, 3));
     MOAO_TRY(moao_matcov_tile(ctx, ss.tomo.get(), slot.ctt.as<double>(), (int)m, (int)m, 0, 0,
                               (int)m, 4));
-    MOAO_TRY(moao_cee_cvv_prec(ctx, n, m, a, Cmm, n, slot.ctt.as<double>(), m, Ctm2, m, Ctm, m,
-                               slot.dx.as<double>(), a, slot.cee.as<double>(), m,
-                               slot.cvv.as<double>(), a, Tmp, a, q.r.prec));
+    if (mixed && !rep->fallback) {
+      // Cee at the refinement's (R_k, E_k): no second R Cmm product (Cee is
+      // stationary in R; second-order difference from Cee at the returned R)
+      MOAO_TRY(cee_cvv_mixed(ctx, n, m, a, Cmm, n, slot.ctt.as<double>(), m, Ctm2, m, Ctm, m,
+                             slot.dx.as<double>(), a, slot.cee.as<double>(), m,
+                             slot.cvv.as<double>(), a, Tmp, a, true));
+    } else {
+      MOAO_TRY(moao_cee_cvv_prec(ctx, n, m, a, Cmm, n, slot.ctt.as<double>(), m, Ctm2, m, Ctm, m,
+                                 slot.dx.as<double>(), a, slot.cee.as<double>(), m,
+                                 slot.cvv.as<double>(), a, Tmp, a, q.r.prec));
+    }
     if (q.r.Cvv)
       MOAO_CUDA_TRY(cudaMemcpyAsync(q.r.Cvv, slot.cvv.as<double>(), bytes_of(a, a),
                                     cudaMemcpyDeviceToHost, cs));

@@ -218,6 +218,7 @@ moao_status moao_reconstructor(moao_ctx* ctx, long nmeas, long nmeasts, double* 
       // the mixed estimate missed the accuracy target: this and the remaining
       // targets from the FP64 path (Cmm and their Ctm are still as given)
       ctx->mx_factored_n = -1;
+      ctx->rstate_valid = false;
       return reconstructor_fp64(ctx, nmeas, nmeasts, d_Cmm, ldCmm, d_Ctm, ldCtm, g, ngal, r);
     }
     if (!ctx->keep_cmm && !ctx->factor_done) MOAO_TRY(finish_mixed(ctx, nmeas, d_Cmm, ldCmm));

@@ -106,3 +106,40 @@ def test_fp64_request_equals_direct_api(built, ctx):
     M.matcov_tile(T, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
     M.reconstructor(nm, nts, C, nm, T, nts, 1, ctx=ctx)
     assert rel(R.reshape(nm, nts).T, T) <= 1e-12
+
+
+def test_mixed_request_cvv_and_psf_against_fp64_oracle(built, cuda, ctx, tmp_path):
+    """A mixed request's Cvv comes from the refinement's last (R_k, E_k) pair
+    (Cee is stationary in R, so the shortcut moves it only to second order); its
+    R, Cvv and PSF against the FP64 oracle (oracle.reconstructor / cee_cvv /
+    intersample, the reference's steps) for a system registered with
+    synthesised PSF tables: R <= 1e-5, Cvv <= 1e-6 relative Frobenius, PSF
+    within 1e-6 of its peak."""
+    import oracle as O
+    sp, ap = P.config_scaled(16, 10)
+    d = str(tmp_path / "sys")
+    P.write_system(d, sp, ap)
+    sf, af = d + "/sys-params.txt", d + "/prof-1-atmos-night0.txt"
+    t = M.Tomo(sf, af)
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    nact, N, idx, a2, otf = M.intersample_inputs(t.info.nssp_ts, t.info.diam, t.info.obs, ctx=ctx)
+    Dx = I.make_dx(nact, nts, seed=7) * 0.2   # Strehl ~0.5 here, not the all-halo regime
+    with Server(slots=1, hbm_budget_gb=40.0) as srv:
+        sid = srv.add_system_synth(sf, af, Dx)
+        R = np.zeros(nm * nts)
+        Cvv = np.zeros(nact * nact)
+        psf = np.zeros(N * N)
+        prof = (np.array(ap.cn2), np.array(ap.h), np.array(ap.L0))
+        r = srv.wait(srv.submit(sid, *prof, prec="mixed", R=R, Cvv=Cvv, psf=psf))
+        assert r["status"] == 0, r
+    g = O.Geometry.from_tomo(t)
+    t.setTarget(0)
+    Cmm = O.matcov(g, nm, nm, 0, 0, 1, nthreads=8)
+    Ctm = O.matcov(g, nts, nm, 0, 0, 3, nthreads=8)
+    Ctt = O.matcov(g, nts, nts, 0, 0, 4, nthreads=8)
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    _, Cvv_ref, *_ = O.cee_cvv(Cmm, Ctt, Ctm, R_ref, Dx)
+    psf_ref = O.intersample(Cvv_ref, idx, a2, otf, t.info.nssp_ts + 1)
+    assert O.rel_fro(R.reshape(nts, nm, order="F"), R_ref) <= 1e-5
+    assert O.rel_fro(Cvv.reshape(nact, nact, order="F"), Cvv_ref) <= 1e-6
+    assert np.max(np.abs(psf.reshape(N, N) - psf_ref)) <= 1e-6 * np.max(np.abs(psf_ref))
