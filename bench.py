@@ -62,6 +62,9 @@ def parse():
                    help="batched uneven instances in one graph launch instead of the build loop")
     p.add_argument("--batch-count", type=int, default=256)
     p.add_argument("--batch-outputs", action="store_true", help="batch: copy every R out")
+    p.add_argument("--batch-packed", type=int, default=0,
+                   help="batch: nmeas bound of the instances packed into the tile-task kernel "
+                        "(0: autotuned, -1: none)")
     p.add_argument("--serve-slots", type=int, default=3)
     p.add_argument("--no-compare", action="store_true",
                    help="mixed path: skip timing the FP64 path beside it")
@@ -603,9 +606,10 @@ BATCH_METRIC = "batched uneven instances: reconstructor builds/s in one graph la
 def batch_main(args):
     """256 uneven instances (grids 20x20 to 50x50, 2-8 WFS + truth sensor, 1-20
     layers at U(0, 20 km), Dirichlet(1) fractions, r0 U(0.08, 0.2) m, L0 U(10, 50)
-    m, seeded) built in one CUDA graph launch with autotuned panel widths and
-    stream count, against the same instances built one after the other through
-    the direct API (FP64 path)."""
+    m, seeded) built in one CUDA graph launch with autotuned panel widths, stream
+    count and packed-instance bound (the small instances in the persistent
+    tile-task kernel), against the same instances built one after the other
+    through the direct API (FP64 path)."""
     import numpy as np
     import torch
     import moao_b200 as M
@@ -630,10 +634,11 @@ def batch_main(args):
     tune = B.autotune(list(classes.values()), prec, ctx=ctx)
     outs = [torch.empty(t.getNMeas() * t.getNMeasTS(), dtype=torch.float64, device="cuda")
             for t in tomos] if args.batch_outputs else None
-    B.batch_reconstructors(tomos, outs, prec=prec, ctx=ctx)  # warm-up (geometry upload, workspaces)
+    pm = args.batch_packed
+    B.batch_reconstructors(tomos, outs, prec=prec, packed_max=pm, ctx=ctx)  # warm-up
     runs = []
     for _ in range(max(1, args.steps)):
-        per, run = B.batch_reconstructors(tomos, outs, prec=prec, ctx=ctx)
+        per, run = B.batch_reconstructors(tomos, outs, prec=prec, packed_max=pm, ctx=ctx)
         runs.append(run)
     ms = float(np.median([r["ms_device"] for r in runs]))
     # sequential direct API on the same instances (FP64, default panel width), device time
@@ -672,6 +677,8 @@ def batch_main(args):
                                 f"(nmeas {int(nmeas.min())}-{int(nmeas.max())}, median {int(np.median(nmeas))})"),
                    "path": prec, "streams": run_last["streams_used"]},
         "graph_nodes": run_last["graph_nodes"], "graph_build_ms": run_last["ms_build"],
+        "packed": {"count": run_last["packed_count"], "tasks": run_last["packed_tasks"],
+                   "nmeas_bound": pm if pm else tune.get("packed_max")},
         "device_gb": run_last["device_gb"], "failed": run_last["failed"], "tuning": tune,
         "sequential_fp64_direct": None if seq_ms is None else {
             "ms": seq_ms, "builds_per_s": len(tomos) / (seq_ms / 1000.0),

@@ -115,6 +115,11 @@ moao_status moao_ctx_set_offsets_from_tomo(moao_ctx* ctx, const moao_tomo* tomo)
  * (default 8; 0 turns the lookahead off, at most 64). Same results either way;
  * turn it off when other work should have every SM. No reference counterpart. */
 moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int sms);
+/* SMs left to the next diagonal block in the last panels of the mixed
+ * factorisation, where the trailing update has shrunk (below 24,576 rows: the
+ * midpoint of the two settings, below 12,288: this one); values at or below the
+ * lookahead setting keep it throughout. No reference counterpart. */
+moao_status moao_ctx_set_lookahead_max(moao_ctx* ctx, int sms);
 
 /* Accuracy target of the mixed reconstructor (relative Frobenius error of R;
  * 0, the default, turns the check off). With a target, the mixed path also
@@ -399,7 +404,15 @@ void moao_server_destroy(moao_server* s);
  * captured as one CUDA graph over several streams and launched once. Each
  * stream keeps one Cmm / Ctm pair and workspace sized for its largest
  * instance, so device memory is streams x largest, not the sum. Instances run
- * longest first onto the least-loaded stream. No reference counterpart. */
+ * longest first onto the least-loaded stream.
+ * Instances with nmeas <= packed_max are instead packed into ONE persistent
+ * tile-task kernel (64 x 64 FP64 tiles; the factorisation and both solves of
+ * all of them as one level-sorted task list whose CTAs claim tasks from an
+ * atomic counter and wait on tile version counters with bounded waits), in a
+ * branch of the same graph beside the streams; they hold their own Cmm / Ctm.
+ * The tile-task DAG follows the reference's runtime-scheduled tile algorithm
+ * (chameleon/compute/reconstructor.cpp:27-55); the batch API itself has no
+ * reference counterpart. */
 typedef struct {
   const moao_tomo* tomo;  /* system, profile and target of this instance */
   double* d_R;            /* device out: nmeasts x nmeas (ld nmeasts), or NULL */
@@ -408,29 +421,47 @@ typedef struct {
   int status;             /* MOAO_OK, MOAO_ERR_NOT_SPD, MOAO_ERR_TIMEOUT, MOAO_ERR_BAD_ARG */
   int info;               /* failing Cholesky column */
   int nb_used, stream;
+  int packed;             /* 1: built by the persistent tile-task kernel (FP64) */
 } moao_batch_item;
 typedef struct {
   moao_prec prec;         /* mixed: fixed max_refine corrections, no residual checks */
   int streams;            /* most streams to use; 0: tuned (default 4) */
   double hbm_budget_gb;   /* device bytes for the streams' buffers; <= 0: 85% of free */
+  long packed_max;        /* nmeas bound of the packed instances; 0: tuned (default
+                             none), < 0: none */
   /* outputs */
   double ms_device;       /* device time of the graph launch */
   double ms_build;        /* host time to capture and instantiate the graph */
   long long graph_nodes;
   int streams_used, failed;
   double device_gb;       /* device bytes of the streams' buffers and workspaces */
+  int packed_count;       /* instances built by the tile-task kernel */
+  long long packed_tasks; /* tasks in its list */
 } moao_batch_opts;
 moao_status moao_batch_reconstructors(moao_ctx* ctx, int count, moao_batch_item* items,
                                       moao_batch_opts* opts);
 /* Autotuner: for each nmeas size class (< 2k, 4k, 8k, 16k, 32k, larger) present
  * in the samples, the panel width (from nb_candidates, default 128, 256, 384,
  * 512, 768, 1024; those above nmeas skipped) with the shortest measured
- * single-instance build, then the stream count
+ * single-instance build; then, from the smallest class up while it wins, the
+ * classes whose samples build faster together in the tile-task kernel (64 x 64
+ * tiles) than as graph instances (the packed_max bound); then the stream count
  * (2, 4, 8) with the shortest batch of all samples; stored on the context. */
 moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samples,
                           moao_prec prec, const int* nb_candidates, int ncand);
 /* Tuned (or default) panel width per size class (6 entries) and stream count. */
 moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, int* streams);
+/* The packed kernel's task list for instances of the given sizes, host-only (no
+ * GPU): 5 ints per task (instance, type, i, j, k; types 0..6 = POTRF(k),
+ * TRSM(i,k), UPDATE(i,j,k), forward update (r=i, c=j, source column k),
+ * forward diagonal (r=i, c=k), backward update (r=i, c=j, source column k),
+ * backward diagonal (r=i, c=k)), in the order the kernel claims them; at most
+ * cap tasks are written, *ntasks receives the total and *levels the number of
+ * DAG levels. For inspection and for replaying the schedule on the host. */
+moao_status moao_packed_task_list(int count, const long* nmeas, const long* nmeasts, int* tasks,
+                                  long cap, long* ntasks, int* levels);
+/* Tuned nmeas bound of the packed instances (0: none). */
+moao_status moao_tuning_get_packed(moao_ctx* ctx, moao_prec prec, long* packed_max);
 moao_status moao_tuning_save(moao_ctx* ctx, const char* path);
 moao_status moao_tuning_load(moao_ctx* ctx, const char* path);
 

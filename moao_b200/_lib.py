@@ -68,14 +68,16 @@ class ServerStats(C.Structure):
 
 class BatchItem(C.Structure):
     _fields_ = [("tomo", vp), ("d_R", vp), ("nb", i32), ("status", i32), ("info", i32),
-                ("nb_used", i32), ("stream", i32)]
+                ("nb_used", i32), ("stream", i32), ("packed", i32)]
 
 
 class BatchOpts(C.Structure):
     _fields_ = [("prec", i32), ("streams", i32), ("hbm_budget_gb", C.c_double),
+                ("packed_max", C.c_long),
                 ("ms_device", C.c_double),
                 ("ms_build", C.c_double), ("graph_nodes", C.c_longlong),
-                ("streams_used", i32), ("failed", i32), ("device_gb", C.c_double)]
+                ("streams_used", i32), ("failed", i32), ("device_gb", C.c_double),
+                ("packed_count", i32), ("packed_tasks", C.c_longlong)]
 
 
 # name -> (restype, argtypes)
@@ -103,6 +105,10 @@ SIGNATURES = {
     "moao_ctx_set_host_precision": (i32, [vp, i32]),
     "moao_ctx_set_wait_limit": (i32, [vp, C.c_longlong]),
     "moao_ctx_set_accuracy": (i32, [vp, C.c_double]),
+    "moao_ctx_set_lookahead_max": (i32, [vp, i32]),
+    "moao_tuning_get_packed": (i32, [vp, i32, C.POINTER(C.c_long)]),
+    "moao_packed_task_list": (i32, [i32, vp, vp, vp, C.c_long, C.POINTER(C.c_long),
+                                    C.POINTER(i32)]),
     "moao_intersample_inputs": (i32, [vp, i64, C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,
                                       vp]),
     "moao_intersample_create_synth": (i32, [vp, i64, C.c_double, C.c_double, C.c_double, vp]),

@@ -182,6 +182,11 @@ class Context:
         check(lib().moao_ctx_set_offsets_from_tomo(self._h, tomo.handle),
               "moao_ctx_set_offsets_from_tomo")
 
+    def set_lookahead_max(self, sms: int = 8):
+        """SMs left to the next diagonal block in the last panels (see
+        moao_ctx_set_lookahead_max)."""
+        check(lib().moao_ctx_set_lookahead_max(self._h, int(sms)), "moao_ctx_set_lookahead_max")
+
     def set_accuracy(self, target: float = 0.0):
         """Accuracy target of the mixed reconstructor (0: off); a miss makes the
         FP64 path compute R (report fallback = 1). See moao_ctx_set_accuracy."""

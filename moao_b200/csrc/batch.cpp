@@ -13,10 +13,16 @@
 // instances, whose kernels are short, overlap with each other and with the
 // large ones on the other streams.
 //
+// Instances up to a size bound (packed_max) are taken out of the streams and
+// built together by the persistent tile-task kernel (packed.cu) in a branch of
+// the same graph: their covariance launches, then one launch for all of their
+// factorisations and solves.
+//
 // Autotuner: per nmeas size class and precision, the panel width (the tile
-// size of the blocked factorisation) with the shortest measured build, and
-// the number of streams with the shortest measured batch; kept on the context
-// and saved to / loaded from a text file.
+// size of the blocked factorisation) with the shortest measured build, the
+// size bound of the packed instances, and the number of streams with the
+// shortest measured batch; kept on the context and saved to / loaded from a
+// text file.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -31,6 +37,7 @@
 
 #include "context.h"
 #include "moao_b200.h"
+#include "packed.h"
 
 namespace moao {
 namespace {
@@ -54,6 +61,7 @@ struct TuneEntry {
 struct moao_tuning {
   moao::TuneEntry entry[2][moao::kClasses];  // [prec][class]
   int streams[2] = {0, 0};
+  long packed[2] = {0, 0};  // nmeas bound of the packed instances (0: none)
 };
 
 namespace moao {
@@ -88,6 +96,15 @@ int tuned_streams(const moao_ctx* ctx, moao_prec prec) {
   return 4;
 }
 
+long tuned_packed(const moao_ctx* ctx, moao_prec prec) {
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  auto it = tuning_tables().find(ctx);
+  return it != tuning_tables().end() ? it->second.packed[prec == MOAO_PREC_MIXED] : 0;
+}
+
+// Size bound of class c (nmeas below it).
+long class_limit(int c) { return 2048L << c; }
+
 struct Inst {
   int item;
   long n, m;
@@ -95,6 +112,7 @@ struct Inst {
   double cost;
   const DevGeometry* g;
   int stream;
+  bool packed;
 };
 
 // Builds one instance on sub-context sc (stream sc->stream): covariances into
@@ -159,6 +177,8 @@ moao_status ensure_subs(moao_ctx* ctx, int S) {
 moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_batch_opts* o) {
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   const moao_prec prec = o->prec;
+  const long pmax = o->packed_max > 0 ? o->packed_max
+                                      : (o->packed_max == 0 ? tuned_packed(ctx, prec) : 0);
   std::vector<Inst> inst;
   for (int i = 0; i < count; ++i) {
     const Tomo_struct<double>& t = items[i].tomo->t;
@@ -173,12 +193,27 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     in.cost = n * n * n / 3 + n * n * m + 40.0 * t.atm.nLayer * n * (n / 2 + m);
     MOAO_TRY(device_geometry(ctx, items[i].tomo, &in.g));
     in.stream = 0;
+    in.packed = in.n <= pmax;
     inst.push_back(in);
   }
+  // packed instances: their own Cmm (ld n) and Ctm (into d_R when given), the
+  // plan's state; counted against the budget first
+  std::vector<int> pk;
+  size_t pk_bytes = 0, pk_data = 0;
+  for (int i = 0; i < count; ++i)
+    if (inst[i].packed) {
+      pk.push_back(i);
+      const size_t nn = (size_t)inst[i].n, mm = (size_t)inst[i].m;
+      pk_data += nn * nn + (items[i].d_R ? 0 : mm * nn);
+      pk_bytes += packed_workspace_bytes(inst[i].n, inst[i].m);
+    }
+  pk_bytes += sizeof(double) * pk_data;
+  const int ngraph = count - (int)pk.size();
   int S = o->streams > 0 ? o->streams : tuned_streams(ctx, prec);
-  S = std::max(1, std::min({S, count, 16}));
+  S = std::max(0, std::min({S, ngraph, 16}));
+  if (ngraph > 0) S = std::max(S, 1);
   // Device bytes of one instance: Cmm, Ctm and the workspace of its path.
-  MOAO_TRY(ensure_subs(ctx, S));
+  MOAO_TRY(ensure_subs(ctx, std::max(S, 1)));
   const moao_ctx* proto = sub_contexts(ctx)[0];
   auto bytes_of_inst = [&](const Inst& in) {
     size_t b = sizeof(double) * ((size_t)in.n * in.n + (size_t)in.m * in.n);
@@ -196,13 +231,17 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   size_t fr = 0, tot = 0, held = 0;
   MOAO_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
   for (moao_ctx* c : sub_contexts(ctx)) held += c->bytes_held();
-  const size_t budget = o->hbm_budget_gb > 0 ? (size_t)(o->hbm_budget_gb * 1e9)
-                                             : (size_t)(0.85 * (double)(fr + held));
+  const size_t budget_all = o->hbm_budget_gb > 0 ? (size_t)(o->hbm_budget_gb * 1e9)
+                                                 : (size_t)(0.85 * (double)(fr + held));
+  if (pk_bytes > budget_all)
+    return set_error(MOAO_ERR_OOM, "batch: the packed instances exceed the device budget");
+  const size_t budget = budget_all - pk_bytes;
   // Longest first onto the least-loaded stream; a new stream is opened only
   // while its first (largest) instance fits the budget, since a stream holds
   // buffers for its largest instance and instances arrive largest first.
-  std::vector<int> order(count);
-  std::iota(order.begin(), order.end(), 0);
+  std::vector<int> order;
+  for (int i = 0; i < count; ++i)
+    if (!inst[i].packed) order.push_back(i);
   std::sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].cost > inst[b].cost; });
   std::vector<double> load;
   std::vector<size_t> foot;
@@ -260,18 +299,26 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   // memory: per stream its largest Cmm / Ctm pair and workspace
   std::vector<moao_ctx*>& subs = sub_contexts(ctx);
   std::vector<DevBuf> cmm(S), ctm(S);
-  DevBuf status;
+  DevBuf status, pkbuf;
+  PackedPlan plan;
+  cudaStream_t ps = nullptr;  // the packed branch
   // DevBuf frees nothing by itself: release the batch's own buffers on every exit
   struct Release {
     std::vector<DevBuf>& a;
     std::vector<DevBuf>& b;
     DevBuf& c;
+    DevBuf& d;
+    PackedPlan& e;
+    cudaStream_t& f;
     ~Release() {
       for (DevBuf& x : a) x.release();
       for (DevBuf& x : b) x.release();
       c.release();
+      d.release();
+      e.release();
+      if (f) cudaStreamDestroy(f);
     }
-  } release_guard{cmm, ctm, status};
+  } release_guard{cmm, ctm, status, pkbuf, plan, ps};
   size_t total = 0;
   for (int k = 0; k < S; ++k) {
     moao_ctx* sc = subs[k];
@@ -329,9 +376,37 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   MOAO_TRY(status.ensure(3 * sizeof(int) * (size_t)count));
   MOAO_CUDA_TRY(cudaMemsetAsync(status.p, 0, 3 * sizeof(int) * (size_t)count, ctx->stream));
   MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  // packed instances: buffers and the task list (host work, before the capture)
+  std::vector<PackedInst> pv;
+  if (!pk.empty()) {
+    MOAO_TRY(pkbuf.ensure(sizeof(double) * std::max<size_t>(pk_data, 1)));
+    size_t off = 0;
+    for (int i : pk) {
+      PackedInst q;
+      q.n = inst[i].n;
+      q.m = inst[i].m;
+      q.A = pkbuf.as<double>() + off;
+      q.lda = q.n;
+      off += (size_t)q.n * q.n;
+      if (items[i].d_R) {
+        q.C = items[i].d_R;
+      } else {
+        q.C = pkbuf.as<double>() + off;
+        off += (size_t)q.m * q.n;
+      }
+      q.ldc = std::max(q.m, 1L);
+      q.info = status.as<int>() + 3 * (size_t)i;
+      pv.push_back(q);
+    }
+    MOAO_TRY(packed_prepare(pv, &plan, ctx->stream));
+    MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    total += pk_bytes;
+  }
 
-  // ---- capture: fork S streams from the context's stream, join at the end
-  std::vector<cudaEvent_t> ev(S + 1);
+  // ---- capture: fork S streams (and the packed branch) from the context's
+  // stream, join at the end. ev[S]: fork; ev[k]: stream k done; ev[S + 1]:
+  // packed branch done.
+  std::vector<cudaEvent_t> ev(S + 2);
   for (auto& e : ev) MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   auto destroy_events = [&] {
     for (auto& e : ev) cudaEventDestroy(e);
@@ -357,6 +432,22 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     }
     if (ce == cudaSuccess && st == MOAO_OK) ce = cudaEventRecord(ev[k], sc->stream);
     if (ce == cudaSuccess && st == MOAO_OK) ce = cudaStreamWaitEvent(s0, ev[k], 0);
+  }
+  if (ps && ce == cudaSuccess && st == MOAO_OK) {
+    ce = cudaStreamWaitEvent(ps, ev[S], 0);
+    for (size_t q = 0; q < pk.size() && ce == cudaSuccess && st == MOAO_OK; ++q) {
+      const Inst& in = inst[pk[q]];
+      st = launch_matcov(*in.g, pv[q].A, (int)in.n, (int)in.n, 0, 0, (int)pv[q].lda, 1, ps,
+                         &ctx->launches);
+      if (st == MOAO_OK && in.m > 0)
+        st = launch_matcov(*in.g, pv[q].C, (int)in.m, (int)in.n, 0, 0, (int)pv[q].ldc, 3, ps,
+                           &ctx->launches);
+    }
+    if (ce == cudaSuccess && st == MOAO_OK)
+      st = packed_launch(plan, ps, ctx->wait_polls, 2.0,
+                         &ctx->launches);
+    if (ce == cudaSuccess && st == MOAO_OK) ce = cudaEventRecord(ev[S + 1], ps);
+    if (ce == cudaSuccess && st == MOAO_OK) ce = cudaStreamWaitEvent(s0, ev[S + 1], 0);
   }
   cudaError_t ce_end = cudaStreamEndCapture(s0, &graph);
   for (int k = 0; k < S; ++k) subs[k]->graph_mode = false;
@@ -392,14 +483,19 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   if (ce != cudaSuccess) return set_error(MOAO_ERR_CUDA, std::string("batch graph launch: ") + cudaGetErrorString(ce));
   std::vector<int> hs(3 * (size_t)count);
   MOAO_CUDA_TRY(cudaMemcpy(hs.data(), status.p, hs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  int pk_err = 0;
+  if (!pk.empty())
+    MOAO_CUDA_TRY(cudaMemcpy(&pk_err, packed_error_flag(plan), sizeof(int), cudaMemcpyDeviceToHost));
   int failed = 0;
   for (const Inst& in : inst) {
     moao_batch_item& it = items[in.item];
     const int* f = &hs[3 * (size_t)in.item];
+    const bool timeout = f[1] || (in.packed && pk_err);
     it.info = f[0];
-    it.nb_used = in.nb;
-    it.stream = in.stream;
-    it.status = f[1] ? MOAO_ERR_TIMEOUT : (f[2] ? MOAO_ERR_BAD_ARG : (f[0] ? MOAO_ERR_NOT_SPD : MOAO_OK));
+    it.nb_used = in.packed ? 64 : in.nb;
+    it.stream = in.packed ? -1 : in.stream;
+    it.packed = in.packed ? 1 : 0;
+    it.status = timeout ? MOAO_ERR_TIMEOUT : (f[2] ? MOAO_ERR_BAD_ARG : (f[0] ? MOAO_ERR_NOT_SPD : MOAO_OK));
     failed += it.status != MOAO_OK;
   }
   o->ms_device = ms;
@@ -408,6 +504,8 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   o->streams_used = S;
   o->device_gb = total / 1e9;
   o->failed = failed;
+  o->packed_count = (int)pk.size();
+  o->packed_tasks = plan.ntasks;
   return MOAO_OK;
 }
 
@@ -466,8 +564,39 @@ moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samp
     for (int c = 0; c < kClasses; ++c)
       if (best_nb[c] > 0) t.entry[p][c].nb = best_nb[c];
   }
-  // stream count: the whole sample set as one batch
   std::vector<moao_batch_item> items(count);
+  // packed bound: from the smallest class up, while the class's samples build
+  // faster together in the tile-task kernel than as graph instances (classes
+  // below 8k only: the task list grows as (nmeas / 64)^3)
+  long packed = 0;
+  for (int c = 0; c < 3; ++c) {
+    std::vector<const moao_tomo*> cls;
+    for (int i = 0; i < count; ++i)
+      if (size_class(samples[i]->t.getNMeas()) == c) cls.push_back(samples[i]);
+    if (cls.empty()) continue;
+    double ms[2] = {0, 0};
+    for (int mode = 0; mode < 2; ++mode) {
+      for (int rep = 0; rep < 2; ++rep) {  // warm-up, then timed
+        for (size_t i = 0; i < cls.size(); ++i) {
+          items[i] = moao_batch_item{};
+          items[i].tomo = cls[i];
+        }
+        moao_batch_opts o{};
+        o.prec = prec;
+        o.streams = 2;
+        o.packed_max = mode ? class_limit(c) : -1;
+        MOAO_TRY(moao_batch_reconstructors(ctx, (int)cls.size(), items.data(), &o));
+        ms[mode] = o.ms_device;
+      }
+    }
+    if (ms[1] < ms[0]) packed = class_limit(c) - 1;
+    else break;
+  }
+  {
+    std::lock_guard<std::mutex> lk(tuning_mutex());
+    tuning_tables()[ctx].packed[p] = packed;
+  }
+  // stream count: the whole sample set as one batch
   double best = 1e300;
   int bestS = 4;
   for (int S : {2, 4, 8}) {
@@ -479,6 +608,7 @@ moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samp
     moao_batch_opts o{};
     o.prec = prec;
     o.streams = S;
+    o.packed_max = packed > 0 ? packed : -1;
     MOAO_TRY(moao_batch_reconstructors(ctx, count, items.data(), &o));
     if (o.ms_device < best) {
       best = o.ms_device;
@@ -502,16 +632,24 @@ moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, in
   return MOAO_OK;
 }
 
+moao_status moao_tuning_get_packed(moao_ctx* ctx, moao_prec prec, long* packed_max) {
+  if (!ctx || !packed_max) return set_error(MOAO_ERR_BAD_ARG, "tuning_get_packed: null");
+  *packed_max = tuned_packed(ctx, prec);
+  return MOAO_OK;
+}
+
 moao_status moao_tuning_save(moao_ctx* ctx, const char* path) {
   if (!ctx || !path) return set_error(MOAO_ERR_BAD_ARG, "tuning_save: null");
   std::ofstream f(path);
   if (!f) return set_error(MOAO_ERR_IO, std::string("tuning_save: cannot create ") + path);
-  f << "# moao_b200 tuning: prec class nb / prec streams\n";
+  f << "# moao_b200 tuning: prec class nb / prec streams / prec packed-nmeas-bound\n";
   for (int p = 0; p < 2; ++p) {
     int nbs[kClasses], S = 0;
-    moao_tuning_get(ctx, p ? MOAO_PREC_MIXED : MOAO_PREC_FP64, nbs, &S);
+    const moao_prec pr = p ? MOAO_PREC_MIXED : MOAO_PREC_FP64;
+    moao_tuning_get(ctx, pr, nbs, &S);
     for (int c = 0; c < kClasses; ++c) f << "nb " << p << " " << c << " " << nbs[c] << "\n";
     f << "streams " << p << " " << S << "\n";
+    f << "packed " << p << " " << tuned_packed(ctx, pr) << "\n";
   }
   return f ? MOAO_OK : set_error(MOAO_ERR_IO, "tuning_save: write failed");
 }
@@ -533,6 +671,8 @@ moao_status moao_tuning_load(moao_ctx* ctx, const char* path) {
       t.entry[p][c].nb = v;
     else if (key == "streams" && (is >> p >> v) && p >= 0 && p < 2 && v >= 1 && v <= 16)
       t.streams[p] = v;
+    else if (key == "packed" && (is >> p >> v) && p >= 0 && p < 2 && v >= 0)
+      t.packed[p] = v;
     else
       return set_error(MOAO_ERR_IO, "tuning_load: bad line: " + line);
   }

@@ -550,6 +550,14 @@ moao_status moao_ctx_set_wait_limit(moao_ctx* c, long long polls) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_lookahead_max(moao_ctx* c, int sms) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: null");
+  if (sms < 0 || sms > 120) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: 0..120 SMs");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->lookahead_max = sms;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_host_precision(moao_ctx* c, moao_prec prec) {
   if (!c || (prec != MOAO_PREC_FP64 && prec != MOAO_PREC_MIXED))
     return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_precision: FP64 or MIXED");

@@ -84,6 +84,7 @@ struct moao_ctx {
   // (created on first use) while the trailing update leaves this many SMs free
   // (0: no lookahead).
   int lookahead_sms = 8;
+  int lookahead_max = 8;  // SMs left to it in the last panels (moao_ctx_set_lookahead_max)
   cudaStream_t aux = nullptr;
   cudaEvent_t la_ev[2] = {};
   // host-buffer entry points: device-to-host copies of finished column blocks

@@ -145,6 +145,17 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
   return tc_gemm(g, ctx->stream, &ctx->launches);
 }
 
+// SMs left to the next diagonal block beside the rest of the trailing update:
+// ctx->lookahead_sms while the update is long, growing to ctx->lookahead_max as
+// the trailing matrix shrinks (below 24,576 rows the update no longer outlasts
+// the diagonal block, whose small GEMMs then set the pace).
+int lookahead_for(const moao_ctx* ctx, long rest) {
+  const int base = ctx->lookahead_sms, top = std::max(base, ctx->lookahead_max);
+  if (rest >= 24576) return base;
+  if (rest >= 12288) return std::min(top, std::max(base, (base + top) / 2));
+  return top;
+}
+
 // fp16 operands: power-of-two scales of the stored factor and solve slices.
 //   erp: per panel p, the row exponents of L(:, panel p) (erp + p*n, indexed by row)
 //   ecf: per column j of L, its exponent (the Lc copy, row j = L(:, j))
@@ -566,7 +577,7 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
         MOAO_TRY(tc_update(ctx, mp.lrA, (int)(k1 + kb1), (int)k0, mp.lrB, (int)(k1 + kb1), (int)k0,
                            nk, full, r2, r2, A32 + (k1 + kb1) + (k1 + kb1) * n, n, true, err,
                            (double)r2 * r2 * kb, er ? er + kb1 : nullptr, er ? er + kb1 : nullptr,
-                           std::max(1, nsm - ctx->lookahead_sms)));
+                           std::max(1, nsm - lookahead_for(ctx, rest))));
         MOAO_CUDA_TRY(cudaStreamWaitEvent(s, ctx->la_ev[1], 0));
       } else {
         MOAO_TRY(tc_update(ctx, mp.lrA, (int)k1, (int)k0, mp.lrB, (int)k1, (int)k0, nk, full, rest,
