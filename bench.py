@@ -62,6 +62,10 @@ def parse():
                    help="batched uneven instances in one graph launch instead of the build loop")
     p.add_argument("--batch-count", type=int, default=256)
     p.add_argument("--batch-outputs", action="store_true", help="batch: copy every R out")
+    p.add_argument("--batch-nssp", default="20,50",
+                   help="batch: range of subapertures across the instances (lo,hi)")
+    p.add_argument("--batch-no-tune", action="store_true",
+                   help="batch: default panel widths and streams instead of the autotuner")
     p.add_argument("--batch-packed", type=int, default=0,
                    help="batch: nmeas bound of the instances packed into the tile-task kernel "
                         "(0: autotuned, -1: none)")
@@ -618,9 +622,10 @@ def batch_main(args):
 
     torch.cuda.init()
     rng = np.random.default_rng(4096)
+    lo, hi = (int(x) for x in args.batch_nssp.split(","))
     tomos = []
     for i in range(args.batch_count):
-        sp, ap = P.config_random(rng)
+        sp, ap = P.config_random(rng, nssp_range=(lo, hi))
         d = tempfile.mkdtemp(prefix=f"moao_batch_{i}_")
         P.write_system(d, sp, ap)
         tomos.append(M.Tomo(os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt")))
@@ -631,7 +636,8 @@ def batch_main(args):
     classes = {}
     for t in tomos:
         classes.setdefault(int(np.log2(max(t.getNMeas(), 1024) / 1024)), t)
-    tune = B.autotune(list(classes.values()), prec, ctx=ctx)
+    tune = B.tuning(prec, ctx=ctx) if args.batch_no_tune else \
+        B.autotune(list(classes.values()), prec, ctx=ctx)
     outs = [torch.empty(t.getNMeas() * t.getNMeasTS(), dtype=torch.float64, device="cuda")
             for t in tomos] if args.batch_outputs else None
     pm = args.batch_packed
@@ -670,10 +676,14 @@ def batch_main(args):
         torch.cuda.synchronize()
         seq_ms = e0.elapsed_time(e1)
         ctx2.close()
+    nts_all = np.array([t.getNMeasTS() for t in tomos], dtype=np.float64)
+    n_all = nmeas.astype(np.float64)
+    flop = float(np.sum(n_all ** 3 / 3 + 2 * nts_all * n_all ** 2))  # POTRF + 2 TRSM per instance
     line = {
         "metric": BATCH_METRIC, "value": len(tomos) / (ms / 1000.0), "unit": "builds/s",
+        "fp64_flop_per_batch": flop, "fp64_equivalent_tflops": flop / (ms * 1e9),
         "n_gpus": 1, "higher_is_better": True, "ms_per_batch": ms,
-        "config": {"workload": (f"{len(tomos)} uneven instances: grids 20-50, 2-8 WFS, 1-20 layers "
+        "config": {"workload": (f"{len(tomos)} uneven instances: grids {lo}-{hi}, 2-8 WFS, 1-20 layers "
                                 f"(nmeas {int(nmeas.min())}-{int(nmeas.max())}, median {int(np.median(nmeas))})"),
                    "path": prec, "streams": run_last["streams_used"]},
         "graph_nodes": run_last["graph_nodes"], "graph_build_ms": run_last["ms_build"],
