@@ -77,7 +77,8 @@ def parse():
                    help="skip the measured CPU-vs-GPU full builds of the small systems")
     p.add_argument("--e2e-steps", type=int, default=5, help="builds timed through the host path")
     p.add_argument("--probe", default=None,
-                   choices=["matcov_ctm", "build_fp64", "build_mixed", "cee_fp64", "cee_mixed"],
+                   choices=["matcov_ctm", "build_fp64", "build_mixed", "cee_fp64", "cee_mixed",
+                            "gemm_tiles"],
                    help="run one stage once on the ELT geometry at --nssp subapertures (for ncu)")
     p.add_argument("--nssp", type=int, default=37, help="probe: subapertures across (64 = ELT)")
     return p.parse_args()
@@ -720,6 +721,42 @@ def probe_main(args):
     nm, nts = t.getNMeas(), t.getNMeasTS()
     Ctm = torch.empty((nm, nts), dtype=torch.float64, device="cuda")
     t0 = time.perf_counter()
+    if args.probe == "gemm_tiles":
+        # FP64 builds with each tile configuration of the large products: the
+        # gemm_f64 family's rate (kernel timing) against cuBLAS DGEMM
+        Cmm = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
+        peak = fp64_peak_tflops(torch)
+        res = []
+        for cfg in range(4):
+            ctx.set_gemm_tile(cfg)
+            rates, builds, leaf_us = [], [], []
+            for rep in range(4):
+                M.matcov_tile(Cmm, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+                M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+                torch.cuda.synchronize()
+                ctx.set_kernel_timing(True)
+                ctx.reset_kernel_stats()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                M.reconstructor(nm, nts, Cmm, nm, Ctm, nts, 1, prec="fp64", ctx=ctx)
+                e1.record()
+                torch.cuda.synchronize()
+                st = ctx.kernel_stats("gemm_f64")
+                lf = ctx.kernel_stats("potrf_leaf")
+                ctx.set_kernel_timing(False)
+                if rep:
+                    rates.append(st["work"] / st["ms"] / 1e9)
+                    builds.append(e0.elapsed_time(e1))
+                    leaf_us.append(1000.0 * lf["ms"] / max(lf["launches"], 1))
+            res.append({"cfg": cfg, "gemm_tflops": float(np.median(rates)),
+                        "of_cublas": float(np.median(rates)) / peak,
+                        "build_ms": float(np.median(builds)),
+                        "leaf_us_per_launch": float(np.median(leaf_us))})
+        ctx.set_gemm_tile(1)
+        print(json.dumps({"probe": "gemm_tiles", "nssp": args.nssp, "nmeas": nm,
+                          "leaf_threads": os.environ.get("MOAO_LEAF_THREADS", "default"),
+                          "cublas_dgemm_tflops": peak, "configs": res}), flush=True)
+        return 0
     if args.probe == "matcov_ctm":
         M.matcov_tile(Ctm, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
     else:

@@ -120,6 +120,12 @@ moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int sms);
  * midpoint of the two settings, below 12,288: this one); values at or below the
  * lookahead setting keep it throughout. No reference counterpart. */
 moao_status moao_ctx_set_lookahead_max(moao_ctx* ctx, int sms);
+/* Tile configuration of the large FP64 products (128 x 64 CTA tiles, 8 warps):
+ * 0: K 16 per stage, 4-stage cp.async ring, two CTAs per SM; 1: K 32, 2 stages,
+ * two CTAs per SM (default); 2: K 32, 3 stages, one CTA per SM; 3: K 16,
+ * 6 stages, one CTA per SM. Bitwise the same results. The batch autotuner picks
+ * it per size class. No reference counterpart. */
+moao_status moao_ctx_set_gemm_tile(moao_ctx* ctx, int cfg);
 
 /* Accuracy target of the mixed reconstructor (relative Frobenius error of R;
  * 0, the default, turns the check off). With a target, the mixed path also
@@ -429,6 +435,8 @@ typedef struct {
   double hbm_budget_gb;   /* device bytes for the streams' buffers; <= 0: 85% of free */
   long packed_max;        /* nmeas bound of the packed instances; 0: tuned (default
                              none), < 0: none */
+  int gemm_tile;          /* FP64 tile configuration + 1 for every instance
+                             (moao_ctx_set_gemm_tile); 0: tuned per size class */
   /* outputs */
   double ms_device;       /* device time of the graph launch */
   double ms_build;        /* host time to capture and instantiate the graph */
@@ -443,7 +451,8 @@ moao_status moao_batch_reconstructors(moao_ctx* ctx, int count, moao_batch_item*
 /* Autotuner: for each nmeas size class (< 2k, 4k, 8k, 16k, 32k, larger) present
  * in the samples, the panel width (from nb_candidates, default 128, 256, 384,
  * 512, 768, 1024; those above nmeas skipped) with the shortest measured
- * single-instance build; then, from the smallest class up while it wins, the
+ * single-instance build, then at that width the FP64 tile configuration
+ * (moao_ctx_set_gemm_tile) with the shortest build; then, from the smallest class up while it wins, the
  * classes whose samples build faster together in the tile-task kernel (64 x 64
  * tiles) than as graph instances (the packed_max bound); then the stream count
  * (2, 4, 8) with the shortest batch of all samples; stored on the context. */
@@ -460,6 +469,8 @@ moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, in
  * DAG levels. For inspection and for replaying the schedule on the host. */
 moao_status moao_packed_task_list(int count, const long* nmeas, const long* nmeasts, int* tasks,
                                   long cap, long* ntasks, int* levels);
+/* Tuned FP64 tile configuration per size class (6 entries). */
+moao_status moao_tuning_get_gemm(moao_ctx* ctx, moao_prec prec, int* cfg_per_class);
 /* Tuned nmeas bound of the packed instances (0: none). */
 moao_status moao_tuning_get_packed(moao_ctx* ctx, moao_prec prec, long* packed_max);
 moao_status moao_tuning_save(moao_ctx* ctx, const char* path);

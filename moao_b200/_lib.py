@@ -73,7 +73,7 @@ class BatchItem(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("prec", i32), ("streams", i32), ("hbm_budget_gb", C.c_double),
-                ("packed_max", C.c_long),
+                ("packed_max", C.c_long), ("gemm_tile", i32),
                 ("ms_device", C.c_double),
                 ("ms_build", C.c_double), ("graph_nodes", C.c_longlong),
                 ("streams_used", i32), ("failed", i32), ("device_gb", C.c_double),
@@ -106,7 +106,9 @@ SIGNATURES = {
     "moao_ctx_set_wait_limit": (i32, [vp, C.c_longlong]),
     "moao_ctx_set_accuracy": (i32, [vp, C.c_double]),
     "moao_ctx_set_lookahead_max": (i32, [vp, i32]),
+    "moao_ctx_set_gemm_tile": (i32, [vp, i32]),
     "moao_tuning_get_packed": (i32, [vp, i32, C.POINTER(C.c_long)]),
+    "moao_tuning_get_gemm": (i32, [vp, i32, vp]),
     "moao_packed_task_list": (i32, [i32, vp, vp, vp, C.c_long, C.POINTER(C.c_long),
                                     C.POINTER(i32)]),
     "moao_intersample_inputs": (i32, [vp, i64, C.c_double, C.c_double, C.c_double, vp, vp, vp, vp,

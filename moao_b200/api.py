@@ -182,6 +182,11 @@ class Context:
         check(lib().moao_ctx_set_offsets_from_tomo(self._h, tomo.handle),
               "moao_ctx_set_offsets_from_tomo")
 
+    def set_gemm_tile(self, cfg: int = 1):
+        """Tile configuration of the large FP64 products (see
+        moao_ctx_set_gemm_tile); same results."""
+        check(lib().moao_ctx_set_gemm_tile(self._h, int(cfg)), "moao_ctx_set_gemm_tile")
+
     def set_lookahead_max(self, sms: int = 8):
         """SMs left to the next diagonal block in the last panels (see
         moao_ctx_set_lookahead_max)."""

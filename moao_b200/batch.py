@@ -45,7 +45,7 @@ def batch_reconstructors(tomos: Sequence[Tomo], outputs=None, prec: str = "fp64"
             "packed": bool(items[i].packed)}
            for i in range(n)]
     run = {k: getattr(opts, k) for k, _ in BatchOpts._fields_
-           if k not in ("prec", "streams", "hbm_budget_gb", "packed_max")}
+           if k not in ("prec", "streams", "hbm_budget_gb", "packed_max", "gemm_tile")}
     return per, run
 
 
@@ -70,7 +70,10 @@ def tuning(prec: str = "fp64", ctx: Optional[Context] = None) -> dict:
     classes = ["<2k", "2k-4k", "4k-8k", "8k-16k", "16k-32k", ">=32k"]
     pm = C.c_long()
     check(lib().moao_tuning_get_packed(ctx.handle, PREC[prec], C.byref(pm)), "moao_tuning_get_packed")
-    return {"nb": dict(zip(classes, list(nbs))), "streams": s.value, "packed_max": pm.value}
+    g = (C.c_int * 6)()
+    check(lib().moao_tuning_get_gemm(ctx.handle, PREC[prec], C.cast(g, C.c_void_p)), "moao_tuning_get_gemm")
+    return {"nb": dict(zip(classes, list(nbs))), "streams": s.value, "packed_max": pm.value,
+            "gemm_tile": dict(zip(classes, list(g)))}
 
 
 def tuning_save(path: str, ctx: Optional[Context] = None):

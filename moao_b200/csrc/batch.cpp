@@ -37,6 +37,7 @@
 
 #include "context.h"
 #include "moao_b200.h"
+#include "dense.h"
 #include "packed.h"
 
 namespace moao {
@@ -51,7 +52,8 @@ int size_class(long n) {
 }
 
 struct TuneEntry {
-  int nb = 0;  // 0: not tuned
+  int nb = 0;     // 0: not tuned
+  int gemm = 1;   // tile configuration of the large FP64 products (GemmArgs::cfg)
 };
 
 }  // namespace
@@ -88,6 +90,13 @@ int tuned_nb(const moao_ctx* ctx, moao_prec prec, long n) {
   return default_nb(n);
 }
 
+int tuned_gemm(const moao_ctx* ctx, moao_prec prec, long n) {
+  std::lock_guard<std::mutex> lk(tuning_mutex());
+  auto it = tuning_tables().find(ctx);
+  if (it != tuning_tables().end()) return it->second.entry[prec == MOAO_PREC_MIXED][size_class(n)].gemm;
+  return 1;
+}
+
 int tuned_streams(const moao_ctx* ctx, moao_prec prec) {
   std::lock_guard<std::mutex> lk(tuning_mutex());
   auto it = tuning_tables().find(ctx);
@@ -109,6 +118,7 @@ struct Inst {
   int item;
   long n, m;
   int nb;
+  int gemm;
   double cost;
   const DevGeometry* g;
   int stream;
@@ -122,6 +132,7 @@ moao_status enqueue_instance(moao_ctx* sc, const moao_tomo* tomo, const Inst& in
   cudaStream_t s = sc->stream;
   const long n = in.n, m = in.m;
   sc->nb = in.nb;
+  sc->gemm_cfg = in.gemm;
   MOAO_TRY(launch_matcov(*in.g, Cmm, (int)n, (int)n, 0, 0, (int)n, 1, s, &sc->launches));
   MOAO_TRY(launch_matcov(*in.g, Ctm, (int)m, (int)n, 0, 0, (int)m, 3, s, &sc->launches));
   int* d_info = sc->ws_info.as<int>();
@@ -189,6 +200,7 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     in.nb = items[i].nb > 0 ? items[i].nb : tuned_nb(ctx, prec, in.n);
     if (in.nb % 64 || in.nb < 64 || in.nb > 2048)
       return set_error(MOAO_ERR_BAD_ARG, "batch: panel width must be a multiple of 64 in [64, 2048]");
+    in.gemm = o->gemm_tile > 0 ? o->gemm_tile - 1 : tuned_gemm(ctx, prec, in.n);
     const double n = (double)in.n, m = (double)in.m;
     in.cost = n * n * n / 3 + n * n * m + 40.0 * t.atm.nLayer * n * (n / 2 + m);
     MOAO_TRY(device_geometry(ctx, items[i].tomo, &in.g));
@@ -564,6 +576,33 @@ moao_status moao_autotune(moao_ctx* ctx, int count, const moao_tomo* const* samp
     for (int c = 0; c < kClasses; ++c)
       if (best_nb[c] > 0) t.entry[p][c].nb = best_nb[c];
   }
+  // FP64 tile configuration of the large products per class, at the class's panel width
+  {
+    std::vector<double> best_g(kClasses, 1e300);
+    std::vector<int> cfg_of(kClasses, 0);
+    for (int i = 0; i < count; ++i) {
+      const int c = size_class(samples[i]->t.getNMeas());
+      for (int g = 0; g < kGemmConfigs; ++g) {
+        moao_batch_item it{};
+        it.tomo = samples[i];
+        moao_batch_opts o{};
+        o.prec = prec;
+        o.streams = 1;
+        o.packed_max = -1;
+        o.gemm_tile = g + 1;
+        MOAO_TRY(moao_batch_reconstructors(ctx, 1, &it, &o));  // warm-up
+        MOAO_TRY(moao_batch_reconstructors(ctx, 1, &it, &o));
+        if (o.ms_device < best_g[c]) {
+          best_g[c] = o.ms_device;
+          cfg_of[c] = g;
+        }
+      }
+    }
+    std::lock_guard<std::mutex> lk(tuning_mutex());
+    moao_tuning& t = tuning_tables()[ctx];
+    for (int c = 0; c < kClasses; ++c)
+      if (best_g[c] < 1e300) t.entry[p][c].gemm = cfg_of[c];
+  }
   std::vector<moao_batch_item> items(count);
   // packed bound: from the smallest class up, while the class's samples build
   // faster together in the tile-task kernel than as graph instances (classes
@@ -632,6 +671,15 @@ moao_status moao_tuning_get(moao_ctx* ctx, moao_prec prec, int* nb_per_class, in
   return MOAO_OK;
 }
 
+moao_status moao_tuning_get_gemm(moao_ctx* ctx, moao_prec prec, int* cfg_per_class) {
+  if (!ctx || !cfg_per_class) return set_error(MOAO_ERR_BAD_ARG, "tuning_get_gemm: null");
+  for (int c = 0; c < kClasses; ++c) {
+    const long n = c == 0 ? 1024 : (1024L << c);
+    cfg_per_class[c] = tuned_gemm(ctx, prec, n);
+  }
+  return MOAO_OK;
+}
+
 moao_status moao_tuning_get_packed(moao_ctx* ctx, moao_prec prec, long* packed_max) {
   if (!ctx || !packed_max) return set_error(MOAO_ERR_BAD_ARG, "tuning_get_packed: null");
   *packed_max = tuned_packed(ctx, prec);
@@ -642,7 +690,8 @@ moao_status moao_tuning_save(moao_ctx* ctx, const char* path) {
   if (!ctx || !path) return set_error(MOAO_ERR_BAD_ARG, "tuning_save: null");
   std::ofstream f(path);
   if (!f) return set_error(MOAO_ERR_IO, std::string("tuning_save: cannot create ") + path);
-  f << "# moao_b200 tuning: prec class nb / prec streams / prec packed-nmeas-bound\n";
+  f << "# moao_b200 tuning: nb prec class width / streams prec n / packed prec nmeas-bound /"
+       " gemm prec class tile-configuration\n";
   for (int p = 0; p < 2; ++p) {
     int nbs[kClasses], S = 0;
     const moao_prec pr = p ? MOAO_PREC_MIXED : MOAO_PREC_FP64;
@@ -650,6 +699,9 @@ moao_status moao_tuning_save(moao_ctx* ctx, const char* path) {
     for (int c = 0; c < kClasses; ++c) f << "nb " << p << " " << c << " " << nbs[c] << "\n";
     f << "streams " << p << " " << S << "\n";
     f << "packed " << p << " " << tuned_packed(ctx, pr) << "\n";
+    int g[kClasses];
+    moao_tuning_get_gemm(ctx, pr, g);
+    for (int c = 0; c < kClasses; ++c) f << "gemm " << p << " " << c << " " << g[c] << "\n";
   }
   return f ? MOAO_OK : set_error(MOAO_ERR_IO, "tuning_save: write failed");
 }
@@ -673,6 +725,9 @@ moao_status moao_tuning_load(moao_ctx* ctx, const char* path) {
       t.streams[p] = v;
     else if (key == "packed" && (is >> p >> v) && p >= 0 && p < 2 && v >= 0)
       t.packed[p] = v;
+    else if (key == "gemm" && (is >> p >> c >> v) && p >= 0 && p < 2 && c >= 0 && c < kClasses &&
+             v >= 0 && v < kGemmConfigs)
+      t.entry[p][c].gemm = v;
     else
       return set_error(MOAO_ERR_IO, "tuning_load: bad line: " + line);
   }

@@ -550,6 +550,14 @@ moao_status moao_ctx_set_wait_limit(moao_ctx* c, long long polls) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_gemm_tile(moao_ctx* c, int cfg) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_gemm_tile: null");
+  if (cfg < 0 || cfg >= kGemmConfigs) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_gemm_tile: 0..3");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->gemm_cfg = cfg;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_lookahead_max(moao_ctx* c, int sms) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: null");
   if (sms < 0 || sms > 120) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: 0..120 SMs");

@@ -85,6 +85,7 @@ struct moao_ctx {
   // (0: no lookahead).
   int lookahead_sms = 8;
   int lookahead_max = 8;  // SMs left to it in the last panels (moao_ctx_set_lookahead_max)
+  int gemm_cfg = 1;       // tile configuration of the large FP64 products (GemmArgs::cfg)
   cudaStream_t aux = nullptr;
   cudaEvent_t la_ev[2] = {};
   // host-buffer entry points: device-to-host copies of finished column blocks

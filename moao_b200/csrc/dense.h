@@ -24,7 +24,11 @@ struct GemmArgs {
   double* C = nullptr;        // M x N, column-major, ldc
   long ldc = 0;
   bool lowerC = false;        // write only C(i, j) with i >= j (SYRK / SYR2K)
+  int cfg = 1;                // tile configuration of the large products (128x64 CTA tiles;
+                              // 0: K 16 per stage, 4 stages; 1: K 32, 2 stages (default);
+                              // 2: K 32, 3 stages; 3: K 16, 6 stages)
 };
+constexpr int kGemmConfigs = 4;
 
 // C = alpha * A * op(B) + beta * C in FP64 on the DMMA tensor-core path.
 moao_status gemm_f64(const GemmArgs& g, cudaStream_t s, long long* launches);

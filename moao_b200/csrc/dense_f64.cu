@@ -21,8 +21,6 @@
 namespace moao {
 namespace {
 
-constexpr int BK = 16;
-constexpr int STAGES = 4;
 constexpr int PAD_MN = 4;  // doubles of padding on m/n-contiguous rows
 constexpr int PAD_K = 4;   // doubles of padding on k-contiguous rows
 
@@ -32,10 +30,12 @@ constexpr int PAD_K = 4;   // doubles of padding on k-contiguous rows
 // products: 26.2 TF/s on the ELT FP64 build against 21.4 for 128x128 tiles with
 // one CTA per SM and 24.4 for 128x64 with 4 warps of 64x32. 64x64 (4 warps of
 // 32x32) when even that would leave most SMs idle (the small products of the
-// diagonal-block recursion).
-template <int BM_, int BN_, int WM_>
+// diagonal-block recursion). BK (K per pipeline stage, a multiple of 16) and
+// STAGES (the cp.async ring) are the other dimensions a configuration sets
+// (GemmArgs::cfg, chosen per context: moao_ctx_set_gemm_tile / the autotuner).
+template <int BM_, int BN_, int WM_, int BK_ = 16, int STAGES_ = 4>
 struct Tile {
-  static constexpr int BM = BM_, BN = BN_, WM = WM_;
+  static constexpr int BM = BM_, BN = BN_, WM = WM_, BK = BK_, STAGES = STAGES_;
   static constexpr int WARPS_M = BM / WM, WARPS_N = BN / 32;
   static constexpr int NTHREADS = 32 * WARPS_M * WARPS_N;
   static constexpr int MF = WM / 8;             // 8-row fragments per warp
@@ -48,6 +48,10 @@ struct Tile {
 };
 using TileL = Tile<128, 64, 32>;
 using TileS = Tile<64, 64, 32>;
+// alternative large-product configurations (GemmArgs::cfg 1..3)
+using TileL32x2 = Tile<128, 64, 32, 32, 2>;   // 102 KB: two CTAs per SM, two k16 steps per barrier
+using TileL32x3 = Tile<128, 64, 32, 32, 3>;   // 154 KB: one CTA per SM
+using TileL16x6 = Tile<128, 64, 32, 16, 6>;   // 154 KB: one CTA per SM, deeper ring
 
 __device__ __forceinline__ void cp_async(double* smem, const double* gmem, int vec, int valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -130,7 +134,7 @@ template <class TL, int VEC, int R, int LDS>
 __device__ __forceinline__ void load_mn_tile(double* s, const double* g, long ld, long rows,
                                              long K, long r0, long k0) {
   constexpr int CH = R / VEC;                // chunks per k column
-  constexpr int TOTAL = CH * BK;
+  constexpr int TOTAL = CH * TL::BK;
   for (int c = threadIdx.x; c < TOTAL; c += TL::NTHREADS) {
     const int kk = c / CH, rr = (c % CH) * VEC;
     const long gr = r0 + rr, gk = k0 + kk;
@@ -146,7 +150,7 @@ __device__ __forceinline__ void load_mn_tile(double* s, const double* g, long ld
 template <class TL, int VEC>
 __device__ __forceinline__ void load_k_tile(double* s, const double* g, long ld, long N,
                                             long K, long n0, long k0) {
-  constexpr int CH = BK / VEC;
+  constexpr int CH = TL::BK / VEC;
   constexpr int TOTAL = CH * TL::BN;
   for (int c = threadIdx.x; c < TOTAL; c += TL::NTHREADS) {
     const int nn = c / CH, kk = (c % CH) * VEC;
@@ -161,6 +165,7 @@ __device__ __forceinline__ void load_k_tile(double* s, const double* g, long ld,
 template <class TL, bool TRANSB, bool LOWERC, int VEC, bool MMA16>
 __global__ void __launch_bounds__(TL::NTHREADS) gemm_f64_kernel(const KParams p) {
   constexpr int BM = TL::BM, BN = TL::BN, NTHREADS = TL::NTHREADS, MF = TL::MF;
+  constexpr int BK = TL::BK, STAGES = TL::STAGES;
   constexpr int LDA_S = TL::LDA_S, LDB_S = TL::LDB_S, LDBT_S = TL::LDBT_S;
   constexpr int A_STAGE = TL::A_STAGE, B_STAGE = TL::B_STAGE;
   extern __shared__ __align__(16) double smem[];
@@ -238,24 +243,27 @@ __global__ void __launch_bounds__(TL::NTHREADS) gemm_f64_kernel(const KParams p)
       cp_commit();
     }
     if (MMA16) {
-      double bf[4][4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int k = r * 4 + tig, n = wn + j * 8 + gid;
-          bf[j][r] = TRANSB ? bs[k * LDB_S + n] : bs[n * LDBT_S + k];
-        }
-#pragma unroll
-      for (int i = 0; i < MF / 2; ++i) {
-        double af[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          af[r] = as[((r >> 1) * 4 + tig) * LDA_S + wm + i * 16 + gid + 8 * (r & 1)];
+      for (int k16 = 0; k16 < BK; k16 += 16) {
+        double bf[4][4];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1],
-                 af, bf[j]);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int k = k16 + r * 4 + tig, n = wn + j * 8 + gid;
+            bf[j][r] = TRANSB ? bs[k * LDB_S + n] : bs[n * LDBT_S + k];
+          }
+#pragma unroll
+        for (int i = 0; i < MF / 2; ++i) {
+          double af[8];
+#pragma unroll
+          for (int r = 0; r < 8; ++r)
+            af[r] = as[(k16 + (r >> 1) * 4 + tig) * LDA_S + wm + i * 16 + gid + 8 * (r & 1)];
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1],
+                   af, bf[j]);
+        }
       }
     } else {
 #pragma unroll
@@ -340,10 +348,16 @@ bool small_tiles(const KParams& p) {
 }
 
 template <bool TRANSB, bool LOWERC, int VEC>
-moao_status launch_gemm(const KParams& p, cudaStream_t s) {
+moao_status launch_gemm(const KParams& p, int cfg, cudaStream_t s) {
   if (small_tiles(p))
     return use_mma16() ? launch_gemm_t<TileS, TRANSB, LOWERC, VEC, true>(p, s)
                        : launch_gemm_t<TileS, TRANSB, LOWERC, VEC, false>(p, s);
+  switch (cfg) {
+    case 1: return launch_gemm_t<TileL32x2, TRANSB, LOWERC, VEC, true>(p, s);
+    case 2: return launch_gemm_t<TileL32x3, TRANSB, LOWERC, VEC, true>(p, s);
+    case 3: return launch_gemm_t<TileL16x6, TRANSB, LOWERC, VEC, true>(p, s);
+    default: break;
+  }
   return use_mma16() ? launch_gemm_t<TileL, TRANSB, LOWERC, VEC, true>(p, s)
                      : launch_gemm_t<TileL, TRANSB, LOWERC, VEC, false>(p, s);
 }
@@ -351,13 +365,18 @@ moao_status launch_gemm(const KParams& p, cudaStream_t s) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // Leaf kernel of the blocked factorisation (leaf_factor_inverse, one CTA).
-__global__ void __launch_bounds__(LEAF_THREADS, 1) potrf_inv_leaf_kernel(double* A, long lda,
-                                                                         double* Linv, long ldi,
-                                                                         int n, long col0,
-                                                                         int* info) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) potrf_inv_leaf_kernel(double* A, long lda,
+                                                                    double* Linv, long ldi, int n,
+                                                                    long col0, int* info) {
   extern __shared__ __align__(16) double leaf_smem[];
-  leaf_factor_inverse(A, lda, Linv, ldi, n, col0, info, leaf_smem);
+  leaf_factor_inverse<THREADS>(A, lda, Linv, ldi, n, col0, info, leaf_smem);
 }
+
+// The leaf CTA has 1,024 threads (two or three triangle elements each): 54 us
+// per 64 x 64 block against 66 us with 512 and 91 us with 256 threads (B200,
+// CUDA events over the leaves of an nmeas 15,936 FP64 build).
+constexpr int kLeafThreads = 1024;
 
 __global__ void copy_kernel(const double* __restrict__ src, long lds, double* __restrict__ dst,
                             long ldd, long m, long n) {
@@ -415,12 +434,13 @@ moao_status gemm_f64(const GemmArgs& g, cudaStream_t s, long long* launches) {
   }
   const bool v2 = aligned16(g.A) && aligned16(g.B) && (g.lda % 2 == 0) && (g.ldb % 2 == 0);
   moao_status st;
+  const int c = g.cfg;
   if (v2) {
-    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 2>(p, s) : launch_gemm<true, false, 2>(p, s);
-    else st = g.lowerC ? launch_gemm<false, true, 2>(p, s) : launch_gemm<false, false, 2>(p, s);
+    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 2>(p, c, s) : launch_gemm<true, false, 2>(p, c, s);
+    else st = g.lowerC ? launch_gemm<false, true, 2>(p, c, s) : launch_gemm<false, false, 2>(p, c, s);
   } else {
-    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 1>(p, s) : launch_gemm<true, false, 1>(p, s);
-    else st = g.lowerC ? launch_gemm<false, true, 1>(p, s) : launch_gemm<false, false, 1>(p, s);
+    if (g.transB) st = g.lowerC ? launch_gemm<true, true, 1>(p, c, s) : launch_gemm<true, false, 1>(p, c, s);
+    else st = g.lowerC ? launch_gemm<false, true, 1>(p, c, s) : launch_gemm<false, false, 1>(p, c, s);
   }
   if (st == MOAO_OK && launches) ++*launches;
   return st;
@@ -431,9 +451,10 @@ moao_status potrf_inv_leaf(double* A, long lda, double* Linv, long ldi, int n, l
   if (n <= 0) return MOAO_OK;
   if (n > LEAF) return set_error(MOAO_ERR_BAD_ARG, "potrf leaf: n > 64");
   static std::atomic<unsigned long long> configured{0};
-  const int smem = (2 * LEAF * LEAF_LD + 3 * LEAF) * (int)sizeof(double);
-  MOAO_CUDA_TRY(set_smem_limit(potrf_inv_leaf_kernel, smem, configured));
-  potrf_inv_leaf_kernel<<<1, LEAF_THREADS, smem, s>>>(A, lda, Linv, ldi, n, col0, d_info);
+  const int smem = LEAF_SMEM_BYTES;
+  MOAO_CUDA_TRY(set_smem_limit(potrf_inv_leaf_kernel<kLeafThreads>, smem, configured));
+  potrf_inv_leaf_kernel<kLeafThreads><<<1, kLeafThreads, smem, s>>>(A, lda, Linv, ldi, n, col0,
+                                                                    d_info);
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;

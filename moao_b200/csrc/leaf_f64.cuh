@@ -9,21 +9,21 @@ namespace moao {
 
 constexpr int LEAF = 64;
 constexpr int LEAF_LD = LEAF + 1;
-constexpr int LEAF_THREADS = 256;
-constexpr int LEAF_TRI = LEAF * (LEAF + 1) / 2;                          // 2,080
-constexpr int LEAF_OWN = (LEAF_TRI + LEAF_THREADS - 1) / LEAF_THREADS;  // 9
+constexpr int LEAF_TRI = LEAF * (LEAF + 1) / 2;  // 2,080
 // shared memory of leaf_factor_inverse, bytes
 constexpr int LEAF_SMEM_BYTES = (2 * LEAF * LEAF_LD + 3 * LEAF) * 8;
 
 // Leaf factorisation of a diagonal block (n <= 64) fused with the inversion of
-// its triangular factor, one CTA of 256 threads. Every thread owns up to nine
-// elements of the 64 x 64 lower triangle (element e = t + 256 s of the
-// row-packed triangle) and keeps them in registers through both phases:
+// its triangular factor, one CTA of THREADS threads (all of which call it).
+// Every thread owns up to OWN = ceil(2,080 / THREADS) elements of the 64 x 64
+// lower triangle (element e = t + THREADS s of the row-packed triangle) and
+// keeps them in registers through both phases:
 //   factor (right-looking, step j = 0..63): the owners of column j publish it
-//     (unscaled) to shared memory; after one barrier every thread takes
-//     d = A(j,j), r = 1/sqrt(d), writes L(i,j) = A(i,j) r (L(j,j) = d r) for
-//     its column-j elements and applies A(i,k) -= (A(i,j) r)(A(k,j) r) to
-//     its elements with k > j (column j is never written during step j);
+//     (unscaled) to shared memory, and the owner of A(j,j) publishes
+//     r = 1/sqrt(A(j,j)); after one barrier every thread writes
+//     L(i,j) = A(i,j) r (L(j,j) = A(j,j) r) for its column-j elements and
+//     applies A(i,k) -= (A(i,j) r)(A(k,j) r) to its elements with k > j
+//     (column j is never written during step j);
 //   inverse (X = L^-1 by rows, step i = 0..63, B = I): the owners of row i
 //     finish X(i,c) = B(i,c) / L(i,i) and publish the row; after one barrier
 //     every thread applies B(r,c) -= L(r,i) X(i,c) to its elements with r > i.
@@ -36,9 +36,12 @@ constexpr int LEAF_SMEM_BYTES = (2 * LEAF * LEAF_LD + 3 * LEAF) * 8;
 // written. A is read through L2 (ld.global.cg): in the tile-task kernel other
 // SMs wrote it moments before.
 
+template <int THREADS>
 __device__ __forceinline__ void leaf_factor_inverse(double* A, long lda, double* Linv, long ldi,
                                                     int n, long col0, int* info,
                                                     double* leaf_smem) {
+  constexpr int LEAF_THREADS = THREADS;
+  constexpr int LEAF_OWN = (LEAF_TRI + THREADS - 1) / THREADS;
   double* Lf = leaf_smem;                     // the factor, column-major, ld LEAF_LD
   double* Xs = leaf_smem + LEAF * LEAF_LD;    // the input block, then the inverse
   double* buf = leaf_smem + 2 * LEAF * LEAF_LD;  // [2][LEAF]: published column / row
@@ -71,25 +74,29 @@ __device__ __forceinline__ void leaf_factor_inverse(double* A, long lda, double*
   for (int j = 0; j < LEAF; ++j) {
     double* cj = buf + (j & 1) * LEAF;
 #pragma unroll
-    for (int s = 0; s < LEAF_OWN; ++s)
-      if (ci[s] == j) cj[ri[s]] = a[s];
-    __syncthreads();
-    double d = cj[j];
-    if (!(d > 0.0)) {
-      if (tid == 0 && j < n) atomicCAS(info, 0, (int)(col0 + j + 1));
-      d = 1.0;
+    for (int s = 0; s < LEAF_OWN; ++s) {
+      if (ci[s] == j) {
+        if (ri[s] == j) {  // the pivot: checked, its reciprocal square root published
+          if (!(a[s] > 0.0)) {
+            if (j < n) atomicCAS(info, 0, (int)(col0 + j + 1));
+            a[s] = 1.0;
+          }
+          rinv[j] = rsqrt(a[s]);
+        }
+        cj[ri[s]] = a[s];
+      }
     }
-    const double r = rsqrt(d);
+    __syncthreads();
+    const double r = rinv[j];
 #pragma unroll
     for (int s = 0; s < LEAF_OWN; ++s) {
       if (ci[s] == j) {
-        Lf[ri[s] + j * LEAF_LD] = (ri[s] == j ? d : a[s]) * r;
+        Lf[ri[s] + j * LEAF_LD] = a[s] * r;
       } else if (ci[s] > j) {
         const double li = cj[ri[s]] * r, lk = cj[ci[s]] * r;
         a[s] = fma(-li, lk, a[s]);
       }
     }
-    if (tid == 0) rinv[j] = r;
   }
   __syncthreads();
   // ---- inverse of the factor, by rows

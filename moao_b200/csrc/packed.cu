@@ -30,12 +30,15 @@
 //
 // Progress: the list is sorted by DAG level (longest dependency chain from the
 // start), so every task a task waits for sits earlier in the list and has
-// already been claimed by a CTA that is running; a CTA claims its next task
-// only after finishing the current one. The earliest unfinished claimed task
-// therefore always has its inputs and completes, whether or not the whole grid
-// is resident. Every wait is bounded as well (poll count and a global-timer
-// deadline): on expiry the CTA raises the error flag and every CTA stops at its
-// next claim or poll; the host reports MOAO_ERR_TIMEOUT.
+// already been claimed by a CTA that is running. A CTA claims its next task
+// only once the inputs of its current one are ready (the current one then
+// runs to the end without waiting), so a claimed task is always either being
+// waited for by a running CTA or queued behind a task that will finish. The
+// earliest unfinished claimed task therefore always has its inputs and
+// completes, whether or not the whole grid is resident. Every wait is bounded
+// as well (poll count and a global-timer deadline): on expiry the CTA raises
+// the error flag and every CTA stops at its next claim or poll; the host
+// reports MOAO_ERR_TIMEOUT.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,7 +56,8 @@ constexpr int T = 64;               // tile edge
 constexpr int TLD = T + 4;          // shared-memory leading dimension (conflict-free fragments)
 constexpr int NTHREADS = 256;       // 8 warps: 4 along m (16 rows) x 2 along n (32 columns)
 constexpr int TILE_SMEM = T * TLD * 8;
-constexpr int SMEM_BYTES = 2 * TILE_SMEM > LEAF_SMEM_BYTES ? 2 * TILE_SMEM : LEAF_SMEM_BYTES;
+// P, Q and (for an update) the old value of the tile written: 102 KB, two CTAs per SM
+constexpr int SMEM_BYTES = 3 * TILE_SMEM > LEAF_SMEM_BYTES ? 3 * TILE_SMEM : LEAF_SMEM_BYTES;
 
 enum TaskType { kPotrf = 0, kTrsm, kUpdate, kFUpd, kFDiag, kBUpd, kBDiag };
 
@@ -95,12 +99,21 @@ __device__ __forceinline__ void mma16(double (&c)[4], const double (&a)[8], cons
 }
 
 // s (column-major, ld TLD) <- the rv x cv corner of the tile at g (ld), zeros
-// elsewhere; read through L2.
+// elsewhere; read through L2 with a thread's 16 loads in flight before its
+// first store.
 __device__ __forceinline__ void load_tile(double* s, const double* g, long ld, int rv, int cv) {
-#pragma unroll 4
-  for (int e = threadIdx.x; e < T * T; e += NTHREADS) {
+  constexpr int PER = T * T / NTHREADS;  // 16
+  double v[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * NTHREADS;
     const int r = e & (T - 1), c = e >> 6;
-    s[c * TLD + r] = (r < rv && c < cv) ? __ldcg(g + (long)c * ld + r) : 0.0;
+    v[q] = (r < rv && c < cv) ? __ldcg(g + (long)c * ld + r) : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * NTHREADS;
+    s[(e >> 6) * TLD + (e & (T - 1))] = v[q];
   }
 }
 
@@ -135,9 +148,10 @@ __device__ __forceinline__ void tile_product(const double* Ps, const double* Qs,
   }
 }
 
-// D (rv x cv, ld) = acc (SET) or D -= acc (SUB); lower: only r >= c.
+// D (rv x cv, ld) = acc (SET) or D = Ds - acc (SUB, Ds the staged old value);
+// lower: only r >= c.
 __device__ __forceinline__ void store_tile(double* D, long ld, int rv, int cv, bool sub, bool lower,
-                                           const double (&acc)[4][4]) {
+                                           const double* Ds, const double (&acc)[4][4]) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
   const int gid = lane >> 2, tig = lane & 3;
@@ -147,8 +161,7 @@ __device__ __forceinline__ void store_tile(double* D, long ld, int rv, int cv, b
     for (int h = 0; h < 4; ++h) {
       const int r = wm + gid + 8 * (h >> 1), c = wn + 8 * j + 2 * tig + (h & 1);
       if (r >= rv || c >= cv || (lower && r < c)) continue;
-      double* d = D + (long)c * ld + r;
-      *d = sub ? __ldcg(d) - acc[j][h] : acc[j][h];
+      D[(long)c * ld + r] = sub ? Ds[c * TLD + r] - acc[j][h] : acc[j][h];
     }
 }
 
@@ -160,12 +173,15 @@ __device__ __forceinline__ void tile_task(double* smem, const double* Pg, long l
                                           long ldd, bool sub, bool lower) {
   double* Ps = smem;
   double* Qs = smem + T * TLD;
+  double* Ds = smem + 2 * T * TLD;
+  const int dcv = TRANSQ ? qrv : qcv;
   load_tile(Ps, Pg, ldp, prv, pcv);
   load_tile(Qs, Qg, ldq, qrv, qcv);
+  if (sub) load_tile(Ds, D, ldd, prv, dcv);
   __syncthreads();
   double acc[4][4];
   tile_product<TRANSQ>(Ps, Qs, acc);
-  store_tile(D, ldd, prv, TRANSQ ? qrv : qcv, sub, lower, acc);
+  store_tile(D, ldd, prv, dcv, sub, lower, Ds, acc);
 }
 
 struct Wait {
@@ -178,19 +194,25 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                         long ntasks, unsigned long long* next, int* err,
                         unsigned long long poll_limit, unsigned long long wait_ns) {
   extern __shared__ __align__(16) double smem[];
-  __shared__ long cur;
+  // The task this CTA runs and the next one it has claimed: thread 0 claims the
+  // next task once the current one's inputs are ready (it then runs without
+  // further waits), so the claim and the task fetch overlap the current work.
+  __shared__ int4 s_task[2];
+  __shared__ int s_valid[2];
   __shared__ int stop;
   const int tid = threadIdx.x;
-  for (;;) {
-    if (tid == 0) {
-      long t = (long)atomicAdd(next, 1ull);
-      if (t >= ntasks || *(volatile int*)err != 0) t = -1;
-      cur = t;
-    }
-    __syncthreads();
-    const long t = cur;
-    if (t < 0) break;
-    const int4 tk = tasks[t];
+  auto claim = [&](int slot) {  // thread 0
+    const long t = (long)atomicAdd(next, 1ull);
+    const bool ok = t < ntasks && *(volatile int*)err == 0;
+    s_valid[slot] = ok;
+    if (ok) s_task[slot] = tasks[t];
+  };
+  if (tid == 0) claim(0);
+  __syncthreads();
+  for (int it = 0;; ++it) {
+    const int sl = it & 1;
+    if (!s_valid[sl]) break;
+    const int4 tk = s_task[sl];
     const PkInst I = insts[tk.x];
     const int type = tk.y, i = tk.z >> 16, j = tk.z & 0xffff, k = tk.w;
     const int nt = I.nt;
@@ -244,27 +266,34 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         break;
     }
     if (tid == 0) {
+      // all counters polled together; bounded by poll count and deadline
       int ok = 1;
       const unsigned long long deadline = global_ns() + wait_ns;
-      for (int q = 0; q < nw && ok; ++q) {
-        unsigned long long polls = 0;
-        while (ld_acquire(wt[q].p) < wt[q].v) {
-          if (*(volatile int*)err != 0) { ok = 0; break; }
-          if (++polls >= poll_limit || global_ns() > deadline) {
-            atomicCAS(err, 0, 1);
-            ok = 0;
-            break;
-          }
-          __nanosleep(128);
+      unsigned long long polls = 0;
+      for (;;) {
+        bool ready = true;
+        unsigned v[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = q < nw ? ld_acquire(wt[q].p) : 0u;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) ready &= q >= nw || v[q] >= wt[q].v;
+        if (ready) break;
+        if (*(volatile int*)err != 0) { ok = 0; break; }
+        if (++polls >= poll_limit || global_ns() > deadline) {
+          atomicCAS(err, 0, 1);
+          ok = 0;
+          break;
         }
+        __nanosleep(128);
       }
       stop = !ok;
+      if (ok) claim(sl ^ 1);
     }
     __syncthreads();
     if (stop) break;
     switch (type) {
       case kPotrf:
-        leaf_factor_inverse(At(k, k), I.lda, I.Linv + (size_t)k * T * T, T, tn(k), (long)k * T,
+        leaf_factor_inverse<NTHREADS>(At(k, k), I.lda, I.Linv + (size_t)k * T * T, T, tn(k), (long)k * T,
                             I.info, smem);
         break;
       case kTrsm:

@@ -25,6 +25,7 @@ moao_status gemm(moao_ctx* ctx, long M, long N, long K, double alpha, const doub
   g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
   g.A = A; g.lda = lda; g.B = B; g.ldb = ldb; g.transB = transB; g.triB = tri;
   g.C = C; g.ldc = ldc; g.lowerC = lowerC;
+  g.cfg = ctx->gemm_cfg;
   // algorithmic flops: 2MNK, halved when only a triangle of C or of B counts
   double fl = 2.0 * M * N * K;
   if (lowerC) fl = (double)M * N * K + (double)std::min(M, N) * K;

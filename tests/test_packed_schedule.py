@@ -132,35 +132,47 @@ def test_task_counts_are_the_tile_algorithm(built):
 
 @pytest.mark.parametrize("workers,seed", [(3, 1), (16, 2), (300, 3)])
 def test_concurrent_claims_always_complete(built, workers, seed):
-    """P workers claim tasks in list order, a claimed task starts once its waits
-    hold and takes a random time; the event simulation must finish every task."""
+    """P workers (CTAs) claim tasks in list order; a claimed task starts once its
+    waits hold and takes a random time; as in the kernel, a worker claims its next
+    task as soon as its current one starts (one task queued behind the running
+    one). The event simulation must finish every task."""
     rng = np.random.default_rng(seed)
     sizes = [(200, 70), (129, 64), (333, 10)]
     tasks, _ = B.packed_task_list([n for n, _ in sizes], [m for _, m in sizes])
     tasks = [tuple(int(x) for x in t) for t in tasks]
     inst = [Replay(spd(n, rng), rng.standard_normal((m, n))) for n, m in sizes]
     nxt, done, now = 0, 0, 0.0
-    running = []   # heap of (finish time, seq, task)
-    waiting = []   # claimed, not started
+    cur = [None] * workers      # claimed task waiting for its inputs, or None
+    busy = [False] * workers    # running (its task is in the heap)
+    queued = [None] * workers   # claimed behind the running task
+    running = []                # heap of (finish time, seq, worker, task)
     seq = 0
-    idle = workers
-    while done < len(tasks):
-        while idle and nxt < len(tasks):   # claims in list order
-            waiting.append(tasks[nxt])
+
+    def claim():
+        nonlocal nxt
+        if nxt < len(tasks):
             nxt += 1
-            idle -= 1
+            return tasks[nxt - 1]
+        return None
+
+    for w in range(workers):
+        cur[w] = claim()
+    while done < len(tasks):
         started = True
         while started:
             started = False
-            for t in list(waiting):
-                if inst[t[0]].ready(t):
-                    waiting.remove(t)
-                    heapq.heappush(running, (now + rng.exponential(1.0), seq, t))
+            for w in range(workers):
+                t = cur[w]
+                if t is not None and not busy[w] and inst[t[0]].ready(t):
+                    busy[w] = True
+                    heapq.heappush(running, (now + rng.exponential(1.0), seq, w, t))
                     seq += 1
+                    queued[w] = claim()  # claim-ahead once the current task runs
                     started = True
         assert running, "no claimed task can start: the schedule would deadlock"
-        now, _, t = heapq.heappop(running)
+        now, _, w, t = heapq.heappop(running)
         inst[t[0]].run(t)
         done += 1
-        idle += 1
-    assert nxt == len(tasks) and not waiting
+        busy[w] = False
+        cur[w], queued[w] = queued[w], None
+    assert nxt == len(tasks) and all(c is None for c in cur)
