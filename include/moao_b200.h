@@ -120,6 +120,16 @@ moao_status moao_ctx_set_lookahead(moao_ctx* ctx, int sms);
  * midpoint of the two settings, below 12,288: this one); values at or below the
  * lookahead setting keep it throughout. No reference counterpart. */
 moao_status moao_ctx_set_lookahead_max(moao_ctx* ctx, int sms);
+/* Host-buffer cache of the drop-in path (off by default). When on, a whole Cmm
+ * (type 1, offsets 0, nrows == ncols) or Ctm (type 3, offsets 0) generated by
+ * moao_matcov_tile_host stays on the device, and moao_reconstructor_host skips
+ * the upload of a buffer that is the same host pointer with the same shape and
+ * leading dimension (Ctm: ngal 1, ldCtm == nmeasts). The caller promises not
+ * to modify those host buffers between the two calls (the reference's driver,
+ * lapack/moao_lapack.cpp, generates them and passes them on unchanged); every
+ * output is still written to the host buffers. Turning it on or off forgets
+ * the cached tiles. No reference counterpart. */
+moao_status moao_ctx_set_host_cache(moao_ctx* ctx, int on);
 /* Tile configuration of the large FP64 products (128 x 64 CTA tiles, 8 warps):
  * 0: K 16 per stage, 4-stage cp.async ring, two CTAs per SM; 1: K 32, 2 stages,
  * two CTAs per SM (default); 2: K 32, 3 stages, one CTA per SM; 3: K 16,

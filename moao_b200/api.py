@@ -182,6 +182,12 @@ class Context:
         check(lib().moao_ctx_set_offsets_from_tomo(self._h, tomo.handle),
               "moao_ctx_set_offsets_from_tomo")
 
+    def set_host_cache(self, on: bool = True):
+        """Host-buffer cache of the drop-in path (see moao_ctx_set_host_cache):
+        the caller promises not to modify the host Cmm / Ctm between
+        matcov_tile on host buffers and reconstructor on host buffers."""
+        check(lib().moao_ctx_set_host_cache(self._h, int(bool(on))), "moao_ctx_set_host_cache")
+
     def set_gemm_tile(self, cfg: int = 1):
         """Tile configuration of the large FP64 products (see
         moao_ctx_set_gemm_tile); same results."""

@@ -32,6 +32,7 @@ moao_status DevBuf::ensure(size_t n) {
                                        cudaGetErrorString(e));
   }
   bytes = n;
+  ++generation;
   return MOAO_OK;
 }
 
@@ -39,6 +40,7 @@ void DevBuf::release() {
   if (p) cudaFree(p);
   p = nullptr;
   bytes = 0;
+  ++generation;
 }
 
 moao_status device_geometry(moao_ctx* ctx, const moao_tomo* tp, const DevGeometry** out) {
@@ -228,6 +230,17 @@ moao_status collect_kernel_stats(moao_ctx* ctx) {
   }
   ctx->pending.clear();
   return MOAO_OK;
+}
+
+// dst(r, c) = src(r, c) for the elements above the diagonal (r < c) of a
+// w x w block (the host path's cached Cmm, moao_reconstructor_host).
+__global__ void upper_of_block_kernel(double* __restrict__ dst, long ldd,
+                                      const double* __restrict__ src, long w) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < w * w;
+       e += (long)gridDim.x * blockDim.x) {
+    const long r = e % w, c = e / w;
+    if (r < c) dst[c * ldd + r] = src[c * w + r];
+  }
 }
 
 }  // namespace moao
@@ -558,6 +571,15 @@ moao_status moao_ctx_set_gemm_tile(moao_ctx* c, int cfg) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_host_cache(moao_ctx* c, int on) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_cache: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->host_cache = on != 0;
+  c->cache_cmm = moao_ctx::HostTile{};
+  c->cache_ctm = moao_ctx::HostTile{};
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_lookahead_max(moao_ctx* c, int sms) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: null");
   if (sms < 0 || sms > 120) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_lookahead_max: 0..120 SMs");
@@ -624,6 +646,26 @@ moao_status copy_lower_panels(double* dst, long ldd, const double* src, long lds
   return MOAO_OK;
 }
 
+// The caller's elements above the diagonal inside the diagonal blocks of the
+// 512-column panels of an n x n matrix (the only upper elements that the lower
+// panel copies carry), brought down into dst without touching anything else.
+moao_status upload_panel_uppers(double* dst, long ldd, const double* src, long lds, long n,
+                                DevBuf& stage, cudaStream_t s, long long* launches) {
+  const long w = 512;
+  MOAO_TRY(stage.ensure(sizeof(double) * (size_t)w * w));
+  for (long c0 = 0; c0 < n; c0 += w) {
+    const long b = std::min(w, n - c0);
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(stage.p, sizeof(double) * b, src + c0 * lds + c0,
+                                    sizeof(double) * lds, sizeof(double) * b, b,
+                                    cudaMemcpyHostToDevice, s));
+    upper_of_block_kernel<<<(unsigned)std::min<long>((b * b + 255) / 256, 1024), 256, 0, s>>>(
+        dst + c0 * ldd + c0, ldd, stage.as<double>(), b);
+    MOAO_CUDA_TRY(cudaGetLastError());
+    if (launches) ++*launches;
+  }
+  return MOAO_OK;
+}
+
 }  // namespace
 
 moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_data, int nrows,
@@ -635,13 +677,21 @@ moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_d
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   const DevGeometry* g = nullptr;
   MOAO_TRY(device_geometry(ctx, t, &g));
-  const size_t bytes = sizeof(double) * (size_t)nrows * ncols;
-  MOAO_TRY(ctx->ws_tmp.ensure(bytes));
-  double* d = ctx->ws_tmp.as<double>();
-  cudaStream_t s = ctx->stream;
   if (type_mat != 1 && type_mat != 2 && type_mat != 3 && type_mat != 4 && type_mat != 5)
     return set_error(MOAO_ERR_BAD_ARG, "matcov_tile_host: unknown type_mat " +
                                            std::to_string(type_mat));
+  const size_t bytes = sizeof(double) * (size_t)nrows * ncols;
+  // With the host cache a whole type-3 tile (Ctm) is generated in the Ctm
+  // workspace of moao_reconstructor_host, so that a whole Cmm left in ws_tmp
+  // survives it; every other tile goes through ws_tmp.
+  const bool whole_cmm = type_mat == 1 && xoffset == 0 && yoffset == 0 && nrows == ncols;
+  const bool ctm_ws = ctx->host_cache && type_mat == 3 && xoffset == 0 && yoffset == 0;
+  DevBuf& buf = ctm_ws ? ctx->ws_host_t : ctx->ws_tmp;
+  MOAO_TRY(buf.ensure(bytes));
+  double* d = buf.as<double>();
+  cudaStream_t s = ctx->stream;
+  if (ctm_ws) ctx->cache_ctm = moao_ctx::HostTile{};
+  else ctx->cache_cmm = moao_ctx::HostTile{};
   // Column blocks at the WFS boundaries of the columns (types 1 and 3 have WFS
   // slopes as columns and write only inside their own columns; a block holds both
   // slope axes of its WFS, so no pair's stencils are evaluated twice): block b is
@@ -692,6 +742,14 @@ moao_status moao_matcov_tile_host(moao_ctx* ctx, const moao_tomo* t, double* h_d
   }
   MOAO_CUDA_TRY(cudaStreamSynchronize(s));
   MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->copy));
+  if (ctx->host_cache && (whole_cmm || ctm_ws)) {
+    moao_ctx::HostTile& c = ctm_ws ? ctx->cache_ctm : ctx->cache_cmm;
+    c.h = h_data;
+    c.ld = lda;
+    c.rows = nrows;
+    c.cols = ncols;
+    c.gen = buf.generation;
+  }
   return MOAO_OK;
 }
 
@@ -705,6 +763,7 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
   const size_t tspan = (size_t)nmeas * nmeasts * (ngal - 1) + (size_t)ldCtm * (nmeas - 1) + nmeasts;
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   double *dC = nullptr, *dT = nullptr;
+  bool cmm_cached = false, ctm_cached = false;
   {
     // device copies in the context's workspaces (kept for the next call)
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -712,6 +771,17 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
     MOAO_TRY(ctx->ws_host_t.ensure(sizeof(double) * tspan));
     dC = ctx->ws_tmp.as<double>();
     dT = ctx->ws_host_t.as<double>();
+    if (ctx->host_cache) {
+      // what moao_matcov_tile_host generated into these very buffers for these
+      // host buffers (the caller promised not to change them since)
+      const moao_ctx::HostTile &a = ctx->cache_cmm, &b = ctx->cache_ctm;
+      cmm_cached = a.h == Cmm && a.ld == ldCmm && a.rows == nmeas && a.cols == nmeas &&
+                   a.gen == ctx->ws_tmp.generation;
+      ctm_cached = b.h == Ctm && ngal == 1 && b.ld == ldCtm && ldCtm == nmeasts &&
+                   b.rows == nmeasts && b.cols == nmeas && b.gen == ctx->ws_host_t.generation;
+    }
+    ctx->cache_cmm = moao_ctx::HostTile{};  // the buffers now become the factor and R
+    ctx->cache_ctm = moao_ctx::HostTile{};
   }
   cudaStream_t s = ctx->stream;
   if (!ctx->copy) MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
@@ -723,10 +793,18 @@ moao_status moao_reconstructor_host(moao_ctx* ctx, long nmeas, long nmeasts, dou
   // Ctm goes down on the copy stream while the factorisation runs (the solves
   // wait for it), and the factor comes back on the copy stream while the solves
   // run.
-  MOAO_TRY(copy_lower_panels(dC, nmeas, Cmm, ldCmm, nmeas, nmeas, 0, false,
-                             cudaMemcpyHostToDevice, s));
-  MOAO_CUDA_TRY(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice,
-                                ctx->copy));
+  // A cached Cmm still takes the caller's elements above the diagonal inside
+  // the panels' diagonal blocks (the covariance tile never wrote them, and they
+  // go back with the factor's panels); nothing of the lower part is read.
+  if (cmm_cached)
+    MOAO_TRY(upload_panel_uppers(dC, nmeas, Cmm, ldCmm, nmeas, ctx->ws_corner, s,
+                                 &ctx->launches));
+  else
+    MOAO_TRY(copy_lower_panels(dC, nmeas, Cmm, ldCmm, nmeas, nmeas, 0, false,
+                               cudaMemcpyHostToDevice, s));
+  if (!ctm_cached)
+    MOAO_CUDA_TRY(cudaMemcpyAsync(dT, Ctm, sizeof(double) * tspan, cudaMemcpyHostToDevice,
+                                  ctx->copy));
   MOAO_CUDA_TRY(cudaEventRecord(ctx->inputs_ready, ctx->copy));
   ctx->wait_inputs = true;
   ctx->host_factor = Cmm;

@@ -24,6 +24,7 @@ namespace moao {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  unsigned long long generation = 0;  // bumped by every (re)allocation and release
   moao_status ensure(size_t n);
   void release();
   template <typename T>
@@ -55,7 +56,7 @@ struct moao_ctx {
   bool graph_mode = false;  // mixed path under stream capture: no host waits or reads
   std::mutex mu;
   std::map<const moao_tomo*, moao::GeomEntry> geom;
-  moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp, ws_host_t;
+  moao::DevBuf ws_w, ws_dinv, ws_info, ws_tmp, ws_host_t, ws_corner;
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
@@ -86,6 +87,17 @@ struct moao_ctx {
   int lookahead_sms = 8;
   int lookahead_max = 8;  // SMs left to it in the last panels (moao_ctx_set_lookahead_max)
   int gemm_cfg = 1;       // tile configuration of the large FP64 products (GemmArgs::cfg)
+  // Host-buffer cache of the drop-in path (moao_ctx_set_host_cache): the device
+  // copy that moao_matcov_tile_host left of a whole Cmm (in ws_tmp) or Ctm (in
+  // ws_host_t), keyed by the host buffer, its shape and the workspace's
+  // generation; moao_reconstructor_host then skips that upload.
+  struct HostTile {
+    const double* h = nullptr;
+    long ld = 0, rows = 0, cols = 0;
+    unsigned long long gen = 0;
+  };
+  bool host_cache = false;
+  HostTile cache_cmm, cache_ctm;
   cudaStream_t aux = nullptr;
   cudaEvent_t la_ev[2] = {};
   // host-buffer entry points: device-to-host copies of finished column blocks
@@ -118,7 +130,7 @@ struct moao_ctx {
 
   // Every workspace buffer of the context (not the geometry caches).
   std::vector<moao::DevBuf*> workspaces() {
-    return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &ws_host_t, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
+    return {&ws_w,  &ws_dinv, &ws_info, &ws_tmp, &ws_host_t, &ws_corner, &mx_a32, &mx_lr,  &mx_lc,    &mx_t32,
             &mx_w1, &mx_w2,   &mx_x,    &mx_r64, &mx_e64, &mx_qa,  &mx_qb,    &mx_ea,
             &mx_fb, &mx_colmax, &mx_norm, &mx_rid, &mx_y, &mx_y2, &mx_zu, &mx_sinv, &mx_exps,
             &mx_dsl, &cx_qc, &cx_ec};

@@ -89,3 +89,55 @@ def test_reconstructor_host_lower_only(ctx, prec):
     lo = np.tril_indices(nm)
     assert np.array_equal(Ch[:nm][lo], L_dev[lo])
     assert np.array_equal(Th, R_dev)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_host_cache_skips_the_uploads(ctx, prec):
+    """With moao_ctx_set_host_cache on, the Cmm and Ctm that matcov_tile left in
+    host buffers are not uploaded again by reconstructor: the outputs equal the
+    uncached host path's bit for bit, the caller's upper triangle and padding
+    survive, and a change the caller makes to the host Cmm in between (breaking
+    the promise on purpose) is not seen, which shows the device copy was used.
+    Another tile generated in between, or a different host buffer, misses the
+    cache."""
+    t = tomo("elt16")
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    pad = 3
+    if prec == "mixed":
+        ctx.set_offsets_from_tomo(t)
+
+    def build(cache, tamper=False, other_tile=False):
+        ctx.set_host_cache(cache)
+        Ch = np.full((nm + pad, nm), SENT, order="F")
+        Th = np.zeros((nts, nm), order="F")
+        M.matcov_tile(Ch, nm, nm, 0, 0, nm + pad, t, 1, ctx=ctx)
+        M.matcov_tile(Th, nts, nm, 0, 0, nts, t, 3, ctx=ctx)
+        if other_tile:
+            Ctt = np.zeros((nts, nts), order="F")
+            M.matcov_tile(Ctt, nts, nts, 0, 0, nts, t, 4, ctx=ctx)
+        if tamper:
+            lo = np.tril_indices(nm, -1)
+            Ch[:nm][lo] *= 0.5
+        M.reconstructor(nm, nts, Ch, nm + pad, Th, nts, 1, prec=prec, ctx=ctx)
+        return Ch, Th
+
+    try:
+        C0, T0 = build(False)
+        C1, T1 = build(True)
+        if prec == "fp64":  # halving the off-diagonal part keeps Cmm SPD
+            C2, T2 = build(True, tamper=True)
+            C3, T3 = build(True, tamper=True, other_tile=True)
+            C4, T4 = build(False, tamper=True)
+    finally:
+        ctx.set_host_cache(False)
+        ctx.set_offsets([], [], [])
+    up = np.triu_indices(nm, 1)
+    for C in (C0, C1):
+        assert np.all(C[:nm][up] == SENT) and np.all(C[nm:] == SENT)
+    assert np.array_equal(C1, C0) and np.array_equal(T1, T0)
+    if prec == "fp64":
+        assert np.array_equal(C2, C0) and np.array_equal(T2, T0), "the device copy was not used"
+        # Cmm's cache was dropped by the Ctt tile: the tampered matrix was uploaded
+        assert np.all(C3[:nm][up] == SENT) and np.all(C3[nm:] == SENT)
+        assert np.array_equal(C3, C4) and np.array_equal(T3, T4)
+        assert not np.array_equal(T3, T0)
