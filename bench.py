@@ -70,6 +70,9 @@ def parse():
                    help="batch: nmeas bound of the instances packed into the tile-task kernel "
                         "(0: autotuned, -1: none)")
     p.add_argument("--serve-slots", type=int, default=3)
+    p.add_argument("--sharded", action="store_true",
+                   help="one ELT system's FP64 build with Cmm spread over the ranks (torchrun, "
+                        "one GPU each) instead of one build per rank")
     p.add_argument("--no-compare", action="store_true",
                    help="mixed path: skip timing the FP64 path beside it")
     p.add_argument("--no-cee", action="store_true", help="skip the Cee/Cvv/PSF stage at ELT size")
@@ -707,6 +710,60 @@ def batch_main(args):
     return 0
 
 
+def sharded_main(args):
+    """The ELT build (matcov of each rank's panels, FP64 factorisation and both
+    solves, R left distributed) with Cmm's column panels spread over the ranks:
+    one build per step for the whole job, panels broadcast over NCCL."""
+    import numpy as np
+    import torch
+    import moao_b200 as M
+    from moao_b200 import sharded as S
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from moao_b200.replicas import max_over_ranks
+    sf, af, sysp, atm = system(args.config)
+    t = M.Tomo(sf, af)
+    nm, nts = t.getNMeas(), t.getNMeasTS()
+    ctx = M.Context(local)
+    nb = args.nb or 1024
+
+    def one():
+        R, lay, B = S.sharded_reconstructor(t, nb=nb, ctx=ctx, dist=dist, gather=False)
+        return B
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, "cuda")
+    if rank == 0:
+        print(json.dumps({
+            "metric": "R builds/s, one ELT system sharded over the ranks (FP64)", "value": 1000.0 / ms,
+            "unit": "builds/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "dtype": "f64",
+            "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "panel_nb": nb,
+                       "parallelism": f"column panels cyclic over {world} ranks"},
+            "data": "synthetic"}), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def probe_main(args):
     """One stage, once, on the ELT geometry scaled to args.nssp subapertures
     across (35 layers; 64 gives the ELT system itself). For profiler captures:
@@ -801,6 +858,8 @@ def main():
         return serving_main(args)
     if args.batch:
         return batch_main(args)
+    if args.sharded:
+        return sharded_main(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -258,6 +258,24 @@ moao_status moao_reconstructor_noalloc(long nmeas, long nmeasts, double* d_Cmm, 
                                        double* d_Ctm, long ldCtm, long ngal, void* stream,
                                        int* info);
 
+/* ---- Dense FP64 building blocks on device buffers (column-major), the ones
+ * the blocked factorisation uses, for callers that distribute the
+ * factorisation themselves (moao_b200/sharded.py: one Cmm spread over several
+ * GPUs). No reference counterpart (the reference's distributed path is
+ * ScaLAPACK's pdpotrf, scalapack/moao_scalapack.c).
+ * moao_dense_potrf_inv: A (n x n, lower read) <- its Cholesky factor L (lower;
+ * the upper triangle is left as is), Ainv <- L^-1 (lower, zeros above); waits
+ * for the result; on a non-positive pivot *info (if not NULL) receives the
+ * 1-based column and MOAO_ERR_NOT_SPD is returned.
+ * moao_dense_gemm: C = alpha A op(B) + beta C, op(B) = B^T if transB, A M x K,
+ * C M x N; lowerC writes only C(i, j) with i >= j. Asynchronous on the
+ * context's stream. */
+moao_status moao_dense_potrf_inv(moao_ctx* ctx, long n, double* A, long lda, double* Ainv,
+                                 long ldi, int* info);
+moao_status moao_dense_gemm(moao_ctx* ctx, int transB, int lowerC, long M, long N, long K,
+                            double alpha, const double* A, long lda, const double* B, long ldb,
+                            double beta, double* C, long ldc);
+
 /* ------------------------------------------------------------------------ */
 /* Error covariances.                                                        */
 /* Replaces MOAO_LAPACK::Cee_Cvv  lapack/compute/cee_cvv.cpp:50-125          */

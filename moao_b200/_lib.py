@@ -108,6 +108,9 @@ SIGNATURES = {
     "moao_ctx_set_lookahead_max": (i32, [vp, i32]),
     "moao_ctx_set_gemm_tile": (i32, [vp, i32]),
     "moao_ctx_set_host_cache": (i32, [vp, i32]),
+    "moao_dense_potrf_inv": (i32, [vp, i64, vp, i64, vp, i64, C.POINTER(i32)]),
+    "moao_dense_gemm": (i32, [vp, i32, i32, i64, i64, i64, C.c_double, vp, i64, vp, i64,
+                              C.c_double, vp, i64]),
     "moao_tuning_get_packed": (i32, [vp, i32, C.POINTER(C.c_long)]),
     "moao_tuning_get_gemm": (i32, [vp, i32, vp]),
     "moao_packed_task_list": (i32, [i32, vp, vp, vp, C.c_long, C.POINTER(C.c_long),

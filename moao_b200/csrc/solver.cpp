@@ -283,4 +283,39 @@ moao_status moao_cee_cvv_prec(moao_ctx* ctx, long nmeas, long nmeasts, long nact
   return MOAO_OK;
 }
 
+moao_status moao_dense_potrf_inv(moao_ctx* ctx, long n, double* A, long lda, double* Ainv,
+                                 long ldi, int* info) {
+  if (!ctx || n < 0 || (n > 0 && (!A || !Ainv)) || lda < std::max(1L, n) ||
+      ldi < std::max(1L, n))
+    return set_error(MOAO_ERR_BAD_ARG, "dense_potrf_inv: bad sizes or pointers");
+  if (info) *info = 0;
+  if (n == 0) return MOAO_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  MOAO_TRY(ctx->ws_w.ensure(sizeof(double) * (size_t)n * n));
+  MOAO_TRY(ctx->ws_info.ensure(3 * sizeof(int)));
+  int* d_info = ctx->ws_info.as<int>();
+  MOAO_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
+  MOAO_TRY(potrf_inv_block(ctx, A, lda, Ainv, ldi, n, 0, d_info, ctx->ws_w.as<double>()));
+  int h = 0;
+  MOAO_CUDA_TRY(cudaMemcpyAsync(&h, d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (info) *info = h;
+  if (h) return set_error(MOAO_ERR_NOT_SPD, "dense_potrf_inv: non-positive pivot at column " +
+                                                std::to_string(h));
+  return MOAO_OK;
+}
+
+moao_status moao_dense_gemm(moao_ctx* ctx, int transB, int lowerC, long M, long N, long K,
+                            double alpha, const double* A, long lda, const double* B, long ldb,
+                            double beta, double* C, long ldc) {
+  if (!ctx) return set_error(MOAO_ERR_BAD_ARG, "dense_gemm: null context");
+  if (M < 0 || N < 0 || K < 0) return set_error(MOAO_ERR_BAD_ARG, "dense_gemm: negative size");
+  if (M == 0 || N == 0) return MOAO_OK;
+  if (!C || (K > 0 && (!A || !B))) return set_error(MOAO_ERR_BAD_ARG, "dense_gemm: null matrix");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
+  return gemm(ctx, M, N, K, alpha, A, lda, B, ldb, transB != 0, beta, C, ldc, lowerC != 0);
+}
+
 }  // extern "C"
