@@ -24,7 +24,7 @@ typedef enum {
   MOAO_ERR_BAD_ARG = 1,     /* invalid size, type or pointer                  */
   MOAO_ERR_NOT_SPD = 2,     /* Cholesky met a non-positive pivot (see report) */
   MOAO_ERR_OOM = 3,         /* device allocation or admission failed          */
-  MOAO_ERR_CUDA = 4,        /* a CUDA runtime / cuFFT call failed             */
+  MOAO_ERR_CUDA = 4,        /* a CUDA runtime call failed                     */
   MOAO_ERR_IO = 5,          /* parameter / input file could not be read       */
   MOAO_ERR_TIMEOUT = 6,     /* a bounded device or host wait ran out          */
   MOAO_ERR_UNSUPPORTED = 7, /* option not available in this build            */
@@ -345,7 +345,8 @@ moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, doub
  * the FFT support; idx (nact^2, 1-based, column-major pairs), abs2fi and otf_tel
  * (N x N each) are filled where not NULL (host arrays). With all three NULL
  * only the sizes are computed (ctx may then be NULL); the FFT tables run on
- * the device (cuFFT). No reference counterpart: the reference reads FITS files. */
+ * the device (the library's FFT). No reference counterpart: the reference reads
+ * FITS files. */
 moao_status moao_intersample_inputs(moao_ctx* ctx, long nssp, double Dtel, double obs,
                                     double coupling, long* nact, long* N, long* idx,
                                     double* abs2fi, double* otf_tel);

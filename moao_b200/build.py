@@ -70,7 +70,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     if cmds or _stale(LIB, objs):
         tmp = LIB + ".tmp"
         link = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + [
-            "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcuda",
+            "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcuda",
             "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")]
         if verbose:
             print(" ".join(link))

@@ -1,22 +1,26 @@
 // Intersample PSF: Cvv -> averaged covariance map -> phase structure function
 // -> long-exposure PSF (common/tomo_struct/intersample.cpp:74-170).
 //
-// Device pipeline (N = 512 for every supported system):
+// Device pipeline (N = 512 for every supported system), the reference's FFTW
+// real-to-complex / complex-to-real steps done as full complex transforms
+// (fft.cu) whose spectra are built Hermitian from the half spectrum the real
+// transforms keep, so the results are those of the half-spectrum pipeline:
 //   gather_place   Map cell c = sum of Cvv[i] over idx[i]-1 == c, in increasing i
 //                  (the reference's sequential scatter order, so the sum is
 //                  bit-identical), divided by its hit count, written straight
 //                  onto the N x N lattice with pitch dactupix; other pixels 0.
-//   cuFFT D2Z      N x N real -> N x (N/2+1)
-//   filter         re *= abs2fi[j*N+i] (transposed index, as in the reference),
-//                  im = 0
-//   cuFFT Z2D
+//   forward FFT    N x N (real input)
+//   filter         half spectrum (columns 0..N/2): re *= abs2fi[j*N+i]
+//                  (transposed index, as in the reference), im = 0; the other
+//                  columns the Hermitian mirror of it
+//   inverse FFT    (its real part is the complex-to-real result)
 //   to_dphi        exp(-0.5 (norm - dphi fact / fact2)) with the reference's
 //                  truncated pi in fact, written through the quadrant swap
 //                  (_eclat_double) so no separate shift pass runs
-//   otf            half spectrum re = otf_tel[j*N+i] * dphi[j*N+i], im = 0
-//   cuFFT Z2D, then a final quadrant swap into the output.
+//   otf            half spectrum re = otf_tel[j*N+i] * dphi[j*N+i], im = 0,
+//                  mirrored the same way
+//   inverse FFT, then a final quadrant swap of its real part into the output.
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
@@ -24,6 +28,7 @@
 #include <vector>
 
 #include "context.h"
+#include "fft.h"
 
 struct moao_isample {
   moao_ctx* ctx = nullptr;
@@ -36,11 +41,11 @@ struct moao_isample {
   int* cell_idx = nullptr;    // nidx
   double* inv_div = nullptr;  // nmap (1/div, or 1 when div == 0)
   double* div = nullptr;      // nmap
-  double* map = nullptr;      // N*N real
   double* dphi = nullptr;     // N*N real
-  cufftDoubleComplex* spec = nullptr;  // N*(N/2+1)
+  moao::Cplx* spec = nullptr;   // N*N: the map, then spectra
+  moao::Cplx* spec2 = nullptr;  // N*N
   double* in_host_cvv = nullptr;
-  cufftHandle fwd = 0, bwd = 0;
+  moao::Fft2d fft;
   double fact = 0, fact2 = 0;
   long idx_norm = 0;
 };
@@ -50,7 +55,7 @@ namespace {
 
 __global__ void gather_place_kernel(const double* __restrict__ cvv, const int* __restrict__ start,
                                     const int* __restrict__ cidx, const double* __restrict__ div,
-                                    double* __restrict__ map, long N, long ncov, long a,
+                                    Cplx* __restrict__ map, long N, long ncov, long a,
                                     long pitch) {
   const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
@@ -69,52 +74,66 @@ __global__ void gather_place_kernel(const double* __restrict__ cvv, const int* _
         v = s;
       }
     }
-    map[e] = v;
+    map[e] = {v, 0.0};
   }
 }
 
-__global__ void filter_kernel(cufftDoubleComplex* __restrict__ spec,
-                              const double* __restrict__ abs2fi, long N) {
-  const long H = N / 2 + 1, total = N * H;
+// Element (i, j) of the full spectrum whose half j <= N/2 is the real value
+// f(i, j) and whose other columns mirror it, f((N - i) mod N, N - j): what a
+// complex-to-real transform reads from a half spectrum.
+template <class F>
+__device__ __forceinline__ double hermitian_real(long i, long j, long N, F f) {
+  return j <= N / 2 ? f(i, j) : f((N - i) % N, N - j);
+}
+
+// out = re(spec) * abs2fi[j*N+i] on the half spectrum (transposed index), im 0
+__global__ void filter_kernel(const Cplx* __restrict__ spec, const double* __restrict__ abs2fi,
+                              Cplx* __restrict__ out, long N) {
+  const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
-    const long i = e / H, j = e % H;
-    spec[e].x *= abs2fi[j * N + i];
-    spec[e].y = 0.0;
+    const long i = e / N, j = e % N;
+    const double v = hermitian_real(i, j, N, [&](long a, long b) {
+      return spec[a * N + b].x * abs2fi[b * N + a];
+    });
+    out[e] = {v, 0.0};
   }
 }
 
-// dst[swap(e)] = exp(-0.5 * (norm - src[e] / fact2 * fact))
-__global__ void to_dphi_kernel(const double* __restrict__ src, double* __restrict__ dst, long N,
+// dst[swap(e)] = exp(-0.5 * (norm - re(src[e]) / fact2 * fact))
+__global__ void to_dphi_kernel(const Cplx* __restrict__ src, double* __restrict__ dst, long N,
                                long idx_norm, double fact, double fact2) {
-  const double norm = src[idx_norm] / fact2 * fact;
+  const double norm = src[idx_norm].x / fact2 * fact;
   const long total = N * N, h = N / 2;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const long x = e % N, y = e / N;
     const long d = ((x + h) % N) + ((y + h) % N) * N;
-    dst[d] = exp(-0.5 * (norm - src[e] / fact2 * fact));
+    dst[d] = exp(-0.5 * (norm - src[e].x / fact2 * fact));
   }
 }
 
-__global__ void otf_kernel(cufftDoubleComplex* __restrict__ spec, const double* __restrict__ otf,
+// spec = otf[j*N+i] * dphi[j*N+i] on the half spectrum, im 0
+__global__ void otf_kernel(Cplx* __restrict__ spec, const double* __restrict__ otf,
                            const double* __restrict__ dphi, long N) {
-  const long H = N / 2 + 1, total = N * H;
+  const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
-    const long i = e / H, j = e % H;
-    spec[e].x = otf[j * N + i] * dphi[j * N + i];
-    spec[e].y = 0.0;
+    const long i = e / N, j = e % N;
+    const double v = hermitian_real(i, j, N, [&](long a, long b) {
+      return otf[b * N + a] * dphi[b * N + a];
+    });
+    spec[e] = {v, 0.0};
   }
 }
 
-__global__ void swap_quadrants_kernel(const double* __restrict__ src, double* __restrict__ dst,
+__global__ void swap_quadrants_kernel(const Cplx* __restrict__ src, double* __restrict__ dst,
                                       long N) {
   const long total = N * N, h = N / 2;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const long x = e % N, y = e / N;
-    dst[((x + h) % N) + ((y + h) % N) * N] = src[e];
+    dst[((x + h) % N) + ((y + h) % N) * N] = src[e].x;
   }
 }
 
@@ -122,19 +141,11 @@ unsigned grid_for(long total) {
   return (unsigned)std::max(1L, std::min((total + 255) / 256, 148L * 8));
 }
 
-moao_status cufft_check(cufftResult r, const char* what) {
-  if (r != CUFFT_SUCCESS)
-    return set_error(MOAO_ERR_CUDA, std::string(what) + " failed (cufftResult " +
-                                        std::to_string((int)r) + ")");
-  return MOAO_OK;
-}
-
 void free_isample(moao_isample* is) {
   if (!is) return;
-  if (is->fwd) cufftDestroy(is->fwd);
-  if (is->bwd) cufftDestroy(is->bwd);
+  fft2d_free(&is->fft);
   void* ptrs[] = {is->abs2fi, is->otf, is->cell_start, is->cell_idx, is->inv_div,
-                  is->div, is->map, is->dphi, is->spec};
+                  is->div, is->dphi, is->spec, is->spec2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete is;
@@ -190,7 +201,7 @@ moao_status moao_intersample_create(moao_ctx* ctx, long nidx, long np, double Dt
   const long ncmap = N / 2 + 1;
   is->idx_norm = N * (ncmap - 1) + ncmap - 1;
 
-  const size_t NN = (size_t)N * N, H = (size_t)N * (N / 2 + 1);
+  const size_t NN = (size_t)N * N;
   moao_status st = MOAO_OK;
   auto alloc = [&](void** p, size_t bytes) {
     if (st == MOAO_OK && cudaMalloc(p, bytes) != cudaSuccess)
@@ -201,9 +212,9 @@ moao_status moao_intersample_create(moao_ctx* ctx, long nidx, long np, double Dt
   alloc((void**)&is->cell_start, (is->nmap + 1) * sizeof(int));
   alloc((void**)&is->cell_idx, nidx * sizeof(int));
   alloc((void**)&is->div, is->nmap * 8);
-  alloc((void**)&is->map, NN * 8);
   alloc((void**)&is->dphi, NN * 8);
-  alloc((void**)&is->spec, H * sizeof(cufftDoubleComplex));
+  alloc((void**)&is->spec, NN * sizeof(Cplx));
+  alloc((void**)&is->spec2, NN * sizeof(Cplx));
   if (st == MOAO_OK) {
     cudaMemcpy(is->abs2fi, abs2fi, NN * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(is->otf, otf_tel, NN * 8, cudaMemcpyHostToDevice);
@@ -212,8 +223,7 @@ moao_status moao_intersample_create(moao_ctx* ctx, long nidx, long np, double Dt
     if (cudaMemcpy(is->div, div.data(), is->nmap * 8, cudaMemcpyHostToDevice) != cudaSuccess)
       st = set_error(MOAO_ERR_CUDA, "intersample_create: upload");
   }
-  if (st == MOAO_OK) st = cufft_check(cufftPlan2d(&is->fwd, (int)N, (int)N, CUFFT_D2Z), "cufftPlan2d D2Z");
-  if (st == MOAO_OK) st = cufft_check(cufftPlan2d(&is->bwd, (int)N, (int)N, CUFFT_Z2D), "cufftPlan2d Z2D");
+  if (st == MOAO_OK) st = fft2d_plan(&is->fft, N);
   if (st != MOAO_OK) {
     free_isample(is);
     return st;
@@ -234,23 +244,21 @@ moao_status moao_intersample_process(moao_isample* is, const double* d_Cvv, doub
   std::lock_guard<std::mutex> lk(ctx->mu);
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
-  const long N = is->info.N, NN = N * N, H = N * (N / 2 + 1);
+  const long N = is->info.N, NN = N * N;
   const long ncmap = N / 2 + 1, nelem = (is->ncov - 1) / 2;
   const long pitch = (long)is->info.dactupix;
   const long a = ncmap - nelem * pitch - 1;
   if (a < 0) return set_error(MOAO_ERR_BAD_ARG, "intersample: map does not fit the FFT support");
-  MOAO_TRY(cufft_check(cufftSetStream(is->fwd, s), "cufftSetStream"));
-  MOAO_TRY(cufft_check(cufftSetStream(is->bwd, s), "cufftSetStream"));
   gather_place_kernel<<<grid_for(NN), 256, 0, s>>>(d_Cvv, is->cell_start, is->cell_idx, is->div,
-                                                    is->map, N, is->ncov, a, pitch);
-  MOAO_TRY(cufft_check(cufftExecD2Z(is->fwd, is->map, is->spec), "cufftExecD2Z"));
-  filter_kernel<<<grid_for(H), 256, 0, s>>>(is->spec, is->abs2fi, N);
-  MOAO_TRY(cufft_check(cufftExecZ2D(is->bwd, is->spec, is->map), "cufftExecZ2D"));
-  to_dphi_kernel<<<grid_for(NN), 256, 0, s>>>(is->map, is->dphi, N, is->idx_norm, is->fact,
+                                                    is->spec, N, is->ncov, a, pitch);
+  MOAO_TRY(fft2d(is->fft, is->spec, -1, s, &ctx->launches));
+  filter_kernel<<<grid_for(NN), 256, 0, s>>>(is->spec, is->abs2fi, is->spec2, N);
+  MOAO_TRY(fft2d(is->fft, is->spec2, +1, s, &ctx->launches));
+  to_dphi_kernel<<<grid_for(NN), 256, 0, s>>>(is->spec2, is->dphi, N, is->idx_norm, is->fact,
                                                is->fact2);
-  otf_kernel<<<grid_for(H), 256, 0, s>>>(is->spec, is->otf, is->dphi, N);
-  MOAO_TRY(cufft_check(cufftExecZ2D(is->bwd, is->spec, is->map), "cufftExecZ2D"));
-  swap_quadrants_kernel<<<grid_for(NN), 256, 0, s>>>(is->map, d_psf, N);
+  otf_kernel<<<grid_for(NN), 256, 0, s>>>(is->spec, is->otf, is->dphi, N);
+  MOAO_TRY(fft2d(is->fft, is->spec, +1, s, &ctx->launches));
+  swap_quadrants_kernel<<<grid_for(NN), 256, 0, s>>>(is->spec, d_psf, N);
   ctx->launches += 5;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;

@@ -16,15 +16,15 @@
 //   otf_tel          intersample.pyx:151-200: inverse FFT2 of |FFT2(pupil)|^2
 //                    over the squared pupil area in pixels
 // The DM geometry and idx are exact integer work on the host; abs2fi and the
-// OTF are N^2 FFTs (cuFFT, complex-to-complex like the tooling's numpy.fft).
+// OTF are N^2 complex FFTs (fft.cu), like the tooling's numpy.fft.
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "context.h"
+#include "fft.h"
 
 namespace moao {
 namespace {
@@ -74,41 +74,41 @@ __device__ __forceinline__ double coord(long i, long N, double scale) {
   return scale * (double)(i + 1 - (N / 2 + 1));
 }
 
-__global__ void influence_kernel(cufftDoubleComplex* out, long N, double ud, double half,
+__global__ void influence_kernel(Cplx* out, long N, double ud, double half,
                                  double x0) {
   const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const long i = e / N, j = e % N;
     const double x = coord_fi(j, N, ud, half), y = coord_fi(i, N, ud, half);
-    out[e] = make_cuDoubleComplex(1.e-6 * exp(-(x * x + y * y) / (2 * x0 * x0)), 0.0);
+    out[e] = Cplx{1.e-6 * exp(-(x * x + y * y) / (2 * x0 * x0)), 0.0};
   }
 }
 
-__global__ void pupil_kernel(cufftDoubleComplex* out, long N, double scale, double obs) {
+__global__ void pupil_kernel(Cplx* out, long N, double scale, double obs) {
   const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const long i = e / N, j = e % N;
     const double xi = coord(i, N, scale), xj = coord(j, N, scale);
     const double r = sqrt(xj * xj + xi * xi);
-    out[e] = make_cuDoubleComplex((r <= 1.0 && r > obs) ? 1.0 : 0.0, 0.0);
+    out[e] = Cplx{(r <= 1.0 && r > obs) ? 1.0 : 0.0, 0.0};
   }
 }
 
 // out[e] = |z[e]|^2 (real), or z[e] <- |z[e]|^2 + 0i
-__global__ void abs2_kernel(cufftDoubleComplex* z, double* out, long total) {
+__global__ void abs2_kernel(Cplx* z, double* out, long total) {
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const double m = sqrt(z[e].x * z[e].x + z[e].y * z[e].y);  // |F|, then squared as b * b
     const double v = m * m;
     if (out) out[e] = v;
-    else z[e] = make_cuDoubleComplex(v, 0.0);
+    else z[e] = Cplx{v, 0.0};
   }
 }
 
 // otf[i][j] = Re(z[j][i]) / N^2 / surface^2  (numpy's ifft2 normalisation, then .T)
-__global__ void otf_out_kernel(const cufftDoubleComplex* z, double* out, long N, double scale) {
+__global__ void otf_out_kernel(const Cplx* z, double* out, long N, double scale) {
   const long total = N * N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
@@ -146,27 +146,24 @@ extern "C" moao_status moao_intersample_inputs(moao_ctx* ctx, long nssp, double 
   MOAO_CUDA_TRY(cudaSetDevice(ctx->device));
   const long NN = N * N;
   const double scale = ud / (Dtel / 2.0);
-  cufftDoubleComplex* z = nullptr;
+  Cplx* z = nullptr;
   double* d = nullptr;
-  if (cudaMalloc(&z, sizeof(cufftDoubleComplex) * NN) != cudaSuccess)
+  if (cudaMalloc(&z, sizeof(Cplx) * NN) != cudaSuccess)
     return set_error(MOAO_ERR_OOM, "intersample_inputs: device buffer");
   if (cudaMalloc(&d, sizeof(double) * NN) != cudaSuccess) {
     cudaFree(z);
     return set_error(MOAO_ERR_OOM, "intersample_inputs: device buffer");
   }
-  cufftHandle plan = 0;
+  Fft2d plan;
   moao_status st = MOAO_OK;
   cudaStream_t s = ctx->stream;
   auto fft = [&](int dir) {
-    if (st == MOAO_OK && cufftExecZ2Z(plan, z, z, dir) != CUFFT_SUCCESS)
-      st = set_error(MOAO_ERR_CUDA, "intersample_inputs: cuFFT");
+    if (st == MOAO_OK) st = fft2d(plan, z, dir, s, &ctx->launches);
   };
-  if (cufftPlan2d(&plan, (int)N, (int)N, CUFFT_Z2Z) != CUFFT_SUCCESS ||
-      cufftSetStream(plan, s) != CUFFT_SUCCESS)
-    st = set_error(MOAO_ERR_CUDA, "intersample_inputs: cuFFT plan");
+  st = fft2d_plan(&plan, N);
   if (st == MOAO_OK && abs2fi) {
     influence_kernel<<<grid_of(NN), 256, 0, s>>>(z, N, ud, Dtel / 2.0, dm.x0);
-    fft(CUFFT_FORWARD);
+    fft(-1);
     abs2_kernel<<<grid_of(NN), 256, 0, s>>>(z, d, NN);
     if (st == MOAO_OK && cudaMemcpyAsync(abs2fi, d, sizeof(double) * NN, cudaMemcpyDeviceToHost,
                                          s) != cudaSuccess)
@@ -177,9 +174,9 @@ extern "C" moao_status moao_intersample_inputs(moao_ctx* ctx, long nssp, double 
     const double pi = 3.14159265358979323846;
     const double surface = Dtel * Dtel * (1 - obs * obs) * pi / 4. / (ud * ud);
     pupil_kernel<<<grid_of(NN), 256, 0, s>>>(z, N, scale, obs);
-    fft(CUFFT_FORWARD);
+    fft(-1);
     abs2_kernel<<<grid_of(NN), 256, 0, s>>>(z, nullptr, NN);
-    fft(CUFFT_INVERSE);
+    fft(+1);
     otf_out_kernel<<<grid_of(NN), 256, 0, s>>>(z, d, N, 1.0 / ((double)NN * surface * surface));
     if (st == MOAO_OK && cudaMemcpyAsync(otf_tel, d, sizeof(double) * NN, cudaMemcpyDeviceToHost,
                                          s) != cudaSuccess)
@@ -190,7 +187,7 @@ extern "C" moao_status moao_intersample_inputs(moao_ctx* ctx, long nssp, double 
     st = set_error(MOAO_ERR_CUDA, "intersample_inputs: kernel launch");
   if (cudaStreamSynchronize(s) != cudaSuccess && st == MOAO_OK)
     st = set_error(MOAO_ERR_CUDA, "intersample_inputs: synchronize");
-  if (plan) cufftDestroy(plan);
+  fft2d_free(&plan);
   cudaFree(z);
   cudaFree(d);
   return st;
