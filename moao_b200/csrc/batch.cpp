@@ -314,6 +314,10 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   DevBuf status, pkbuf;
   PackedPlan plan;
   cudaStream_t ps = nullptr;  // the packed branch
+  // the packed instances' covariance launches, spread over a few streams (small
+  // instances' launches fill the GPU one at a time only partly)
+  constexpr int kCovStreams = 4;
+  std::vector<cudaStream_t> cs;
   // DevBuf frees nothing by itself: release the batch's own buffers on every exit
   struct Release {
     std::vector<DevBuf>& a;
@@ -322,6 +326,7 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     DevBuf& d;
     PackedPlan& e;
     cudaStream_t& f;
+    std::vector<cudaStream_t>& g;
     ~Release() {
       for (DevBuf& x : a) x.release();
       for (DevBuf& x : b) x.release();
@@ -329,8 +334,9 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
       d.release();
       e.release();
       if (f) cudaStreamDestroy(f);
+      for (cudaStream_t x : g) cudaStreamDestroy(x);
     }
-  } release_guard{cmm, ctm, status, pkbuf, plan, ps};
+  } release_guard{cmm, ctm, status, pkbuf, plan, ps, cs};
   size_t total = 0;
   for (int k = 0; k < S; ++k) {
     moao_ctx* sc = subs[k];
@@ -412,13 +418,19 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
     }
     MOAO_TRY(packed_prepare(pv, &plan, ctx->stream));
     MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    for (int k = 0; k < kCovStreams && k < (int)pk.size(); ++k) {
+      cudaStream_t x;
+      MOAO_CUDA_TRY(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      cs.push_back(x);
+    }
     total += pk_bytes;
   }
 
   // ---- capture: fork S streams (and the packed branch) from the context's
   // stream, join at the end. ev[S]: fork; ev[k]: stream k done; ev[S + 1]:
-  // packed branch done.
-  std::vector<cudaEvent_t> ev(S + 2);
+  // packed branch done; ev[S + 2]: the packed branch's covariance fork;
+  // ev[S + 3 + c]: its covariance stream c done.
+  std::vector<cudaEvent_t> ev(S + 3 + cs.size());
   for (auto& e : ev) MOAO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   auto destroy_events = [&] {
     for (auto& e : ev) cudaEventDestroy(e);
@@ -447,13 +459,21 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
   }
   if (ps && ce == cudaSuccess && st == MOAO_OK) {
     ce = cudaStreamWaitEvent(ps, ev[S], 0);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[S + 2], ps);
+    for (size_t c = 0; c < cs.size() && ce == cudaSuccess; ++c)
+      ce = cudaStreamWaitEvent(cs[c], ev[S + 2], 0);
     for (size_t q = 0; q < pk.size() && ce == cudaSuccess && st == MOAO_OK; ++q) {
       const Inst& in = inst[pk[q]];
-      st = launch_matcov(*in.g, pv[q].A, (int)in.n, (int)in.n, 0, 0, (int)pv[q].lda, 1, ps,
+      cudaStream_t x = cs[q % cs.size()];
+      st = launch_matcov(*in.g, pv[q].A, (int)in.n, (int)in.n, 0, 0, (int)pv[q].lda, 1, x,
                          &ctx->launches);
       if (st == MOAO_OK && in.m > 0)
-        st = launch_matcov(*in.g, pv[q].C, (int)in.m, (int)in.n, 0, 0, (int)pv[q].ldc, 3, ps,
+        st = launch_matcov(*in.g, pv[q].C, (int)in.m, (int)in.n, 0, 0, (int)pv[q].ldc, 3, x,
                            &ctx->launches);
+    }
+    for (size_t c = 0; c < cs.size() && ce == cudaSuccess && st == MOAO_OK; ++c) {
+      ce = cudaEventRecord(ev[S + 3 + c], cs[c]);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(ps, ev[S + 3 + c], 0);
     }
     if (ce == cudaSuccess && st == MOAO_OK)
       st = packed_launch(plan, ps, ctx->wait_polls, 2.0,
