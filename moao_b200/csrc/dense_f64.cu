@@ -285,26 +285,41 @@ __global__ void __launch_bounds__(TL::NTHREADS) gemm_f64_kernel(const KParams p)
   }
   cp_wait<0>();
 
-  // Epilogue: C = alpha * acc + beta * C (C is not read when beta == 0).
+  // Epilogue through shared memory (the operand ring is free now): the C tile
+  // is read with coalesced loads, all in flight (only when beta != 0), each
+  // thread combines its accumulators with it in place, and the tile goes back
+  // with coalesced stores, lower part only for a lower C. Leading dimension
+  // BM + 2 keeps the fragment accesses free of bank conflicts.
+  // k4: fragment i covers rows wm + 8 i; k16: acc[2q][j] and acc[2q+1][j] hold
+  // the 4 values of m16 fragment q (rows wm + 16 q + gid and + 8).
+  constexpr int LDC_S = BM + 2;
+  static_assert((size_t)BN * LDC_S * sizeof(double) <= TL::SMEM_BYTES, "C tile exceeds the ring");
+  __syncthreads();
+  double* Cs = smem;
+  const bool read_c = p.beta != 0.0;
+  for (int e = threadIdx.x; e < BM * BN; e += NTHREADS) {
+    const int rr = e % BM, cc = e / BM;
+    const long r = m0 + rr, c = n0 + cc;
+    Cs[cc * LDC_S + rr] = (read_c && r < p.M && c < p.N) ? p.C[c * p.ldc + r] : 0.0;
+  }
+  __syncthreads();
 #pragma unroll
   for (int i = 0; i < MF; ++i) {
-    // k4: fragment i covers rows wm + 8 i; k16: acc[2q][j] and acc[2q+1][j] hold
-    // the 4 values of m16 fragment q (rows wm + 16 q + gid and + 8).
-    const long r = MMA16 ? m0 + wm + (i >> 1) * 16 + (i & 1) * 8 + gid : m0 + wm + i * 8 + gid;
-    if (r >= p.M) continue;
+    const int rr = MMA16 ? wm + (i >> 1) * 16 + (i & 1) * 8 + gid : wm + i * 8 + gid;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const long c = n0 + wn + j * 8 + 2 * tig + h;
-        if (c >= p.N) continue;
-        if (LOWERC && r < c) continue;
-        double* dst = p.C + c * p.ldc + r;
-        double v = p.alpha * acc[i][j][h];
-        if (p.beta != 0.0) v += p.beta * *dst;
-        *dst = v;
+        const int cc = wn + j * 8 + 2 * tig + h;
+        double* d = Cs + cc * LDC_S + rr;
+        *d = read_c ? p.alpha * acc[i][j][h] + p.beta * *d : p.alpha * acc[i][j][h];
       }
-    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < BM * BN; e += NTHREADS) {
+    const int rr = e % BM, cc = e / BM;
+    const long r = m0 + rr, c = n0 + cc;
+    if (r < p.M && c < p.N && !(LOWERC && r < c)) p.C[c * p.ldc + r] = Cs[cc * LDC_S + rr];
   }
 }
 
