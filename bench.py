@@ -818,7 +818,6 @@ def probe_main(args):
                         "leaf_us_per_launch": float(np.median(leaf_us))})
         ctx.set_gemm_tile(1)
         print(json.dumps({"probe": "gemm_tiles", "nssp": args.nssp, "nmeas": nm,
-                          "leaf_threads": os.environ.get("MOAO_LEAF_THREADS", "default"),
                           "cublas_dgemm_tflops": peak, "configs": res}), flush=True)
         return 0
     if args.probe == "matcov_ctm":
