@@ -7,8 +7,9 @@
  * MOAO_COMMON::matcov_tile, MOAO_LAPACK::reconstructor / Cee_Cvv / geadd, the
  * intersample entry points and the FITS helpers then come from this library
  * (moao_b200_compat.hpp), while the drivers keep the reference's own
- * command-line and timer utilities (common/io/arguments.hpp,
- * common/utils/timer.hpp, compiled from the reference tree with the driver).
+ * command-line, timer and matrix-comparison utilities (common/io/arguments.hpp,
+ * common/utils/timer.hpp, common/compute/check_utils.hpp, compiled from the
+ * reference tree with the driver).
  * The standard headers are those the reference's common headers bring in.
  */
 #ifndef COMMON_H
@@ -21,6 +22,7 @@
 #include <string>
 
 #include "moao_b200_compat.hpp"
+#include "compute/check_utils.hpp"
 #include "io/arguments.hpp"
 #include "utils/timer.hpp"
 

@@ -153,3 +153,91 @@ def test_reference_driver_runs_unchanged_on_the_library(tmp_path, built, ctx):
     got = read_fits(os.path.join(out, "psf_oloop0_iloop0_gal0.fits"))
     err = np.max(np.abs(got - psf)) / np.max(np.abs(psf))
     assert err <= 1e-12, err
+
+
+CHECK = os.path.join(ROOT, "oracle", "_ref", "check_moao_lapack_dropin")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(CHECK), reason="reference check program not built")
+def test_reference_check_program_passes_on_the_library(tmp_path, built, ctx):
+    """The reference's own check program (lapack/check_moao_lapack.cpp, compiled
+    unchanged against this library with its own compareMatrices) run on the
+    reference's nx456 two-layer check system against golden FITS files that the
+    reference's own code wrote (oracle/_ref: its Tomo_struct and matcov_tile,
+    its lapack reconstructor and Cee_Cvv, its intersample): every stage it
+    compares (Cmm, Ctm, Ctt, R, Cee, Cvv, PSF) agrees, relative Frobenius norms
+    within the bounds of the FP64 parity tests, and its maximum elementwise
+    relative error within the reference CI's 1e-3 (--accuracy; the default
+    1e-7 is exceeded by any second correct FP64 build on small elements: R's
+    reaches ~4e-5 at kappa ~2e7). For Cmm the program's metric,
+    1 - B/A per element, is 1 wherever the reference evaluates a covariance to
+    exactly 0 (XY terms of aligned WFS pairs whose stencil cancels) and the
+    library to a rounding residue (~1e-20 of the matrix maximum), and large on
+    other nearly cancelling elements: the test checks that every element past
+    1e-3 differs by at most 1e-15 of the matrix maximum."""
+    import oracle as O
+    import systems
+    if not (O.RefTomo.available() and O.RefDense.available()):
+        pytest.skip("oracle/_ref not built")
+    name = "check2"
+    sysp, atm = systems.SYSTEMS[name]()
+    d = str(tmp_path / "sys") + "/"
+    os.makedirs(d)
+    P.write_system(d, sysp, atm)
+    sf, af = d + "sys-params.txt", d + "prof-1-atmos-night0.txt"
+    rt = O.RefTomo(sf, af)
+    info = rt.info
+    nm, nts = info.nmeas, info.nmeasts
+    x, Dx = write_inputs(d, sysp, nts)
+    nact = x.nact
+    # goldens from the reference's own code, laid out as the check program reads them
+    Cmm = np.zeros((nm, nm), order="F")
+    rt.matcov_tile(Cmm, nm, nm, 0, 0, nm, 1)
+    Ctm = np.zeros((nts, nm), order="F")
+    rt.matcov_tile(Ctm, nts, nm, 0, 0, nts, 3)
+    Ctt = np.zeros((nts, nts), order="F")
+    rt.matcov_tile(Ctt, nts, nts, 0, 0, nts, 4)
+    _, R = O.RefDense.reconstructor(Cmm, Ctm)
+    Cee, Cvv, *_ = O.RefDense.cee_cvv(Cmm, Ctt, Ctm, R, Dx)
+    psf = O.RefDense.intersample(Cvv, x.idx, x.abs2fi, x.otf, x.np_, sysp.diam)
+    gold = {"Cmm": Cmm, "Ctm": Ctm, "Ctt": Ctt, "R": R, "Cee": Cee, "Cvv": Cvv}
+    for k, A in gold.items():
+        write_fits(d + k + ".fits", A.T)   # column-major data, NAXIS1 = rows
+    write_fits(d + "psf.fits", psf)
+    gold["psf"] = psf
+    r = subprocess.run([CHECK, f"--sys_path={d}", f"--sys_check={d}", f"--atm_path={d}",
+                        "--compare_all=1", "--accuracy=1e-3"], capture_output=True, text=True,
+                       timeout=600, cwd=str(tmp_path))
+    assert "F norm   :" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+    assert r.returncode == 0 or "bad accuracy" in r.stderr, r.stderr[-2000:]
+    fro = [float(v) for v in r.stdout.split("F norm   :")[1].split()[:7]]
+    mx = [float(v) for v in r.stdout.split("max err  :")[1].split()[:7]]
+    names = ["Cmm", "Ctm", "Ctt", "R", "Cee", "Cvv", "psf"]
+    rel = {n: f / np.linalg.norm(gold[n]) for n, f in zip(names, fro)}
+    for n, e in zip(names[1:], mx[1:]):
+        assert e <= 1e-3, (n, e)
+    ours = np.zeros((nm, nm), order="F")
+    t = M.Tomo(sf, af)
+    M.matcov_tile(ours, nm, nm, 0, 0, nm, t, 1, ctx=ctx)
+    nz = ours != 0
+    big = np.zeros_like(nz)
+    big[nz] = np.abs(1 - Cmm[nz] / ours[nz]) > 1e-3
+    big |= (~nz) & (np.abs(Cmm) > 1e-3)
+    gap = np.abs(ours[big] - Cmm[big])
+    assert np.all(gap <= 1e-15 * np.abs(Cmm).max()), (int(big.sum()), float(gap.max()))
+    S = np.tril(Cmm) + np.tril(Cmm, -1).T
+    kappa = np.linalg.cond(S)
+    eps = np.finfo(float).eps
+    bound = {"Cmm": 1e-11, "Ctm": 1e-11, "Ctt": 1e-11, "R": max(1e-10, 50 * kappa * eps),
+             "Cee": 200 * np.sqrt(nm) * eps * np.linalg.norm(Ctt) / np.linalg.norm(Cee),
+             "Cvv": 200 * np.sqrt(nm) * eps * np.linalg.norm(Ctt) / np.linalg.norm(Cee),
+             "psf": 1e-9}
+    for n in names:
+        assert rel[n] <= bound[n], (n, rel[n], bound[n], r.stdout[-1500:])
+    report = os.environ.get("MOAO_PARITY_REPORT")
+    if report:
+        import json
+        with open(report, "a") as f:
+            f.write(json.dumps({"test": "reference_check_program", "system": name,
+                                "rel_fro": rel, "bound": bound}) + "\n")
