@@ -20,7 +20,9 @@
 //
 // MOAO_B200_PRECISION=mixed selects the mixed-precision reconstructor for
 // reconstructor<double> (FP64 otherwise); the LGS constant blocks of the tomo
-// last used for a type-1 matcov_tile of the same size are declared as offsets.
+// last used for a type-1 matcov_tile of the same size are declared as offsets,
+// and a build whose estimated error of R exceeds MOAO_B200_ACCURACY (default
+// 1e-5; 0 turns the check off) is redone on the FP64 path.
 #ifndef MOAO_B200_COMPAT_HPP
 #define MOAO_B200_COMPAT_HPP
 

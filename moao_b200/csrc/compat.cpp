@@ -41,7 +41,13 @@ Compat& compat() {
       std::exit(1);
     }
     c.mixed = prec && std::string(prec) == "mixed";
-    if (c.mixed) moao_ctx_set_host_precision(c.ctx, MOAO_PREC_MIXED);
+    if (c.mixed) {
+      moao_ctx_set_host_precision(c.ctx, MOAO_PREC_MIXED);
+      // the accuracy guard: R's estimated error above the target (default
+      // 1e-5, MOAO_B200_ACCURACY, 0 turns it off) falls back to FP64
+      const char* acc = std::getenv("MOAO_B200_ACCURACY");
+      moao_ctx_set_accuracy(c.ctx, acc ? std::atof(acc) : 1e-5);
+    }
   });
   return c;
 }
