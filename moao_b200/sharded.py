@@ -137,7 +137,7 @@ def factor_and_solve(lay: Layout, A, B, ops, dist=None, group=None) -> int:
     for k in range(lay.nt):
         k0, kb, o = k * nb, lay.width(k), lay.owner(k)
         rest = n - k0 - kb
-        buf = torch.empty(1 + kb * rest + kb * m, dtype=f64, device=dev)
+        buf = torch.empty(1 + (kb * rest + kb * m if P > 1 else 0), dtype=f64, device=dev)
         if rank == o:
             lc = lay.local_col(k)
             Lk = torch.zeros((kb, kb), dtype=f64, device=dev)
@@ -154,20 +154,30 @@ def factor_and_solve(lay: Layout, A, B, ops, dist=None, group=None) -> int:
                     ops.gemm(True, False, m, kb, kb, 1.0, (B, lc, 0), (Lk, 0, 0), 0.0, (W, 0, 0))
                     B[lc:lc + kb, :] = W
             buf[0] = float(info + k0 if info else 0)
-            if rest:
-                buf[1:1 + kb * rest].view(kb, rest).copy_(A[lc:lc + kb, k0 + kb:n])
-            if m:
-                buf[1 + kb * rest:].view(kb, m).copy_(B[lc:lc + kb, :])
+            if P > 1:
+                if rest:
+                    buf[1:1 + kb * rest].view(kb, rest).copy_(A[lc:lc + kb, k0 + kb:n])
+                if m:
+                    buf[1 + kb * rest:].view(kb, m).copy_(B[lc:lc + kb, :])
         bcast(buf, o)
         info = int(buf[0].item())
         if info:
             return info
-        Lp = buf[1:1 + kb * rest].view(kb, rest)   # L(k0+kb : n, panel k), ld rest
-        Xk = buf[1 + kb * rest:].view(kb, m)       # X_k, ld m
         later = [j for j in owned if j > k]
         if not later:
             continue
-        for j in later:  # A(j0:n, panel j) -= L(j0:n, k) L(j0:j0+jb, k)^T, lower on the diagonal block
+        if P == 1:  # the later panels are the whole trailing matrix: one lower SYRK
+            lc = lay.local_col(k)
+            Lv, Xv = (A, lc, k0 + kb), (B, lc, 0)  # L(k0+kb : n, panel k) and X_k in place
+            ops.gemm(True, True, rest, rest, kb, -1.0, Lv, Lv, 1.0,
+                     (A, lay.local_col(later[0]), k0 + kb))
+            if m:
+                ops.gemm(True, False, m, rest, kb, -1.0, Xv, Lv, 1.0,
+                         (B, lay.local_col(later[0]), 0))
+            continue
+        Lp = buf[1:1 + kb * rest].view(kb, rest)   # L(k0+kb : n, panel k), ld rest
+        Xk = buf[1 + kb * rest:].view(kb, m)       # X_k, ld m
+        for j in later:  # A(j0:n, panel j) -= L(j0:n, k) L(j0:j0+jb, k)^T, lower on its diagonal block
             j0, jb = j * nb, lay.width(j)
             r = j0 - (k0 + kb)
             ops.gemm(True, True, n - j0, jb, kb, -1.0, (Lp, 0, r), (Lp, 0, r), 1.0,
