@@ -79,6 +79,9 @@ def parse():
     p.add_argument("--no-pairs", action="store_true",
                    help="skip the measured CPU-vs-GPU full builds of the small systems")
     p.add_argument("--e2e-steps", type=int, default=5, help="builds timed through the host path")
+    p.add_argument("--tc-pair", type=int, default=-1, choices=[-1, 0, 1],
+                   help="tensor-core products on CTA pairs (1) or single CTAs (0); "
+                        "-1: the library's default")
     p.add_argument("--probe", default=None,
                    choices=["matcov_ctm", "build_fp64", "build_mixed", "cee_fp64", "cee_mixed",
                             "gemm_tiles"],
@@ -778,6 +781,8 @@ def probe_main(args):
     P.write_system(d, sp, ap)
     torch.cuda.set_device(0)
     ctx = M.Context(0)
+    if args.tc_pair >= 0:
+        ctx.set_tc_pair(args.tc_pair)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     ctx.set_block(args.nb or 1024)
     t = M.Tomo(os.path.join(d, "sys-params.txt"), os.path.join(d, "prof-1-atmos-night0.txt"))
@@ -925,6 +930,8 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = M.Context(dev)
+    if args.tc_pair >= 0:
+        ctx.set_tc_pair(args.tc_pair)
     ctx.set_stream(stream.cuda_stream)
     nb_main = args.nb or 1024
     ctx.set_block(nb_main)

@@ -107,6 +107,7 @@ SIGNATURES = {
     "moao_ctx_set_accuracy": (i32, [vp, C.c_double]),
     "moao_ctx_set_lookahead_max": (i32, [vp, i32]),
     "moao_ctx_set_gemm_tile": (i32, [vp, i32]),
+    "moao_ctx_set_tc_pair": (i32, [vp, i32]),
     "moao_ctx_set_host_cache": (i32, [vp, i32]),
     "moao_dense_potrf_inv": (i32, [vp, i64, vp, i64, vp, i64, C.POINTER(i32)]),
     "moao_dense_gemm": (i32, [vp, i32, i32, i64, i64, i64, C.c_double, vp, i64, vp, i64,

@@ -193,6 +193,11 @@ class Context:
         moao_ctx_set_gemm_tile); same results."""
         check(lib().moao_ctx_set_gemm_tile(self._h, int(cfg)), "moao_ctx_set_gemm_tile")
 
+    def set_tc_pair(self, on: bool = True):
+        """Tensor-core products of the mixed path on CTA pairs (256 x 256 tiles,
+        the default) or single CTAs (moao_ctx_set_tc_pair); same results."""
+        check(lib().moao_ctx_set_tc_pair(self._h, int(bool(on))), "moao_ctx_set_tc_pair")
+
     def set_lookahead_max(self, sms: int = 8):
         """SMs left to the next diagonal block in the last panels (see
         moao_ctx_set_lookahead_max)."""

@@ -571,6 +571,13 @@ moao_status moao_ctx_set_gemm_tile(moao_ctx* c, int cfg) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_tc_pair(moao_ctx* c, int on) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_tc_pair: null");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->tc_pair = on != 0;
+  return MOAO_OK;
+}
+
 moao_status moao_ctx_set_host_cache(moao_ctx* c, int on) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_host_cache: null");
   std::lock_guard<std::mutex> lk(c->mu);

@@ -116,6 +116,7 @@ moao_status tc_update(moao_ctx* ctx, const TcTensor* A, int a_row0, int ka, cons
   TcGemm g;
   g.max_ctas = max_ctas;
   g.spin_limit = ctx->wait_polls;
+  g.pair = ctx->tc_pair;
   g.kind = A[0].kind;
   g.erow = erow;
   g.ecol = ecol;
@@ -207,6 +208,7 @@ moao_status block_product(moao_ctx* ctx, const Scales& sc, const TcTensor* A, co
   MOAO_TRY(split_block(sc, W, ldw, m, kb, slices, xr, ldx, ctx->stream));
   TcGemm g;
   g.spin_limit = ctx->wait_polls;
+  g.pair = ctx->tc_pair;
   g.kind = A[0].kind;
   g.epi = kTcEpiF32;
   g.M = m;
@@ -313,6 +315,7 @@ moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTenso
     for (size_t b0 = 0; b0 < pairs.size(); b0 += pair_cap) {
       TcGemm g;
       g.spin_limit = ctx->wait_polls;
+      g.pair = ctx->tc_pair;
       g.kind = kTcI8;
       g.epi = kTcEpiF64Scaled;
       g.M = M;

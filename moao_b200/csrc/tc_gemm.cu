@@ -3,13 +3,14 @@
 //   C[M x N] (+)= sum over segments s of  A_s[M x K_s] * B_s[N x K_s]^T
 //
 // Both operands are K-major (rows of K contiguous elements) and are fetched by
-// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a 3-stage
-// shared-memory ring; one thread issues tcgen05.mma (M = 128, N = 128) into a
-// TMEM accumulator; four epilogue warps drain TMEM with tcgen05.ld and update
-// C in global memory with coalesced column stores. The K dimension is a list of
-// segments, each naming its own A and B tensor (slices) and K offset, so that a
-// split-precision product (hi*hi + hi*lo + lo*hi, or the int8 slice pairs of one
-// Ozaki diagonal) accumulates in one accumulator and C is read and written once.
+// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a shared-memory
+// ring; one thread issues tcgen05.mma into a double-buffered TMEM accumulator;
+// eight epilogue warps drain TMEM with tcgen05.ld and update C. A tile is 128 x
+// 256 on one CTA, or 256 x 256 on a cluster of two CTAs (M = 256 MMAs,
+// cta_group::2). The K dimension is a list of segments, each naming its own A
+// and B tensor (slices) and K offset, so that a split-precision product
+// (hi*hi + hi*lo + lo*hi, or the int8 slice pairs of one Ozaki diagonal)
+// accumulates in one accumulator and C is read and written once.
 //
 // Kinds:
 //   BF16 -> FP32 accumulate (kind::f16);   epilogue C32 = alpha*acc + beta*C32
@@ -35,21 +36,37 @@
 namespace moao {
 namespace {
 
-constexpr int TBM = 128, TBN = 256;
-constexpr int KBYTES = 128;             // bytes of K per stage row (one 128B swizzle atom)
-constexpr int STAGES = 4;
-constexpr int A_TILE = TBM * KBYTES;    // 16 KB
-constexpr int B_TILE = TBN * KBYTES;    // 32 KB
-constexpr int STAGE_BYTES = A_TILE + B_TILE;
-constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quadrant
+constexpr int TBM = 128, TBN = 256;      // accumulator of one CTA: TMEM lanes x columns
+constexpr int BOX_ROWS = 128;            // rows of one TMA box (A and B operands alike)
+constexpr int KBYTES = 128;              // bytes of K per stage row (one 128B swizzle atom)
+constexpr int A_TILE = TBM * KBYTES;     // 16 KB
+constexpr int BOX_BYTES = BOX_ROWS * KBYTES;
+constexpr int EPI_WARPS = 8;             // two warps per TMEM lane quadrant
 constexpr int THREADS = (4 + EPI_WARPS) * 32;
-constexpr int ACC_COLS = TBN;           // fp32 / int32 columns of one accumulator
-constexpr int TMEM_COLS = 2 * ACC_COLS; // double-buffered accumulator
-constexpr int STAGE_C = 32 * 32 * 4;    // per epilogue warp: one 32x32 FP32 chunk for TMA
-constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ +
-                       EPI_WARPS * 32 * sizeof(float) /*per-warp column scales*/ +
-                       (size_t)EPI_WARPS * STAGE_C /*per-warp C staging*/;
+constexpr int ACC_COLS = TBN;            // fp32 / int32 columns of one accumulator
+constexpr int TMEM_COLS = 2 * ACC_COLS;  // double-buffered accumulator
+constexpr int STAGE_C = 32 * 32 * 4;     // per epilogue warp: one 32x32 FP32 chunk for TMA
 constexpr unsigned long long kSpinLimit = 1ull << 28;  // default polls of a bounded wait
+
+// PAIR = 0: one CTA computes a 128 x 256 tile of C.
+// PAIR = 1: a cluster of two CTAs computes a 256 x 256 tile with M = 256 MMAs
+// (tcgen05.mma.cta_group::2): each CTA holds 128 rows of A and 128 rows of B in
+// its shared memory and 128 rows of the accumulator in its TMEM; the first CTA
+// of the pair issues the MMAs for both. Per SM a stage then carries 32 KB of
+// operands instead of 48 KB for the same tensor work.
+template <int PAIR>
+struct TcCfg {
+  static constexpr int B_ROWS = PAIR ? TBN / 2 : TBN;  // B rows held by one CTA
+  static constexpr int B_TILE = B_ROWS * KBYTES;
+  static constexpr int STAGE_BYTES = A_TILE + B_TILE;
+  static constexpr int STAGES = PAIR ? 6 : 4;
+  static constexpr int TILE_M = PAIR ? 2 * TBM : TBM;  // rows of C per tile
+  static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ +
+                                 EPI_WARPS * 32 * sizeof(float) /*per-warp column scales*/ +
+                                 (size_t)EPI_WARPS * STAGE_C /*per-warp C staging*/;
+  static_assert(SMEM <= 232448, "shared memory per CTA");
+  static_assert(2 * STAGES + 5 <= 31, "barrier area");
+};
 
 struct __align__(64) TcParams {
   CUtensorMap mapA[kTcMaxMaps];
@@ -70,6 +87,7 @@ struct __align__(64) TcParams {
   const int* erow;         // INT8: per-row exponent of A (length M, indexed by r)
   const int* ecol;         // INT8: per-column exponent of B (length N)
   int shift;
+  int tile_m;              // rows of C per tile (128, or 256 for CTA pairs)
   int tiles_m, tiles_n;
   int total_tiles;         // tiles that intersect the written part of C
   int* err;
@@ -92,6 +110,31 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Arrive on a barrier named by its shared::cluster address (this CTA's or the
+// pair's other CTA's), releasing this thread's prior accesses to the cluster.
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t caddr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(caddr)
+               : "memory");
+}
+
+// shared::cluster address of the variable at shared address saddr in CTA rank.
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+
+// Every thread of both CTAs of the cluster (release / acquire on shared memory).
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;\nbarrier.cluster.wait.acquire;\n" ::: "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -123,6 +166,17 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
       "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Load into this CTA's shared memory, the bytes counted on the barrier at
+// shared::cluster address bar (in either CTA of the pair). No multicast.
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int x, int y,
+                                                 uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
       : "memory");
 }
 
@@ -166,6 +220,25 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t a, uint64_t b, ui
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
+// M = 256 across the pair: A and B descriptors name this CTA's stage; the
+// other CTA's tiles sit at the same shared-memory offsets. No output lane is
+// disabled (all-zero mask).
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem, uint64_t a, uint64_t b,
+                                             uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n}\n"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem, uint64_t a, uint64_t b,
+                                            uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n}\n"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u));
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
@@ -173,23 +246,31 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
       : "memory");
 }
 
-// Instruction descriptors (M = 128, N = 256, both operands K-major).
+// Arrives (once each) on the barrier at this shared offset in both CTAs of the
+// pair when every MMA the thread issued before has completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+      "[%0], %1;\n" ::"r"(smem_u32(bar)),
+      "h"((unsigned short)3)
+      : "memory");
+}
+
+// Instruction descriptors (N = 256, both operands K-major; M = 128 for one
+// CTA, 256 for a pair).
 //   bits 4-5 D format (1 F32, 2 S32), 7-9 A format, 10-12 B format
 //   (kind::f16: 1 BF16; kind::i8: 1 S8), 15/16 A/B major (0 = K),
 //   17-22 N >> 3, 24-28 M >> 4.
-constexpr uint32_t idesc_of(int dfmt, int abfmt) {
+constexpr uint32_t idesc_of(int dfmt, int abfmt, int m) {
   return (uint32_t)(dfmt << 4) | (uint32_t)(abfmt << 7) | (uint32_t)(abfmt << 10) |
-         (uint32_t)((TBN >> 3) << 17) | (uint32_t)((TBM >> 4) << 24);
+         (uint32_t)((TBN >> 3) << 17) | (uint32_t)((m >> 4) << 24);
 }
-constexpr uint32_t kIdescBf16 = idesc_of(1, 1);
-constexpr uint32_t kIdescF16 = idesc_of(1, 0);
-constexpr uint32_t kIdescI8 = idesc_of(2, 1);
 
 // First row tile of column tile nt that reaches the written (lower) part.
 __device__ __forceinline__ int first_mt(const TcParams& p, int nt) {
   if (!p.lower) return 0;
-  const int num = nt * TBN - p.diag_off - (TBM - 1);
-  return num <= 0 ? 0 : (num + TBM - 1) / TBM;
+  const int num = nt * TBN - p.diag_off - (p.tile_m - 1);
+  return num <= 0 ? 0 : (num + p.tile_m - 1) / p.tile_m;
 }
 
 // v-th tile (in column-major tile order over the tiles that are written).
@@ -212,8 +293,15 @@ __device__ __forceinline__ void decode_tile(const TcParams& p, int v, int* mt, i
 
 // Persistent warp-specialised kernel: warp 0 TMA producer, warp 1 MMA issuer,
 // warp 2 TMEM allocator, warps 4.. epilogue. The accumulator is double-buffered
-// in TMEM so the epilogue of one tile overlaps the main loop of the next.
+// in TMEM so the epilogue of one tile overlaps the main loop of the next. With
+// PAIR, a cluster of two CTAs walks the tiles together: both load their halves
+// of the operands (the bytes counted on the first CTA's barrier), the first
+// CTA's issuer runs the MMAs and its commits reach both CTAs, and both
+// epilogues drain their own TMEM and report to the first CTA.
+template <int PAIR>
 __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
+  using Cfg = TcCfg<PAIR>;
+  constexpr int STAGES = Cfg::STAGES, STAGE_BYTES = Cfg::STAGE_BYTES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -229,6 +317,9 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
   float* c_stage = col_scale + EPI_WARPS * 32;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t crank = PAIR ? cluster_rank() : 0;        // 0: the CTA that issues MMAs
+  const int group = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int ngroups = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -237,18 +328,26 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], EPI_WARPS);
+      mbar_init(&tempty_bar[b], PAIR ? 2 * EPI_WARPS : EPI_WARPS);
     }
     mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 2) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    if (PAIR) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(TMEM_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(TMEM_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
   }
   __syncthreads();
+  if (PAIR) cluster_sync_all();  // both CTAs' barriers initialised, both allocations done
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
@@ -257,12 +356,14 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer
+    const uint32_t full0 = PAIR ? cluster_addr(smem_u32(full_bar), 0) : 0;
     int it = 0;
     bool ok = true;
-    for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x) {
+    for (int v = group; v < p.total_tiles && ok; v += ngroups) {
       int mt, nt;
       decode_tile(p, v, &mt, &nt);
-      const int m0 = mt * TBM, n0 = nt * TBN;
+      const int m0 = mt * Cfg::TILE_M + (int)crank * TBM;
+      const int n0 = nt * TBN + (int)crank * Cfg::B_ROWS;
       for (int s = 0; s < p.nseg && ok; ++s) {
         const TcSegment sg = p.seg[s];
         for (int kb = 0; kb < sg.nk; ++kb, ++it) {
@@ -274,55 +375,78 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
           }
           uint8_t* sa = smem + st * STAGE_BYTES;
           uint8_t* sb = sa + A_TILE;
-          mbar_expect_tx(&full_bar[st], STAGE_BYTES);
-          tma_load_2d(sa, &p.mapA[sg.a], sg.ka + kb * sg.kstep, p.a_row0 + m0, &full_bar[st]);
-          tma_load_2d(sb, &p.mapB[sg.b], sg.kb + kb * sg.kstep, p.b_row0 + n0, &full_bar[st]);
+          const int xa = sg.ka + kb * sg.kstep, xb = sg.kb + kb * sg.kstep;
+          if (PAIR) {
+            if (crank == 0) mbar_expect_tx(&full_bar[st], 2 * STAGE_BYTES);
+            const uint32_t fb = full0 + (uint32_t)(st * 8);
+            tma_load_2d_pair(sa, &p.mapA[sg.a], xa, p.a_row0 + m0, fb);
+            tma_load_2d_pair(sb, &p.mapB[sg.b], xb, p.b_row0 + n0, fb);
+          } else {
+            mbar_expect_tx(&full_bar[st], STAGE_BYTES);
+            tma_load_2d(sa, &p.mapA[sg.a], xa, p.a_row0 + m0, &full_bar[st]);
+            tma_load_2d(sb, &p.mapB[sg.b], xb, p.b_row0 + n0, &full_bar[st]);
+            tma_load_2d(sb + BOX_BYTES, &p.mapB[sg.b], xb, p.b_row0 + n0 + BOX_ROWS, &full_bar[st]);
+          }
         }
       }
     }
-    // Never leave the CTA with a bulk copy still writing its shared memory.
+    // Never leave the CTA with a bulk copy still writing shared memory: wait for
+    // the last stages to land (their full barriers) or, in the second CTA of a
+    // pair, whose loads are counted on the first CTA's barriers, to be consumed.
     for (int j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
       const int st = j % STAGES;
-      for (unsigned long long i = 0;
-           i < kSpinLimit && !mbar_try_wait(&full_bar[st], (j / STAGES) & 1); ++i) {
+      uint64_t* bar = (PAIR && crank != 0) ? &empty_bar[st] : &full_bar[st];
+      for (unsigned long long i = 0; i < kSpinLimit && !mbar_try_wait(bar, (j / STAGES) & 1); ++i) {
       }
     }
   } else if (warp == 1 && lane == 0) {
-    // ---------------- MMA issuer
-    const uint32_t idesc =
-        (p.kind == kTcBf16) ? kIdescBf16 : (p.kind == kTcF16 ? kIdescF16 : kIdescI8);
-    int it = 0, tc = 0;
-    bool ok = true;
-    for (int v = blockIdx.x; v < p.total_tiles && ok; v += gridDim.x, ++tc) {
-      const int buf = tc & 1;
-      const uint32_t use = tc >> 1;
-      if (use > 0 && !mbar_wait(&tempty_bar[buf], (use - 1) & 1, p.err, 4, p.spin_limit)) break;
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t acc = tmem + (uint32_t)(buf * ACC_COLS);
-      for (int k = 0; k < kblocks; ++k, ++it) {
-        const int st = it % STAGES;
-        if (!mbar_wait(&full_bar[st], (it / STAGES) & 1, p.err, 2, p.spin_limit)) {
-          ok = false;
-          break;
-        }
+    if (!PAIR || crank == 0) {
+      // ---------------- MMA issuer
+      const uint32_t idesc =
+          (p.kind == kTcBf16) ? idesc_of(1, 1, Cfg::TILE_M)
+                              : (p.kind == kTcF16 ? idesc_of(1, 0, Cfg::TILE_M)
+                                                  : idesc_of(2, 1, Cfg::TILE_M));
+      int it = 0, tc = 0;
+      bool ok = true;
+      for (int v = group; v < p.total_tiles && ok; v += ngroups, ++tc) {
+        const int buf = tc & 1;
+        const uint32_t use = tc >> 1;
+        if (use > 0 && !mbar_wait(&tempty_bar[buf], (use - 1) & 1, p.err, 4, p.spin_limit)) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const uint32_t sa = smem_u32(smem + st * STAGE_BYTES);
-        const uint64_t da = sw128_desc(sa), db = sw128_desc(sa + A_TILE);
+        const uint32_t acc = tmem + (uint32_t)(buf * ACC_COLS);
+        for (int k = 0; k < kblocks; ++k, ++it) {
+          const int st = it % STAGES;
+          if (!mbar_wait(&full_bar[st], (it / STAGES) & 1, p.err, 2, p.spin_limit)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t sa = smem_u32(smem + st * STAGE_BYTES);
+          const uint64_t da = sw128_desc(sa), db = sw128_desc(sa + A_TILE);
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-          const uint64_t off = (uint64_t)((kk * 32) >> 4);
-          const uint32_t accum = (k | kk) ? 1u : 0u;
-          if (p.kind != kTcI8) mma_f16(acc, da + off, db + off, idesc, accum);
-          else mma_i8(acc, da + off, db + off, idesc, accum);
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t off = (uint64_t)((kk * 32) >> 4);
+            const uint32_t accum = (k | kk) ? 1u : 0u;
+            if (PAIR) {
+              if (p.kind != kTcI8) mma_f16_pair(acc, da + off, db + off, idesc, accum);
+              else mma_i8_pair(acc, da + off, db + off, idesc, accum);
+            } else {
+              if (p.kind != kTcI8) mma_f16(acc, da + off, db + off, idesc, accum);
+              else mma_i8(acc, da + off, db + off, idesc, accum);
+            }
+          }
+          if (PAIR) mma_commit_pair(&empty_bar[st]);
+          else mma_commit(&empty_bar[st]);
         }
-        mma_commit(&empty_bar[st]);
+        if (!ok) break;  // this tile's accumulator is incomplete: never hand it on
+        if (PAIR) mma_commit_pair(&tfull_bar[buf]);
+        else mma_commit(&tfull_bar[buf]);
       }
-      if (!ok) break;  // this tile's accumulator is incomplete: never hand it on
-      mma_commit(&tfull_bar[buf]);
+      // Every MMA this thread issued has finished writing TMEM (both CTAs' in a
+      // pair) before the CTAs free it, also when a wait gave up mid-tile.
+      if (PAIR) mma_commit_pair(drain_bar);
+      else mma_commit(drain_bar);
     }
-    // Every MMA this thread issued has finished writing TMEM before the CTA
-    // frees it, also when a wait gave up in the middle of a tile.
-    mma_commit(drain_bar);
     for (unsigned long long i = 0; i < kSpinLimit && !mbar_try_wait(drain_bar, 0); ++i) {
     }
   } else if (warp >= 4) {
@@ -330,11 +454,12 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
     // half of the tile's columns
     const int q = warp & 3;
     const int half = (warp - 4) >> 2;
+    const uint32_t tempty0 = PAIR ? cluster_addr(smem_u32(tempty_bar), 0) : 0;
     int tc = 0;
-    for (int v = blockIdx.x; v < p.total_tiles; v += gridDim.x, ++tc) {
+    for (int v = group; v < p.total_tiles; v += ngroups, ++tc) {
       int mt, nt;
       decode_tile(p, v, &mt, &nt);
-      const int m0 = mt * TBM, n0 = nt * TBN;
+      const int m0 = mt * Cfg::TILE_M + (int)crank * TBM, n0 = nt * TBN;
       const int buf = tc & 1;
       // every lane waits; the warp leaves together if any lane gave up
       const bool got = mbar_wait(&tfull_bar[buf], (tc >> 1) & 1, p.err, 3, p.spin_limit);
@@ -443,16 +568,24 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
       // release this accumulator buffer to the MMA issuer
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
+      if (lane == 0) {
+        if (PAIR) mbar_arrive_cluster(tempty0 + (uint32_t)(buf * 8));
+        else mbar_arrive(&tempty_bar[buf]);
+      }
     }
     // every reduction into C complete before the CTA's shared memory goes away
     if (p.c_tma && lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
   }
   __syncthreads();
+  if (PAIR) cluster_sync_all();  // neither CTA leaves while the other may still signal it
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 2) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(TMEM_COLS));
+    if (PAIR)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                   "r"(TMEM_COLS));
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                   "r"(TMEM_COLS));
   }
 }
 
@@ -485,7 +618,9 @@ moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows,
     return set_error(MOAO_ERR_BAD_ARG, "tc map: bad extents");
   cuuint64_t dims[2] = {(cuuint64_t)kcols, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)(row_stride_elems * esz)};
-  cuuint32_t box[2] = {(cuuint32_t)(KBYTES / esz), (cuuint32_t)box_rows};
+  // Every box is 128 rows; a B operand's 256-row tile is two boxes (one per CTA
+  // of a pair).
+  cuuint32_t box[2] = {(cuuint32_t)(KBYTES / esz), (cuuint32_t)BOX_ROWS};
   cuuint32_t estr[2] = {1, 1};
   const CUtensorMapDataType dt = kind == kTcBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                  : kind == kTcF16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
@@ -552,14 +687,18 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   p.shift = g.shift;
   p.err = g.err;
   p.spin_limit = g.spin_limit > 0 ? g.spin_limit : kSpinLimit;
-  p.tiles_m = (int)((g.M + TBM - 1) / TBM);
+  // Pairs of CTAs (256-row tiles) when asked for and C has more than one
+  // 128-row tile; a grid capped below four CTAs keeps single CTAs.
+  const bool pair = g.pair && g.M > TBM && (g.max_ctas <= 0 || g.max_ctas >= 4);
+  p.tile_m = pair ? TcCfg<1>::TILE_M : TcCfg<0>::TILE_M;
+  p.tiles_m = (int)((g.M + p.tile_m - 1) / p.tile_m);
   p.tiles_n = (int)((g.N + TBN - 1) / TBN);
   long total = 0;
   for (int nt = 0; nt < p.tiles_n; ++nt) {
     long first = 0;
     if (g.lower) {
-      const long num = (long)nt * TBN - g.diag_off - (TBM - 1);
-      first = num <= 0 ? 0 : (num + TBM - 1) / TBM;
+      const long num = (long)nt * TBN - g.diag_off - (p.tile_m - 1);
+      first = num <= 0 ? 0 : (num + p.tile_m - 1) / p.tile_m;
     }
     total += std::max(0L, (long)p.tiles_m - first);
   }
@@ -589,10 +728,43 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (num_sms <= 0) num_sms = 148;
   }
-  static std::atomic<unsigned long long> configured{0};
-  MOAO_CUDA_TRY(set_smem_limit(tc_gemm_kernel, (int)SMEM, configured));
-  const long ctas = std::min<long>(total, g.max_ctas > 0 ? std::min(g.max_ctas, num_sms) : num_sms);
-  tc_gemm_kernel<<<(unsigned)ctas, THREADS, SMEM, s>>>(p);
+  if (!pair) {
+    static std::atomic<unsigned long long> configured{0};
+    MOAO_CUDA_TRY(set_smem_limit(tc_gemm_kernel<0>, (int)TcCfg<0>::SMEM, configured));
+    const long ctas =
+        std::min<long>(total, g.max_ctas > 0 ? std::min(g.max_ctas, num_sms) : num_sms);
+    tc_gemm_kernel<0><<<(unsigned)ctas, THREADS, TcCfg<0>::SMEM, s>>>(p);
+  } else {
+    static std::atomic<unsigned long long> configured{0};
+    MOAO_CUDA_TRY(set_smem_limit(tc_gemm_kernel<1>, (int)TcCfg<1>::SMEM, configured));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = TcCfg<1>::SMEM;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // Pairs that can be resident at once (an SM without a partner in its
+    // cluster group stays idle), looked up once per device.
+    static std::atomic<int> resident[64] = {};
+    int dev = 0;
+    MOAO_CUDA_TRY(cudaGetDevice(&dev));
+    int groups = dev < 64 ? resident[dev].load() : 0;
+    if (groups <= 0) {
+      cfg.gridDim = dim3((unsigned)(num_sms & ~1));
+      MOAO_CUDA_TRY(cudaOccupancyMaxActiveClusters(&groups, tc_gemm_kernel<1>, &cfg));
+      if (groups <= 0) groups = num_sms / 2;
+      if (dev < 64) resident[dev].store(groups);
+    }
+    if (g.max_ctas > 0) groups = std::min(groups, g.max_ctas / 2);
+    groups = (int)std::min<long>(groups, total);
+    cfg.gridDim = dim3((unsigned)(2 * groups));
+    MOAO_CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<1>, p));
+  }
   if (launches) ++*launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
@@ -646,6 +818,7 @@ extern "C" moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long 
   g.erow = erow;
   g.ecol = ecol;
   g.shift = shift;
+  g.pair = ctx->tc_pair;
   MOAO_TRY(ctx->ws_info.ensure(2 * sizeof(int)));
   int* err = ctx->ws_info.as<int>() + 1;
   MOAO_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));

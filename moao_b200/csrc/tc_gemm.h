@@ -22,7 +22,7 @@ struct TcTensor {
   alignas(64) CUtensorMap map;
   int kind = 0;
   int kstep = 0;     // K elements per pipeline stage (64 bf16, 128 int8)
-  int box_rows = 0;  // rows per TMA box: 128 for an A operand, 256 for a B operand
+  int box_rows = 0;  // role: 128 for an A operand, 256 for a B operand
 };
 
 // One K segment: A tensor a over K elements [ka, ka + nk*kstep) times B tensor
@@ -54,11 +54,14 @@ struct TcGemm {
   int shift = 0;
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
   int max_ctas = 0;            // cap on the persistent grid (0: one CTA per SM)
+  int pair = 0;                // 1: 256 x 256 tiles on clusters of two CTAs where M > 128
+                               // (the context's tc_pair, on by default)
   unsigned long long spin_limit = 0;  // polls of each bounded wait (0: 2^28)
 };
 
 // Describes a row-major (K-contiguous) device matrix for TMA. The output tile is
-// 128 x 256: A operands use boxes of 128 rows, B operands boxes of 256 rows.
+// 128 x 256 (256 x 256 on a pair of CTAs): box_rows names the operand's role,
+// 128 for A and 256 for B; the TMA boxes are 128 rows either way.
 moao_status make_tc_map(TcTensor* t, const void* base, int kind, long long rows, long long kcols,
                         long long row_stride_elems, int box_rows = 128);
 moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches);

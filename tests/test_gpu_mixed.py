@@ -170,6 +170,33 @@ def test_mixed_lookahead_gives_the_same_result(ctx):
     assert torch.equal(outs[0][0], outs[1][0])
 
 
+@pytest.mark.parametrize("fmt", ["f16x2", "bf16x3"])
+def test_mixed_on_cta_pairs_gives_the_same_result(ctx, fmt):
+    """Tensor-core products on clusters of two CTAs (256 x 256 tiles, M = 256
+    MMAs) against one CTA per 128 x 256 tile: every product sums the same terms
+    in the same K order, so R and the factor come out bit-identical (fp16
+    slice products and the int8 residual); the reported residual norm is a
+    sum accumulated with atomics, equal to rounding."""
+    import torch
+    nm, nts, Cmm, Ctm = case("elt16")
+    ctx.set_block(256)
+    outs = []
+    ctx.set_factor_format(fmt)
+    try:
+        for on in (False, True):
+            ctx.set_tc_pair(on)
+            dC, dT = dev(Cmm), dev(Ctm)
+            rep = M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=ctx)
+            ctx.synchronize()
+            outs.append((dC, dT, rep["refine_resid"]))
+    finally:
+        ctx.set_tc_pair(True)
+        ctx.set_factor_format("f16x2")
+    assert torch.equal(outs[0][1], outs[1][1])
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert abs(outs[0][2] - outs[1][2]) <= 1e-12 * outs[0][2]
+
+
 @pytest.mark.parametrize("n,m,nb", [(1000, 77, 256), (1370, 130, 512)])
 def test_mixed_default_format_ragged_panels(ctx, n, m, nb):
     """Default fp16x2 format on sizes that are not multiples of the panel width

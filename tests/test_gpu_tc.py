@@ -5,6 +5,10 @@
   fp32, in different orders).
 * int8 -> int32 -> scaled fp64 (Ozaki slices): compared with an exact int64
   product; tolerance 1e-15 relative (one fp64 rounding per added term).
+
+Every case runs on single CTAs (128 x 256 tiles) and on CTA pairs (256 x 256
+tiles, M = 256 MMAs; used where M > 128): sizes include a second B box wholly
+past N (N = 77) and A rows of the second CTA partly past M.
 """
 import ctypes as C
 
@@ -17,34 +21,41 @@ from moao_b200._lib import check, lib
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=[0, 1], ids=["cta", "pair"])
+def tcx(ctx, request):
+    ctx.set_tc_pair(request.param)
+    yield ctx
+    ctx.set_tc_pair(True)
+
+
 def _ints(xs):
     return (C.c_int * len(xs))(*xs)
 
 
-def tc_bf16(ctx, A, B, Cm, pairs, alpha=1.0, beta=0.0, lower=0):
+def tc_bf16(tcx, A, B, Cm, pairs, alpha=1.0, beta=0.0, lower=0):
     """A: [na, M, Kp] bf16, B: [nb, N, Kp] bf16 (row-major, Kp padded), Cm: [N, M] f32 (col-major C)."""
     na, Mr, Kp = A.shape
     nb, Nr, _ = B.shape
     pa, pb = _ints([p[0] for p in pairs]), _ints([p[1] for p in pairs])
-    check(lib().moao_debug_tc_gemm(ctx.handle, 0, Mr, Nr, Kp, A.data_ptr(), Kp, na, B.data_ptr(), Kp,
+    check(lib().moao_debug_tc_gemm(tcx.handle, 0, Mr, Nr, Kp, A.data_ptr(), Kp, na, B.data_ptr(), Kp,
                                    nb, len(pairs), pa, pb, Cm.data_ptr(), Mr, alpha, beta, None,
                                    None, 0, lower), "tc_gemm")
 
 
 @pytest.mark.parametrize("Mr,Nr,K", [(128, 128, 64), (256, 384, 512), (300, 200, 136), (1000, 77, 1000)])
-def test_bf16_single_product(ctx, Mr, Nr, K):
+def test_bf16_single_product(tcx, Mr, Nr, K):
     import torch
     g = torch.Generator(device="cuda").manual_seed(1)
     A = torch.randn(1, Mr, K, device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn(1, Nr, K, device="cuda", generator=g).to(torch.bfloat16)
     Cm = torch.randn(Nr, Mr, device="cuda", generator=g)
     want = (0.5 * (A[0].float() @ B[0].float().T) + 2.0 * Cm.T).T.contiguous()
-    tc_bf16(ctx, A, B, Cm, [(0, 0)], alpha=0.5, beta=2.0)
+    tc_bf16(tcx, A, B, Cm, [(0, 0)], alpha=0.5, beta=2.0)
     err = (Cm - want).abs().max() / want.abs().max()
     assert err < 1e-5, float(err)
 
 
-def test_bf16_split_products_and_lower(ctx):
+def test_bf16_split_products_and_lower(tcx):
     import torch
     g = torch.Generator(device="cuda").manual_seed(2)
     Mr = Nr = 384
@@ -54,7 +65,7 @@ def test_bf16_split_products_and_lower(ctx):
     lo = (X - hi.double()).to(torch.bfloat16)
     A = torch.stack([hi, lo])
     Cm = torch.zeros(Nr, Mr, device="cuda")
-    tc_bf16(ctx, A, A, Cm, [(0, 0), (0, 1), (1, 0)], alpha=1.0, beta=0.0, lower=1)
+    tc_bf16(tcx, A, A, Cm, [(0, 0), (0, 1), (1, 0)], alpha=1.0, beta=0.0, lower=1)
     h, l = hi.double(), lo.double()
     want = (h @ h.T + h @ l.T + l @ h.T)
     got = Cm.T.double()
@@ -69,7 +80,7 @@ def test_bf16_split_products_and_lower(ctx):
 
 @pytest.mark.parametrize("Mr,Nr,K,pairs", [(128, 128, 128, [(0, 0)]), (200, 330, 384, [(0, 1), (1, 0)]),
                                            (640, 256, 4096, [(0, 2), (1, 1), (2, 0)])])
-def test_int8_scaled_fp64(ctx, Mr, Nr, K, pairs):
+def test_int8_scaled_fp64(tcx, Mr, Nr, K, pairs):
     import torch
     rng = np.random.default_rng(3)
     na = max(p[0] for p in pairs) + 1
@@ -86,14 +97,14 @@ def test_int8_scaled_fp64(ctx, Mr, Nr, K, pairs):
     dC = torch.from_numpy(np.ascontiguousarray(C0.T)).cuda()
     der, dec = torch.from_numpy(er).cuda(), torch.from_numpy(ec).cuda()
     pa, pb = _ints([p[0] for p in pairs]), _ints([p[1] for p in pairs])
-    check(lib().moao_debug_tc_gemm(ctx.handle, 1, Mr, Nr, K, dA.data_ptr(), K, na, dB.data_ptr(), K, nb,
+    check(lib().moao_debug_tc_gemm(tcx.handle, 1, Mr, Nr, K, dA.data_ptr(), K, na, dB.data_ptr(), K, nb,
                                    len(pairs), pa, pb, dC.data_ptr(), Mr, 1.0, 0.0, der.data_ptr(),
                                    dec.data_ptr(), shift, 0), "tc_gemm int8")
     got = dC.cpu().numpy().T
     assert np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-300)) < 1e-15
 
 
-def test_f16_scaled_products(ctx):
+def test_f16_scaled_products(tcx):
     """fp16 operands stored scaled by 2^-e per row (two slices, 3 products): the
     epilogue's 2^(erow[r] + ecol[c]) restores the product of the unscaled values
     to ~2^-22 relative; rows span 2^-30..2^20 in magnitude."""
@@ -115,7 +126,7 @@ def test_f16_scaled_products(ctx):
     B, eb = slices(Y)
     Cm = torch.zeros(Nr, Mr, device="cuda")
     pairs = [(1, 0), (0, 1), (0, 0)]
-    check(lib().moao_debug_tc_gemm(ctx.handle, 2, Mr, Nr, K, A.data_ptr(), K, 2, B.data_ptr(), K, 2,
+    check(lib().moao_debug_tc_gemm(tcx.handle, 2, Mr, Nr, K, A.data_ptr(), K, 2, B.data_ptr(), K, 2,
                                    3, _ints([p[0] for p in pairs]), _ints([p[1] for p in pairs]),
                                    Cm.data_ptr(), Mr, -1.0, 0.0, ea.data_ptr(), eb.data_ptr(), 0, 0),
           "tc_gemm f16")
@@ -128,7 +139,7 @@ def test_f16_scaled_products(ctx):
 
 
 @pytest.mark.parametrize("kind,lower", [(0, 1), (2, 0), (2, 1)])
-def test_accumulate_epilogue_through_tma_reduce(ctx, kind, lower):
+def test_accumulate_epilogue_through_tma_reduce(tcx, kind, lower):
     """beta = 1 with a 16-byte aligned C and ldc % 4 == 0 takes the TMA reduce-add
     epilogue: C += alpha * products, entries above the diagonal (lower = 1) and
     outside M x N (M, N not multiples of 32) left untouched."""
@@ -144,7 +155,7 @@ def test_accumulate_epilogue_through_tma_reduce(ctx, kind, lower):
     ea = torch.full((Mr,), 1, dtype=torch.int32, device="cuda")
     eb = torch.full((Nr,), -2, dtype=torch.int32, device="cuda")
     exps = kind == 2
-    check(lib().moao_debug_tc_gemm(ctx.handle, kind, Mr, Nr, K, A.data_ptr(), K, 1, B.data_ptr(), K, 1,
+    check(lib().moao_debug_tc_gemm(tcx.handle, kind, Mr, Nr, K, A.data_ptr(), K, 1, B.data_ptr(), K, 1,
                                    1, _ints([0]), _ints([0]), Cfull.data_ptr(), ldc, -0.5, 1.0,
                                    ea.data_ptr() if exps else None, eb.data_ptr() if exps else None,
                                    0, lower), "tc_gemm reduce")
@@ -159,3 +170,20 @@ def test_accumulate_epilogue_through_tma_reduce(ctx, kind, lower):
     err = (Cfull - want).abs().max() / upd.abs().max()
     assert err < 1e-5, float(err)
     assert torch.equal(Cfull[:, Mr:], C0[:, Mr:]) and torch.equal(Cfull[Nr:], C0[Nr:])
+
+
+def test_more_tiles_than_resident_ctas(tcx):
+    """121 pair tiles (242 single-CTA tiles) on at most 74 pairs (148 CTAs):
+    every CTA walks several tiles, so both accumulator buffers are reused and
+    the epilogues hand them back across the pair."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(11)
+    Mr = Nr = 2600
+    K = 256
+    A = torch.randn(1, Mr, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(1, Nr, K, device="cuda", generator=g).to(torch.bfloat16)
+    Cm = torch.zeros(Nr, Mr, device="cuda")
+    tc_bf16(tcx, A, B, Cm, [(0, 0)], alpha=1.0, beta=0.0)
+    want = (A[0].float() @ B[0].float().T).T
+    err = (Cm - want).abs().max() / want.abs().max()
+    assert err < 1e-5, float(err)
