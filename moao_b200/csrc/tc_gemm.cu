@@ -3,8 +3,9 @@
 //   C[M x N] (+)= sum over segments s of  A_s[M x K_s] * B_s[N x K_s]^T
 //
 // Both operands are K-major (rows of K contiguous elements) and are fetched by
-// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a shared-memory
-// ring; one thread issues tcgen05.mma into a double-buffered TMEM accumulator;
+// TMA (cp.async.bulk.tensor, 128-byte swizzle, each CTA loading only its own
+// tiles) into a shared-memory ring; one thread issues tcgen05.mma into a
+// double-buffered TMEM accumulator;
 // eight epilogue warps drain TMEM with tcgen05.ld and update C. A tile is 128 x
 // 256 on one CTA, or 256 x 256 on a cluster of two CTAs (M = 256 MMAs,
 // cta_group::2). The K dimension is a list of segments, each naming its own A
@@ -170,7 +171,7 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // Load into this CTA's shared memory, the bytes counted on the barrier at
-// shared::cluster address bar (in either CTA of the pair). No multicast.
+// shared::cluster address bar (in either CTA of the pair).
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int x, int y,
                                                  uint32_t bar) {
   asm volatile(
