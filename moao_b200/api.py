@@ -194,8 +194,8 @@ class Context:
         check(lib().moao_ctx_set_gemm_tile(self._h, int(cfg)), "moao_ctx_set_gemm_tile")
 
     def set_tc_pair(self, on: bool = True):
-        """Tensor-core products of the mixed path on CTA pairs (256 x 256 tiles,
-        the default) or single CTAs (moao_ctx_set_tc_pair); same results."""
+        """Tensor-core products of the mixed path on CTA pairs (256 x 256 tiles)
+        or single CTAs (the default; moao_ctx_set_tc_pair); same results."""
         check(lib().moao_ctx_set_tc_pair(self._h, int(bool(on))), "moao_ctx_set_tc_pair")
 
     def set_lookahead_max(self, sms: int = 8):

@@ -87,7 +87,7 @@ struct moao_ctx {
   int lookahead_sms = 8;
   int lookahead_max = 8;  // SMs left to it in the last panels (moao_ctx_set_lookahead_max)
   int gemm_cfg = 1;       // tile configuration of the large FP64 products (GemmArgs::cfg)
-  int tc_pair = 1;        // tensor-core products on CTA pairs (TcGemm::pair)
+  int tc_pair = 0;        // tensor-core products on CTA pairs (TcGemm::pair)
   // Host-buffer cache of the drop-in path (moao_ctx_set_host_cache): the device
   // copy that moao_matcov_tile_host left of a whole Cmm (in ws_tmp) or Ctm (in
   // ws_host_t), keyed by the host buffer, its shape and the workspace's

@@ -48,6 +48,8 @@ constexpr int ACC_COLS = TBN;            // fp32 / int32 columns of one accumula
 constexpr int TMEM_COLS = 2 * ACC_COLS;  // double-buffered accumulator
 constexpr int STAGE_C = 32 * 32 * 4;     // per epilogue warp: one 32x32 FP32 chunk for TMA
 constexpr unsigned long long kSpinLimit = 1ull << 28;  // default polls of a bounded wait
+constexpr int kBandRows = 2048;          // rows of C per band of the tile order
+constexpr int kMaxBands = 64;
 
 // PAIR = 0: one CTA computes a 128 x 256 tile of C.
 // PAIR = 1: a cluster of two CTAs computes a 256 x 256 tile with M = 256 MMAs
@@ -91,6 +93,8 @@ struct __align__(64) TcParams {
   int tile_m;              // rows of C per tile (128, or 256 for CTA pairs)
   int tiles_m, tiles_n;
   int total_tiles;         // tiles that intersect the written part of C
+  int band;                // row tiles per band of the tile order
+  int band_start[kMaxBands + 1];  // tiles before each band
   int* err;
   unsigned long long spin_limit;  // polls of a role's bounded wait before it gives up
 };
@@ -274,22 +278,42 @@ __device__ __forceinline__ int first_mt(const TcParams& p, int nt) {
   return num <= 0 ? 0 : (num + p.tile_m - 1) / p.tile_m;
 }
 
-// v-th tile (in column-major tile order over the tiles that are written).
+// v-th tile of the walk over the tiles that are written. The row tiles are
+// taken in bands of p.band (about 2,048 rows); a band is walked column by
+// column and each column down the band's rows. A wave of the persistent grid
+// then covers a block of roughly 2,048 rows by 2,300 columns of C, whose A rows
+// and B rows stay in L2 while its tiles run (a column-major walk over all rows
+// streams every A row through L2 in every wave).
 __device__ __forceinline__ void decode_tile(const TcParams& p, int v, int* mt, int* nt) {
-  if (!p.lower) {
-    *mt = v % p.tiles_m;
-    *nt = v / p.tiles_m;
+  int b = 0;
+  while (b + 1 < kMaxBands && p.band_start[b + 1] <= v && b + 1 < (p.tiles_m + p.band - 1) / p.band)
+    ++b;
+  v -= p.band_start[b];
+  const int r0 = b * p.band, r1 = min(r0 + p.band, p.tiles_m), h = r1 - r0;
+  // columns whose first written row tile is at or above r0 hold all h tiles of the band
+  int full = p.tiles_n;
+  if (p.lower) {
+    const int num = r0 * p.tile_m + p.diag_off + p.tile_m - 1;
+    full = num < 0 ? 0 : min(p.tiles_n, num / TBN + 1);
+  }
+  if (v < full * h) {
+    *nt = v / h;
+    *mt = r0 + v % h;
     return;
   }
-  int c = 0;
-  for (;;) {
-    const int cnt = max(0, p.tiles_m - first_mt(p, c));
-    if (v < cnt || c == p.tiles_n - 1) break;
+  v -= full * h;
+  for (int c = full; c < p.tiles_n; ++c) {
+    const int f = max(r0, first_mt(p, c));
+    const int cnt = max(0, r1 - f);
+    if (v < cnt || c == p.tiles_n - 1) {
+      *nt = c;
+      *mt = f + v;
+      return;
+    }
     v -= cnt;
-    ++c;
   }
-  *nt = c;
-  *mt = first_mt(p, c) + v;
+  *nt = p.tiles_n - 1;
+  *mt = r0;
 }
 
 // Persistent warp-specialised kernel: warp 0 TMA producer, warp 1 MMA issuer,
@@ -694,15 +718,22 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   p.tile_m = pair ? TcCfg<1>::TILE_M : TcCfg<0>::TILE_M;
   p.tiles_m = (int)((g.M + p.tile_m - 1) / p.tile_m);
   p.tiles_n = (int)((g.N + TBN - 1) / TBN);
+  p.band = std::max(kBandRows / p.tile_m, (p.tiles_m + kMaxBands - 1) / kMaxBands);
+  const int nbands = (p.tiles_m + p.band - 1) / p.band;
   long total = 0;
-  for (int nt = 0; nt < p.tiles_n; ++nt) {
-    long first = 0;
-    if (g.lower) {
-      const long num = (long)nt * TBN - g.diag_off - (p.tile_m - 1);
-      first = num <= 0 ? 0 : (num + p.tile_m - 1) / p.tile_m;
+  for (int b = 0; b < nbands; ++b) {
+    p.band_start[b] = (int)total;
+    const long r0 = (long)b * p.band, r1 = std::min<long>(r0 + p.band, p.tiles_m);
+    for (int nt = 0; nt < p.tiles_n; ++nt) {
+      long first = 0;
+      if (g.lower) {
+        const long num = (long)nt * TBN - g.diag_off - (p.tile_m - 1);
+        first = num <= 0 ? 0 : (num + p.tile_m - 1) / p.tile_m;
+      }
+      total += std::max(0L, r1 - std::max(r0, first));
     }
-    total += std::max(0L, (long)p.tiles_m - first);
   }
+  for (int b = nbands; b <= kMaxBands; ++b) p.band_start[b] = (int)total;
   if (total == 0) return MOAO_OK;
   p.total_tiles = (int)total;
   // C += alpha * acc (beta 1) through TMA reductions when C's layout allows a

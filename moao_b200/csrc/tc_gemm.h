@@ -55,7 +55,7 @@ struct TcGemm {
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
   int max_ctas = 0;            // cap on the persistent grid (0: one CTA per SM)
   int pair = 0;                // 1: 256 x 256 tiles on clusters of two CTAs where M > 128
-                               // (the context's tc_pair, on by default)
+                               // (the context's tc_pair, off by default)
   unsigned long long spin_limit = 0;  // polls of each bounded wait (0: 2^28)
 };
 

@@ -190,7 +190,7 @@ def test_mixed_on_cta_pairs_gives_the_same_result(ctx, fmt):
             ctx.synchronize()
             outs.append((dC, dT, rep["refine_resid"]))
     finally:
-        ctx.set_tc_pair(True)
+        ctx.set_tc_pair(False)
         ctx.set_factor_format("f16x2")
     assert torch.equal(outs[0][1], outs[1][1])
     assert torch.equal(outs[0][0], outs[1][0])

@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 def tcx(ctx, request):
     ctx.set_tc_pair(request.param)
     yield ctx
-    ctx.set_tc_pair(True)
+    ctx.set_tc_pair(False)
 
 
 def _ints(xs):
@@ -172,18 +172,26 @@ def test_accumulate_epilogue_through_tma_reduce(tcx, kind, lower):
     assert torch.equal(Cfull[:, Mr:], C0[:, Mr:]) and torch.equal(Cfull[Nr:], C0[Nr:])
 
 
-def test_more_tiles_than_resident_ctas(tcx):
-    """121 pair tiles (242 single-CTA tiles) on at most 74 pairs (148 CTAs):
-    every CTA walks several tiles, so both accumulator buffers are reused and
-    the epilogues hand them back across the pair."""
+@pytest.mark.parametrize("Mr,Nr,lower", [(2600, 2600, 0), (5000, 900, 0), (4700, 4700, 1)])
+def test_more_tiles_than_resident_ctas(tcx, Mr, Nr, lower):
+    """More tiles than resident CTAs (pairs): every CTA walks several tiles, so
+    both accumulator buffers are reused and the epilogues hand them back across
+    the pair; M spans several bands of the tile walk (2,048 rows each), the
+    lower case with bands that end inside the triangle. Entries above the
+    diagonal stay untouched."""
     import torch
-    g = torch.Generator(device="cuda").manual_seed(11)
-    Mr = Nr = 2600
-    K = 256
+    g = torch.Generator(device="cuda").manual_seed(11 + Mr + lower)
+    K = 128
     A = torch.randn(1, Mr, K, device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn(1, Nr, K, device="cuda", generator=g).to(torch.bfloat16)
-    Cm = torch.zeros(Nr, Mr, device="cuda")
-    tc_bf16(tcx, A, B, Cm, [(0, 0)], alpha=1.0, beta=0.0)
+    Cm = torch.full((Nr, Mr), 7.0, device="cuda")
+    tc_bf16(tcx, A, B, Cm, [(0, 0)], alpha=1.0, beta=0.0, lower=lower)
     want = (A[0].float() @ B[0].float().T).T
+    if lower:
+        r = torch.arange(Mr, device="cuda")[None, :]
+        c = torch.arange(Nr, device="cuda")[:, None]
+        low = r >= c
+        assert bool((Cm[~low] == 7.0).all()), "wrote above the diagonal"
+        want = torch.where(low, want, Cm)
     err = (Cm - want).abs().max() / want.abs().max()
     assert err < 1e-5, float(err)
