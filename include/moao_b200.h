@@ -144,6 +144,17 @@ moao_status moao_ctx_set_gemm_tile(moao_ctx* ctx, int cfg);
  * products, summed in the same order per element. No reference counterpart. */
 moao_status moao_ctx_set_tc_pair(moao_ctx* ctx, int on);
 
+/* Refinement residual E = Ctm - R Cmm of the mixed reconstructor: scheme 1
+ * (the default) computes the product of the two operands rounded to the int8
+ * slice precision (moao_ctx_set_mixed, default 5 slices = 35 bits per operand)
+ * exactly, by the Chinese remainder theorem: residues modulo 11 pairwise
+ * coprime moduli <= 256 at nmeas 47,552 (one exact int8 tensor-core GEMM
+ * each) and mixed-radix reconstruction in 128-bit integers. Scheme 0 sums the
+ * int8 slice products whose slice indices add up to at most slices + 1 (15 at
+ * 5 slices). Scheme 1 falls back to 0 where its moduli would not cover the
+ * product (nmeas >= 131,072). No reference counterpart. */
+moao_status moao_ctx_set_residual(moao_ctx* ctx, int scheme);
+
 /* Accuracy target of the mixed reconstructor (relative Frobenius error of R;
  * 0, the default, turns the check off). With a target, the mixed path also
  * evaluates the residual after its last correction and estimates the error of

@@ -26,6 +26,16 @@ moao_status moao_debug_tc_gemm(moao_ctx* ctx, int kind, long M, long N, long K, 
                                const int* pa, const int* pb, void* C, long ldc, float alpha,
                                float beta, const int* erow, const int* ecol, int shift, int lower);
 
+/* The mixed path's refinement residual on its own (device pointers, context
+ * stream): E (m x n, ldE) = Ctm - R sym(Cmm), Cmm n x n read through its lower
+ * triangle, both operands rounded to the context's int8 slice precision
+ * (moao_ctx_set_mixed, default 5 slices = 35 bits). scheme 0: the int8 slice
+ * products (pairs of slice indices summing to at most slices + 1); scheme 1:
+ * exact products by the Chinese remainder theorem. Synchronises. */
+moao_status moao_debug_residual(moao_ctx* ctx, int scheme, long m, long n, const double* R,
+                                long ldR, const double* Cmm, long ldCmm, const double* Ctm,
+                                long ldCtm, double* E, long ldE);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,7 @@ SIGNATURES = {
     "moao_ctx_set_lookahead_max": (i32, [vp, i32]),
     "moao_ctx_set_gemm_tile": (i32, [vp, i32]),
     "moao_ctx_set_tc_pair": (i32, [vp, i32]),
+    "moao_ctx_set_residual": (i32, [vp, i32]),
     "moao_ctx_set_host_cache": (i32, [vp, i32]),
     "moao_dense_potrf_inv": (i32, [vp, i64, vp, i64, vp, i64, C.POINTER(i32)]),
     "moao_dense_gemm": (i32, [vp, i32, i32, i64, i64, i64, C.c_double, vp, i64, vp, i64,
@@ -162,6 +163,7 @@ SIGNATURES = {
     "moao_intersample_destroy": (None, [vp]),
     "moao_debug_tc_gemm": (i32, [vp, i32, i64, i64, i64, dp, i64, i32, dp, i64, i32, i32, dp, dp, dp,
                                  i64, C.c_float, C.c_float, dp, dp, i32, i32]),
+    "moao_debug_residual": (i32, [vp, i32, i64, i64, dp, i64, dp, i64, dp, i64, dp, i64]),
 }
 
 

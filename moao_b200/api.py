@@ -193,6 +193,13 @@ class Context:
         moao_ctx_set_gemm_tile); same results."""
         check(lib().moao_ctx_set_gemm_tile(self._h, int(cfg)), "moao_ctx_set_gemm_tile")
 
+    def set_residual_scheme(self, scheme: str = "crt"):
+        """Refinement residual of the mixed path: 'crt' (exact products of the
+        sliced operands by the Chinese remainder theorem, the default) or
+        'slices' (int8 slice products); moao_ctx_set_residual."""
+        code = {"slices": 0, "crt": 1}[scheme]
+        check(lib().moao_ctx_set_residual(self._h, code), "moao_ctx_set_residual")
+
     def set_tc_pair(self, on: bool = True):
         """Tensor-core products of the mixed path on CTA pairs (256 x 256 tiles)
         or single CTAs (the default; moao_ctx_set_tc_pair); same results."""

@@ -233,7 +233,7 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
       const Tomo_struct<double>& t = items[in.item].tomo->t;
       const int nro = t.sys.lgsCst > 0 ? 2 * t.sys.nLgs : 0;
       b += mixed_sizes(in.n, in.m, in.nb, std::max(2, std::min(kMaxBfSlices, proto->bf16_slices)),
-                       proto->ozaki_slices, nro).total();
+                       proto->ozaki_slices, nro, proto->residual_crt != 0).total();
     } else {
       b += sizeof(double) * (size_t)in.nb * ((size_t)in.n + std::max(in.n, in.m));
     }
@@ -352,7 +352,7 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
         const Tomo_struct<double>& t = items[in.item].tomo->t;
         const int nro = t.sys.lgsCst > 0 ? 2 * t.sys.nLgs : 0;
         const MixedSizes z = mixed_sizes(in.n, in.m, in.nb, std::max(2, std::min(kMaxBfSlices, sc->bf16_slices)),
-                                         sc->ozaki_slices, nro);
+                                         sc->ozaki_slices, nro, sc->residual_crt != 0);
         // size every workspace buffer for the largest instance of this stream
         MOAO_TRY(sc->mx_a32.ensure(z.a32));
         MOAO_TRY(sc->mx_lr.ensure(z.lr));
@@ -365,6 +365,9 @@ moao_status run_batch(moao_ctx* ctx, int count, moao_batch_item* items, moao_bat
         MOAO_TRY(sc->mx_e64.ensure(z.r64));
         MOAO_TRY(sc->mx_qa.ensure(z.qa));
         MOAO_TRY(sc->mx_qb.ensure(z.qb));
+        MOAO_TRY(sc->mx_qr.ensure(z.qr));
+        MOAO_TRY(sc->mx_qs.ensure(z.qs));
+        MOAO_TRY(sc->mx_z.ensure(z.z));
         MOAO_TRY(sc->mx_ea.ensure(z.ea));
         MOAO_TRY(sc->mx_fb.ensure(z.fb));
         MOAO_TRY(sc->mx_colmax.ensure(z.colmax));

@@ -571,6 +571,28 @@ moao_status moao_ctx_set_gemm_tile(moao_ctx* c, int cfg) {
   return MOAO_OK;
 }
 
+moao_status moao_ctx_set_residual(moao_ctx* c, int scheme) {
+  if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_residual: null");
+  if (scheme != 0 && scheme != 1)
+    return set_error(MOAO_ERR_BAD_ARG, "ctx_set_residual: 0 (slice products) or 1 (CRT)");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->residual_crt = scheme;
+  c->mx_factored_n = -1;  // a kept factorisation holds the other scheme's operands
+  c->rstate_valid = false;
+  return MOAO_OK;
+}
+
+moao_status moao_debug_residual(moao_ctx* c, int scheme, long m, long n, const double* R, long ldR,
+                                const double* Cmm, long ldCmm, const double* Ctm, long ldCtm,
+                                double* E, long ldE) {
+  if (!c || !R || !Cmm || !Ctm || !E || m <= 0 || n <= 0 || ldR < m || ldCmm < n || ldCtm < m ||
+      ldE < m || (scheme != 0 && scheme != 1))
+    return set_error(MOAO_ERR_BAD_ARG, "debug_residual: bad arguments");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MOAO_CUDA_TRY(cudaSetDevice(c->device));
+  return debug_residual(c, scheme, m, n, R, ldR, Cmm, ldCmm, Ctm, ldCtm, E, ldE);
+}
+
 moao_status moao_ctx_set_tc_pair(moao_ctx* c, int on) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_tc_pair: null");
   std::lock_guard<std::mutex> lk(c->mu);

@@ -60,6 +60,9 @@ struct moao_ctx {
   // mixed-precision workspace
   moao::DevBuf mx_a32, mx_lr, mx_lc, mx_t32, mx_w1, mx_w2, mx_x, mx_r64, mx_e64, mx_qa, mx_qb,
       mx_ea, mx_fb, mx_colmax, mx_norm;
+  // refinement residual by the Chinese remainder theorem: residues of R's rows
+  // and of sym(Cmm)'s columns, and of the product, one per modulus
+  moao::DevBuf mx_qr, mx_qs, mx_z;
   moao::DevBuf mx_rid, mx_y, mx_y2, mx_zu, mx_sinv, mx_exps, mx_dsl;
   // mixed Cee/Cvv chain: int8 slices of Ctm's rows (then of E's), their exponents
   moao::DevBuf cx_qc, cx_ec;
@@ -71,6 +74,7 @@ struct moao_ctx {
   int factor_format = 1;     // MOAO_FACTOR_F16X2 (default) or MOAO_FACTOR_BF16X3
   int corr_slices = 0;       // factor slices in the correction solves (0: 1 for fp16x2, 2 for bf16x3)
   int ozaki_slices = 5;      // int8 slices per operand of the refinement residual
+  int residual_crt = 1;      // refinement residual as exact CRT products (moao_ctx_set_residual)
   int max_refine = 1;        // refinement corrections per target
   double refine_tol = 0.0;   // stop refining once ||E||/||Ctm|| is at or below this
   int final_residual = 0;    // evaluate the residual once more after the last correction
@@ -183,13 +187,16 @@ moao_status potrf_inv_block(moao_ctx* ctx, double* A, long lda, double* D, long 
 // nsl bf16 slices, ns int8 slices and nranges declared offset ranges.
 struct MixedSizes {
   size_t a32 = 0, lr = 0, t32 = 0, w = 0, x = 0, r64 = 0, qa = 0, qb = 0, ea = 0, fb = 0,
-         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0, exps = 0, dsl = 0;
+         colmax = 0, norm = 0, dinv = 0, info = 0, offsets = 0, exps = 0, dsl = 0, qr = 0, qs = 0,
+         z = 0;
+  int nmod = 0;  // moduli of the CRT residual (0: int8 slice products)
   size_t total() const {
     return a32 + 2 * lr + t32 + 2 * w + x + 2 * r64 + qa + qb + ea + fb + colmax + norm +
-           2 * dinv + info + offsets + exps + dsl;
+           2 * dinv + info + offsets + exps + dsl + qr + qs + z;
   }
 };
-MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges);
+// crt: the refinement residual by CRT products where the moduli cover it
+MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges, bool crt);
 // Mixed-precision reconstructor for one target (see mixed.cpp); reuse = 1 keeps
 // the factorisation of the previous call.
 moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long ldCmm,
@@ -198,6 +205,11 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
 void release_batch_state(moao_ctx* ctx);
 // Writes the mixed factorisation's (FP32) factor into the lower triangle of Cmm.
 moao_status finish_mixed(moao_ctx* ctx, long n, double* Cmm, long ldCmm);
+// E = Ctm - R sym(Cmm) by the refinement residual alone (scheme 0: int8 slice
+// products, 1: CRT products); for tests.
+moao_status debug_residual(moao_ctx* ctx, int scheme, long m, long n, const double* R, long ldR,
+                           const double* Cmm, long ldCmm, const double* Ctm, long ldCtm,
+                           double* E, long ldE);
 // The host-buffer path's overlap hooks: the stream waits for inputs that arrive on
 // the copy stream, and the finished lower factor in Cmm (ld n) goes back to the
 // host on the copy stream while the solves run.

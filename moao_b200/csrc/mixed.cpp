@@ -341,17 +341,51 @@ moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTenso
   return MOAO_OK;
 }
 
-MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges) {
+// Residues of the product A B^T (M x N over K) modulo the first nmod moduli:
+// one int8 GEMM per modulus on the operands' residues (exact int32 sums, K <
+// 2^17), reduced in the epilogue into Z + i*M*N (uint8, column-major, ld M).
+moao_status crt_gemm(moao_ctx* ctx, const TcTensor* ta, const TcTensor* tb, int nmod, long M,
+                     long N, long K, uint8_t* Z, int* err) {
+  if (nmod < 2 || nmod > kCrtMaxModuli || K >= (1L << 17))
+    return set_error(MOAO_ERR_BAD_ARG, "crt_gemm: moduli or K");
+  for (int i = 0; i < nmod; ++i) {
+    TcGemm g;
+    g.spin_limit = ctx->wait_polls;
+    g.pair = ctx->tc_pair;
+    g.kind = kTcI8;
+    g.epi = kTcEpiMod8;
+    g.modulus = kCrtMod[i];
+    g.M = M;
+    g.N = N;
+    g.A[0] = &ta[i];
+    g.B[0] = &tb[i];
+    g.nA = g.nB = 1;
+    g.seg[0] = TcSegment{0, 0, 0, 0, (int)((K + 127) / 128), 0};
+    g.nseg = 1;
+    g.C = Z + (size_t)i * M * N;
+    g.ldc = M;
+    g.err = err;
+    KernelTimer kt(ctx, "tc_int8", 2.0 * M * (double)N * K);
+    MOAO_TRY(tc_gemm(g, ctx->stream, &ctx->launches));
+  }
+  return MOAO_OK;
+}
+
+MixedSizes mixed_sizes(long n, long m, long nb, int nsl, int ns, int nranges, bool crt) {
   const long ldn = round_up(n, 64), ldq = round_up(n, 128);
   MixedSizes z;
+  z.nmod = crt ? crt_moduli_for(ns, n) : 0;
   z.a32 = sizeof(float) * (size_t)n * n;
   z.lr = nsl * sizeof(uint16_t) * (size_t)n * ldn;
   z.t32 = sizeof(float) * (size_t)m * n;
   z.w = sizeof(double) * (size_t)std::max(n, m) * nb;
   z.x = nsl * sizeof(uint16_t) * (size_t)std::max(n, m) * nb;
   z.r64 = sizeof(double) * (size_t)m * n;
-  z.qa = (size_t)ns * m * ldq;
-  z.qb = (size_t)ns * n * ldq;
+  z.qa = (size_t)ns * m * ldq;  // the slices of R_k stay for a Cee from the refinement
+  z.qb = z.nmod ? 0 : (size_t)ns * n * ldq;
+  z.qr = (size_t)z.nmod * m * ldq;
+  z.qs = (size_t)z.nmod * n * ldq;
+  z.z = (size_t)z.nmod * m * n;
   z.ea = sizeof(int) * (size_t)m;
   z.fb = sizeof(int) * (size_t)n;
   z.colmax = sizeof(unsigned long long) * (size_t)n;
@@ -389,7 +423,8 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   const bool f16 = ctx->factor_format == MOAO_FACTOR_F16X2;
   const int tck = f16 ? kTcF16 : kTcBf16;
   const int nsl = f16 ? 2 : std::max(2, std::min(kMaxBfSlices, ctx->bf16_slices));
-  const MixedSizes z = mixed_sizes(n, m, nb, nsl, ns, ctx->offsets.n);
+  const MixedSizes z = mixed_sizes(n, m, nb, nsl, ns, ctx->offsets.n, ctx->residual_crt != 0);
+  const int nmod = z.nmod;  // > 0: the residual by CRT products
   MOAO_TRY(ctx->mx_a32.ensure(z.a32));
   MOAO_TRY(ctx->mx_lr.ensure(z.lr));
   MOAO_TRY(ctx->mx_lc.ensure(z.lr));
@@ -401,6 +436,9 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   MOAO_TRY(ctx->mx_e64.ensure(z.r64));
   MOAO_TRY(ctx->mx_qa.ensure(z.qa));
   MOAO_TRY(ctx->mx_qb.ensure(z.qb));
+  MOAO_TRY(ctx->mx_qr.ensure(z.qr));
+  MOAO_TRY(ctx->mx_qs.ensure(z.qs));
+  MOAO_TRY(ctx->mx_z.ensure(z.z));
   MOAO_TRY(ctx->mx_ea.ensure(z.ea));
   MOAO_TRY(ctx->mx_fb.ensure(z.fb));
   MOAO_TRY(ctx->mx_colmax.ensure(z.colmax));
@@ -435,6 +473,9 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   double* E64 = ctx->mx_e64.as<double>();
   int8_t* qa = ctx->mx_qa.as<int8_t>();
   int8_t* qb = ctx->mx_qb.as<int8_t>();
+  int8_t* qr = ctx->mx_qr.as<int8_t>();
+  int8_t* qs = ctx->mx_qs.as<int8_t>();
+  uint8_t* Zr = ctx->mx_z.as<uint8_t>();
   int* ea = ctx->mx_ea.as<int>();
   int* fb = ctx->mx_fb.as<int>();
   double* dinv = ctx->ws_dinv.as<double>();
@@ -600,9 +641,13 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
                                                std::to_string(info[0]));
       }
     }
-    // int8 slices of sym(Cmm) for the refinement residual
-    MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
-                             ldq, rid, off, s));
+    // int8 slices (or CRT residues) of sym(Cmm) for the refinement residual
+    if (nmod)
+      MOAO_TRY(crt_split_sym(Cmm, ldCmm, n, ns, nmod, fb, ctx->mx_colmax.as<unsigned long long>(),
+                             qs, ldq, rid, off, s));
+    else
+      MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, ctx->mx_colmax.as<unsigned long long>(), qb,
+                               ldq, rid, off, s));
     if (nro > 0) {
       // Y = U^T M_B^-1 (one 128-row solve), S = D^-1 + Y U, Y2 = S^-1 Y
       MOAO_TRY(fill_range_indicators(Y32, kYRows, n, off, s));
@@ -635,10 +680,17 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   }
   if (!graph) cudaEventRecord(ev[5], s);
   // ---- refinement
-  TcTensor ta[kMaxOzakiSlices], tb[kMaxOzakiSlices];
-  for (int i = 0; i < ns; ++i) {
-    MOAO_TRY(make_tc_map(&ta[i], qa + (size_t)i * m * ldq, kTcI8, m, n, ldq));
-    MOAO_TRY(make_tc_map(&tb[i], qb + (size_t)i * n * ldq, kTcI8, n, n, ldq, 256));
+  TcTensor ta[kCrtMaxModuli], tb[kCrtMaxModuli];
+  if (nmod) {
+    for (int i = 0; i < nmod; ++i) {
+      MOAO_TRY(make_tc_map(&ta[i], qr + (size_t)i * m * ldq, kTcI8, m, n, ldq));
+      MOAO_TRY(make_tc_map(&tb[i], qs + (size_t)i * n * ldq, kTcI8, n, n, ldq, 256));
+    }
+  } else {
+    for (int i = 0; i < ns; ++i) {
+      MOAO_TRY(make_tc_map(&ta[i], qa + (size_t)i * m * ldq, kTcI8, m, n, ldq));
+      MOAO_TRY(make_tc_map(&tb[i], qb + (size_t)i * n * ldq, kTcI8, n, n, ldq, 256));
+    }
   }
   double* dnorm = ctx->mx_norm.as<double>();
   double ctm2 = 0, e2 = 0;
@@ -647,11 +699,19 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   bool ran_residual = false;
   auto residual = [&]() -> moao_status {
     ran_residual = true;
-    // E = Ctm - R sym(Cmm) from the int8 slice products
-    MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
-                                    m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+    // E = Ctm - R sym(Cmm): exact CRT products of the ns-slice operands, or
+    // the int8 slice products (the slices of R_k are kept either way for a
+    // Cee from this refinement)
     MOAO_TRY(ozaki_split_rows(R64, m, m, n, ns, ea, qa, ldq, s));
-    MOAO_TRY(ozaki_gemm(ctx, ta, ns, tb, ns, ns + 1, m, n, n, -1.f, E64, m, ea, fb, err));
+    if (nmod) {
+      MOAO_TRY(crt_split_rows(R64, m, m, n, ns, nmod, ea, qr, ldq, s));
+      MOAO_TRY(crt_gemm(ctx, ta, tb, nmod, m, n, n, Zr, err));
+      MOAO_TRY(crt_combine(Zr, m, n, nmod, ns, ea, fb, Ctm, ldCtm, -1.0, E64, m, s));
+    } else {
+      MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, m * sizeof(double), Ctm, ldCtm * sizeof(double),
+                                      m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+      MOAO_TRY(ozaki_gemm(ctx, ta, ns, tb, ns, ns + 1, m, n, n, -1.f, E64, m, ea, fb, err));
+    }
     if (nro > 0) {  // the offsets' part of R Cmm
       MOAO_TRY(range_sums(R64, m, m, off, ZU, s));
       MOAO_TRY(subtract_offset_products(E64, m, m, n, ZU, rid, off, s));
@@ -739,6 +799,63 @@ moao_status reconstructor_mixed(moao_ctx* ctx, long n, long m, double* Cmm, long
   rep->ms_solve += ms;
   cudaEventElapsedTime(&ms, ev[5], ev[6]);
   rep->ms_refine += ms;
+  return MOAO_OK;
+}
+
+// E = Ctm - R sym(Cmm) by the refinement's residual alone (test entry point).
+moao_status debug_residual(moao_ctx* ctx, int scheme, long m, long n, const double* R, long ldR,
+                           const double* Cmm, long ldCmm, const double* Ctm, long ldCtm,
+                           double* E, long ldE) {
+  HelperCount hc(ctx);
+  cudaStream_t s = ctx->stream;
+  const int ns = ctx->ozaki_slices;
+  const long ldq = round_up(n, 128);
+  const int nmod = scheme == 1 ? crt_moduli_for(ns, n) : 0;
+  if (scheme == 1 && !nmod) return set_error(MOAO_ERR_BAD_ARG, "debug_residual: no moduli cover n");
+  const int nq = nmod ? nmod : ns;
+  DevBuf qa, qb, z, ex, cm, info;
+  struct Release {
+    DevBuf* b[6];
+    ~Release() {
+      for (DevBuf* x : b) x->release();
+    }
+  } release_all{{&qa, &qb, &z, &ex, &cm, &info}};
+  MOAO_TRY(qa.ensure((size_t)nq * m * ldq));
+  MOAO_TRY(qb.ensure((size_t)nq * n * ldq));
+  MOAO_TRY(ex.ensure(sizeof(int) * (size_t)(m + n)));
+  MOAO_TRY(cm.ensure(sizeof(unsigned long long) * (size_t)n));
+  MOAO_TRY(info.ensure(sizeof(int)));
+  int* ea = ex.as<int>();
+  int* fb = ea + m;
+  int* err = info.as<int>();
+  MOAO_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+  OffsetRanges none{};
+  TcTensor ta[kCrtMaxModuli], tb[kCrtMaxModuli];
+  for (int i = 0; i < nq; ++i) {
+    MOAO_TRY(make_tc_map(&ta[i], qa.as<int8_t>() + (size_t)i * m * ldq, kTcI8, m, n, ldq));
+    MOAO_TRY(make_tc_map(&tb[i], qb.as<int8_t>() + (size_t)i * n * ldq, kTcI8, n, n, ldq, 256));
+  }
+  if (nmod) {
+    MOAO_TRY(z.ensure((size_t)nmod * m * n));
+    MOAO_TRY(crt_split_sym(Cmm, ldCmm, n, ns, nmod, fb, cm.as<unsigned long long>(),
+                           qb.as<int8_t>(), ldq, nullptr, none, s));
+    // row exponents as the slices use them, then the residues
+    MOAO_TRY(ozaki_split_rows(R, ldR, m, n, 1, ea, qa.as<int8_t>(), ldq, s));
+    MOAO_TRY(crt_split_rows(R, ldR, m, n, ns, nmod, ea, qa.as<int8_t>(), ldq, s));
+    MOAO_TRY(crt_gemm(ctx, ta, tb, nmod, m, n, n, z.as<uint8_t>(), err));
+    MOAO_TRY(crt_combine(z.as<uint8_t>(), m, n, nmod, ns, ea, fb, Ctm, ldCtm, -1.0, E, ldE, s));
+  } else {
+    MOAO_TRY(ozaki_split_sym(Cmm, ldCmm, n, ns, fb, cm.as<unsigned long long>(),
+                             qb.as<int8_t>(), ldq, nullptr, none, s));
+    MOAO_TRY(ozaki_split_rows(R, ldR, m, n, ns, ea, qa.as<int8_t>(), ldq, s));
+    MOAO_CUDA_TRY(cudaMemcpy2DAsync(E, ldE * sizeof(double), Ctm, ldCtm * sizeof(double),
+                                    m * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+    MOAO_TRY(ozaki_gemm(ctx, ta, ns, tb, ns, ns + 1, m, n, n, -1.f, E, ldE, ea, fb, err));
+  }
+  int herr = 0;
+  MOAO_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MOAO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) return set_error(MOAO_ERR_TIMEOUT, "debug_residual: bounded wait expired");
   return MOAO_OK;
 }
 

@@ -12,6 +12,20 @@ namespace moao {
 
 constexpr int kMaxOzakiSlices = 6;
 
+// Exact products by the Chinese remainder theorem. An operand of ns-slice
+// precision is the integer X = rint(x 2^(7 ns - 1 - e)) of its row (column)
+// exponent e, |X| <= 2^(7 ns - 1); its residues modulo pairwise coprime
+// m_i <= 256 are int8 values, one exact int8 GEMM per modulus gives the
+// product's residues, and mixed-radix (Garner) reconstruction the product
+// itself, exact while |product| < M / 2 (M = the moduli's product).
+constexpr int kCrtMaxModuli = 13;
+constexpr int kCrtMod[kCrtMaxModuli] = {256, 255, 253, 251, 247, 241, 239,
+                                        233, 229, 227, 223, 217, 211};
+// Moduli needed for a product over K terms of two ns-slice operands: the
+// fewest leading kCrtMod whose product exceeds 2 K 2^(2 (7 ns - 1)); 0 when
+// none suffice or K breaks the int32 accumulation (K * 2^14 >= 2^31).
+int crt_moduli_for(int ns, long K);
+
 // Kernels launched so far on this thread by the helpers declared here.
 long long helper_launches();
 constexpr int kMaxBfSlices = 3;
@@ -67,6 +81,23 @@ moao_status split_rows_f16(const float* src, long lds, long m, long kb, int ns, 
 // slice s at out + s*m*ldo, row-major with row stride ldo.
 moao_status ozaki_split_rows(const double* A, long lda, long m, long n, int ns, int* e,
                              int8_t* out, long ldo, cudaStream_t st);
+// Residues (nmod of them, int8, centred) of the rows of A at ns-slice
+// precision, with the row exponents e[m] already computed (ozaki_split_rows
+// computes the same exponents): residue i at out + i*m*ldo, row-major.
+moao_status crt_split_rows(const double* A, long lda, long m, long n, int ns, int nmod,
+                           const int* e, int8_t* out, long ldo, cudaStream_t st);
+// Residues of the columns of sym(A) - offsets (lower-stored n x n A) at
+// ns-slice precision; computes the column exponents f[n]; residue i at
+// out + i*n*ldo with row j holding column j.
+moao_status crt_split_sym(const double* A, long lda, long n, int ns, int nmod, int* f,
+                          unsigned long long* colmax, int8_t* out, long ldo, const int* rid,
+                          const OffsetRanges& off, cudaStream_t st);
+// E (m x n, lde) = C (ldc) + alpha * P 2^(e[r] + f[c] - 2 (7 ns - 1)), P the
+// product whose residues modulo kCrtMod[i] are Z + i*m*n (uint8 in [0, m_i),
+// column-major, ld m).
+moao_status crt_combine(const uint8_t* Z, long m, long n, int nmod, int ns, const int* e,
+                        const int* f, const double* C, long ldc, double alpha, double* E,
+                        long lde, cudaStream_t st);
 // int8 slices of the columns of sym(A) - offsets for a lower-stored n x n A
 // (rid: range of every index or -1, null for no offsets): per-column exponents
 // in f[n]; slice s at out + s*n*ldo with row j holding column j.

@@ -402,6 +402,258 @@ __global__ void split_sym_i8_kernel(const double* __restrict__ A, long lda, long
   }
 }
 
+// ---- exact products by the Chinese remainder theorem
+
+constexpr int crt_modinv(int a, int m) {  // a^-1 mod m (gcd(a, m) = 1), extended Euclid
+  int t = 0, nt = 1, r = m, nr = a % m;
+  while (nr != 0) {
+    const int q = r / nr;
+    const int t2 = t - q * nt;
+    t = nt;
+    nt = t2;
+    const int r2 = r - q * nr;
+    r = nr;
+    nr = r2;
+  }
+  return t < 0 ? t + m : t;
+}
+
+// kCrtMod[i] as a constant expression usable in device code
+constexpr int crt_mod(int i) {
+  constexpr int tab[kCrtMaxModuli] = {256, 255, 253, 251, 247, 241, 239,
+                                      233, 229, 227, 223, 217, 211};
+  return tab[i];
+}
+
+constexpr bool crt_table_matches() {
+  for (int i = 0; i < kCrtMaxModuli; ++i)
+    if (crt_mod(i) != kCrtMod[i]) return false;
+  return true;
+}
+static_assert(crt_table_matches(), "device and host moduli tables");
+static_assert(crt_mod(0) == 256, "the first modulus is taken from the low byte");
+
+// Rounding to the nearest integer by the FP64 magic constant 1.5 * 2^52: for
+// |y| < 2^51, y + kMagic64 holds round(y) in its low mantissa bits, and
+// subtracting kMagic64 again gives it as a double (exact); the low 32 bits of
+// the sum are round(y) in two's complement.
+constexpr double kMagic64 = 6755399441055744.0;
+constexpr float kMagic32 = 12582912.0f;  // 1.5 * 2^23, for |y| < 2^22 in FP32
+
+// Centred residue of the integer x (|x| <= 2^41, exact in FP64) modulo the
+// I-th modulus and those after it, for I < nmod: r = x - M round(x / M). The
+// quotient's error, |x / M| 2^-52 <= 2^-19, is far below the distance of x / M
+// from a half-integer for odd M (at least 1 / 2M), so the rounding picks the
+// nearest integer, r is exact and lies in [-(M - 1) / 2, (M - 1) / 2].
+template <int I>
+__device__ __forceinline__ void crt_residue_from(double x, int nmod, int8_t* r) {
+  if constexpr (I < kCrtMaxModuli) {
+    if (I < nmod) {
+      constexpr int M = crt_mod(I);
+      constexpr double INV = 1.0 / M;
+      const double q = fma(x, INV, kMagic64) - kMagic64;
+      const double t = fma(-(double)M, q, x);
+      r[I] = (int8_t)__double2loint(t + kMagic64);
+    }
+    crt_residue_from<I + 1>(x, nmod, r);
+  }
+}
+
+// Centred residues of the integer x (|x| <= 2^41) modulo the first nmod moduli:
+// m_0 = 256 from the low byte of its two's complement.
+__device__ __forceinline__ void crt_residues(double x, int nmod, int8_t* r) {
+  r[0] = (int8_t)(__double2loint(x + kMagic64) & 0xFF);
+  crt_residue_from<1>(x, nmod, r);
+}
+
+// Garner's step for modulus I: t <- (((t - v_0) m_0^-1 - v_1) m_1^-1 - ...) mod m_I,
+// centred, in FP32: every operand is an integer below 2^17 in magnitude (exact),
+// and y / M (error <= 2^-14) is at least 1 / 2M from a half-integer.
+template <int I, int J>
+__device__ __forceinline__ float crt_garner_inner(float t, const float* v) {
+  if constexpr (J < I) {
+    constexpr int M = crt_mod(I);
+    constexpr float INV = 1.0f / M;
+    constexpr float MINV = (float)crt_modinv(crt_mod(J) % M, M);
+    const float y = (t - v[J]) * MINV;
+    t = fmaf(-(float)M, fmaf(y, INV, kMagic32) - kMagic32, y);
+    return crt_garner_inner<I, J + 1>(t, v);
+  } else {
+    return t;
+  }
+}
+
+// Centred mixed-radix digits v_I.. of the value whose residues are z_i
+template <int I>
+__device__ __forceinline__ void crt_digits_from(const uint8_t* __restrict__ Z, long idx,
+                                                long zstride, int nmod, float* v) {
+  if constexpr (I < kCrtMaxModuli) {
+    if (I < nmod) {
+      v[I] = crt_garner_inner<I, 0>((float)Z[I * zstride + idx], v);  // I >= 1 steps: centred
+    }
+    crt_digits_from<I + 1>(Z, idx, zstride, nmod, v);
+  }
+}
+
+// Horner over the digits I..min(nmod, END)-1 in 64-bit integers:
+// v_I + m_I (v_(I+1) + m_(I+1) (...)).
+template <int I, int END>
+__device__ __forceinline__ long long crt_horner64(const float* v, int nmod) {
+  if constexpr (I < END) {
+    if (I >= nmod) return 0;
+    return (long long)(int)v[I] + (long long)crt_mod(I) * crt_horner64<I + 1, END>(v, nmod);
+  } else {
+    return 0;
+  }
+}
+
+// The value of the digits as a double: P = L + W_7 H with L the first seven
+// digits' part (|L| < 2^55) and H the rest's (|H| < 2^47), both exact in int64;
+// W_7 = m_0 ... m_6 = 2^8 times a 48-bit odd number is exact in FP64, so P
+// comes out within two roundings.
+constexpr int kCrtSplit = 7;
+constexpr double crt_w7() {
+  double w = 1.0;
+  for (int i = 0; i < kCrtSplit; ++i) w *= crt_mod(i);
+  return w;
+}
+__device__ __forceinline__ double crt_digits_value(const float* v, int nmod) {
+  const long long L = crt_horner64<0, kCrtSplit>(v, nmod);
+  if (nmod <= kCrtSplit) return (double)L;
+  const long long H = crt_horner64<kCrtSplit, kCrtMaxModuli>(v, nmod);
+  return fma((double)H, crt_w7(), (double)L);
+}
+
+// Residues of the rows of a column-major m x n block into row-major int8 (ldo),
+// X = rint(A(r, c) 2^(sh - e[r])), sh = 7 ns - 1.
+__global__ void crt_rows_kernel(const double* __restrict__ A, long lda, long m, long n,
+                                const int* __restrict__ e, int sh, int nmod, int8_t* out,
+                                long ldo, long stride) {
+  __shared__ int8_t q[kCrtMaxModuli][32][36];
+  const long r0 = (long)blockIdx.x * 32, c0 = (long)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const long r = r0 + tx, c = c0 + jj;
+    double v = 0;
+    if (r < m && c < n) v = ldexp(A[c * lda + r], sh - e[r]);
+    int8_t res[kCrtMaxModuli] = {};
+    crt_residues((v + kMagic64) - kMagic64, nmod, res);
+#pragma unroll
+    for (int i = 0; i < kCrtMaxModuli; ++i)
+      if (i < nmod) q[i][tx][jj] = res[i];
+  }
+  __syncthreads();
+  for (int ii = ty; ii < 32; ii += 8) {
+    const long r = r0 + ii, c = c0 + tx;
+    if (r < m && c < n)
+      for (int i = 0; i < nmod; ++i) out[i * stride + r * ldo + c] = q[i][ii][tx];
+  }
+}
+
+// Residues of sym(A) by columns, written as B[j * ldo + k] = residue(S(k, j))
+// (the K-major B operand), S(k, j) = A(max(k,j), min(k,j)) minus offsets,
+// whose exponent is f[j]. B is not symmetric (the scale is per column), but
+// B[j][k] and B[k][j] scale the same stored element: a block of 32 x 32 tiles
+// at or below the diagonal (kb >= jb) loads its stored elements once, and its
+// residues for both orientations are written, the mirrored ones staged through
+// shared memory so that both sets of stores are 32-bit and coalesced.
+__global__ void crt_sym_kernel(const double* __restrict__ A, long lda, long n,
+                               const int* __restrict__ f, int sh, int nmod, int8_t* out,
+                               long ldo, long stride, const int* rid, const OffsetValues ov) {
+  __shared__ double t[32][33];                       // t[jj][kk] = S(k0+kk, j0+jj)
+  __shared__ int8_t rs[kCrtMaxModuli][32][36];       // rs[i][kk][jj]: residue of S(j, k) at f[k]
+  // tile (jb, kb) with kb >= jb from the linear index (kb rows of the lower triangle)
+  const long tix = blockIdx.x;
+  long kb = (long)((sqrt(8.0 * (double)tix + 1.0) - 1.0) * 0.5);
+  while ((kb + 1) * (kb + 2) / 2 <= tix) ++kb;
+  while (kb * (kb + 1) / 2 > tix) --kb;
+  const long jb = tix - kb * (kb + 1) / 2;
+  const long j0 = jb * 32, k0 = kb * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (k0 > j0) {
+    // k > j everywhere: S(k, j) = A(k, j), contiguous in k
+    for (int jj = ty; jj < 32; jj += 8) {
+      const long k = k0 + tx, j = j0 + jj;
+      t[jj][tx] = (k < n && j < n) ? stored_minus(A, lda, k, j, rid, ov) : 0.0;
+    }
+  } else {
+    for (int jj = ty; jj < 32; jj += 8) {
+      const long k = k0 + tx, j = j0 + jj;
+      double v = 0;
+      if (k < n && j < n)
+        v = (k >= j) ? stored_minus(A, lda, k, j, rid, ov) : stored_minus(A, lda, j, k, rid, ov);
+      t[jj][tx] = v;
+    }
+  }
+  __syncthreads();
+  // direct orientation: row j, 4 consecutive k per thread, one 32-bit store per residue
+  const int tid = ty * 32 + tx;
+  const int jj = tid >> 3, kq = (tid & 7) * 4;
+  const long j = j0 + jj, k = k0 + kq;
+  const bool mirror = k0 > j0;
+  if (j < n && k < n) {
+    const double sc = pow2i(sh - f[j]);
+    uint32_t w[kCrtMaxModuli];
+#pragma unroll
+    for (int i = 0; i < kCrtMaxModuli; ++i) w[i] = 0;
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4) {
+      const double v = (k + q4 < n) ? t[jj][kq + q4] * sc : 0.0;
+      int8_t res[kCrtMaxModuli] = {};
+      crt_residues((v + kMagic64) - kMagic64, nmod, res);
+#pragma unroll
+      for (int i = 0; i < kCrtMaxModuli; ++i) w[i] |= (uint32_t)(uint8_t)res[i] << (8 * q4);
+    }
+#pragma unroll
+    for (int i = 0; i < kCrtMaxModuli; ++i)
+      if (i < nmod) *reinterpret_cast<uint32_t*>(out + i * stride + j * ldo + k) = w[i];
+  }
+  if (!mirror) return;  // a diagonal tile's mirror is itself
+  // mirrored orientation: row k (column k of S, exponent f[k]), entries j: the
+  // thread computes S(k0+kk, j0+jq..jq+3) at f[k0+kk] and stages them
+  {
+    const int kk = tid >> 3, jq = (tid & 7) * 4;
+    const long kr = k0 + kk;
+    if (kr < n) {
+      const double sc = pow2i(sh - f[kr]);
+#pragma unroll
+      for (int q4 = 0; q4 < 4; ++q4) {
+        const double v = (j0 + jq + q4 < n) ? t[jq + q4][kk] * sc : 0.0;
+        int8_t res[kCrtMaxModuli] = {};
+        crt_residues((v + kMagic64) - kMagic64, nmod, res);
+#pragma unroll
+        for (int i = 0; i < kCrtMaxModuli; ++i)
+          if (i < nmod) rs[i][kk][jq + q4] = res[i];
+      }
+      // the thread's own 4 bytes per residue are contiguous: store them as one word
+#pragma unroll
+      for (int i = 0; i < kCrtMaxModuli; ++i)
+        if (i < nmod && j0 + jq < n)
+          *reinterpret_cast<uint32_t*>(out + i * stride + kr * ldo + j0 + jq) =
+              *reinterpret_cast<const uint32_t*>(&rs[i][kk][jq]);
+    }
+  }
+}
+
+// E = C + alpha * P 2^(e[r] + f[c] - 2 sh) from P's residues: centred mixed-
+// radix digits by Garner's method, then P from them (crt_digits_value). One
+// element per thread: blockIdx.x is the column, blockIdx.y the block of rows.
+__global__ void crt_combine_kernel(const uint8_t* __restrict__ Z, long m, long zstride, int nmod,
+                                   int sh, const int* __restrict__ e, const int* __restrict__ f,
+                                   const double* __restrict__ C, long ldc, double alpha,
+                                   double* __restrict__ E, long lde) {
+  const long r = (long)blockIdx.y * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const long c = blockIdx.x;
+  const long idx = c * m + r;
+  float v[kCrtMaxModuli];
+  const int z0 = Z[idx];
+  v[0] = (float)(z0 >= 128 ? z0 - 256 : z0);
+  crt_digits_from<1>(Z, idx, zstride, nmod, v);
+  const double val = crt_digits_value(v, nmod);
+  E[c * lde + r] = C[c * ldc + r] + alpha * (val * pow2i(e[r] + f[c] - 2 * sh));
+}
+
 // ---- offsets by the Woodbury identity
 
 __global__ void cvt_lower_minus_kernel(const double* __restrict__ s, long lds,
@@ -789,6 +1041,68 @@ moao_status ozaki_split_sym(const double* A, long lda, long n, int ns, int* f,
   exponents_from_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(colmax, n, f);
   ++tl_launches;
   split_sym_i8_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, f, ns, out, ldo, n * ldo, r, ov);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+
+int crt_moduli_for(int ns, long K) {
+  if (ns < 1 || ns > kMaxOzakiSlices || K < 1 || K >= (1L << 17)) return 0;
+  // |product| <= K 2^(2 (7 ns - 1)); exact while it stays below M / 2
+  const double need = std::log2((double)K) + 2.0 * (7 * ns - 1) + 1.0;
+  double have = 0;
+  for (int i = 0; i < kCrtMaxModuli; ++i) {
+    have += std::log2((double)kCrtMod[i]);
+    if (have > need + 1e-9) return i + 1;
+  }
+  return 0;
+}
+
+moao_status crt_split_rows(const double* A, long lda, long m, long n, int ns, int nmod,
+                           const int* e, int8_t* out, long ldo, cudaStream_t st) {
+  if (ns < 1 || ns > kMaxOzakiSlices || nmod < 2 || nmod > kCrtMaxModuli)
+    return set_error(MOAO_ERR_BAD_ARG, "crt: slices or moduli");
+  dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+  crt_rows_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, m, n, e, 7 * ns - 1, nmod, out, ldo,
+                                                 m * ldo);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status crt_split_sym(const double* A, long lda, long n, int ns, int nmod, int* f,
+                          unsigned long long* colmax, int8_t* out, long ldo, const int* rid,
+                          const OffsetRanges& off, cudaStream_t st) {
+  if (ns < 1 || ns > kMaxOzakiSlices || nmod < 2 || nmod > kCrtMaxModuli)
+    return set_error(MOAO_ERR_BAD_ARG, "crt: slices or moduli");
+  if ((ldo & 3) || (reinterpret_cast<uintptr_t>(out) & 3))
+    return set_error(MOAO_ERR_BAD_ARG, "crt: residue rows must be 4-byte aligned");
+  MOAO_CUDA_TRY(cudaMemsetAsync(colmax, 0, n * sizeof(unsigned long long), st));
+  const int* r = off.n ? rid : nullptr;
+  const OffsetValues ov = values_of(off);
+  dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+  sym_col_max_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, n, colmax, r, ov);
+  ++tl_launches;
+  exponents_from_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(colmax, n, f);
+  ++tl_launches;
+  const long nt = (n + 31) / 32;
+  crt_sym_kernel<<<(unsigned)(nt * (nt + 1) / 2), dim3(32, 8), 0, st>>>(
+      A, lda, n, f, 7 * ns - 1, nmod, out, ldo, n * ldo, r, ov);
+  ++tl_launches;
+  MOAO_CUDA_TRY(cudaGetLastError());
+  return MOAO_OK;
+}
+
+moao_status crt_combine(const uint8_t* Z, long m, long n, int nmod, int ns, const int* e,
+                        const int* f, const double* C, long ldc, double alpha, double* E,
+                        long lde, cudaStream_t st) {
+  if (nmod < 2 || nmod > kCrtMaxModuli) return set_error(MOAO_ERR_BAD_ARG, "crt: moduli");
+  if (m <= 0 || n <= 0) return MOAO_OK;
+  if ((m + 255) / 256 > 65535) return set_error(MOAO_ERR_BAD_ARG, "crt: too many rows");
+  const dim3 grid((unsigned)n, (unsigned)((m + 255) / 256));
+  crt_combine_kernel<<<grid, 256, 0, st>>>(Z, m, m * n, nmod, 7 * ns - 1, e, f, C, ldc, alpha, E,
+                                           lde);
   ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;

@@ -117,7 +117,7 @@ size_t footprint(const moao_server* s, const System& sys, const moao_request& r)
   size_t f = bytes_of(n, n) + bytes_of(m, n);
   if (r.prec == MOAO_PREC_MIXED) {
     const int nro = sys.tomo.sys.lgsCst > 0 ? 2 * sys.tomo.sys.nLgs : 0;
-    f += mixed_sizes(n, m, nb, 3, 5, nro).total();
+    f += mixed_sizes(n, m, nb, 3, 5, nro, true).total();
   } else {
     f += 2 * bytes_of(n, nb);
   }

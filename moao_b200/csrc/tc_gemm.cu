@@ -90,6 +90,7 @@ struct __align__(64) TcParams {
   const int* erow;         // INT8: per-row exponent of A (length M, indexed by r)
   const int* ecol;         // INT8: per-column exponent of B (length N)
   int shift;
+  int modulus;             // kTcEpiMod8
   int tile_m;              // rows of C per tile (128, or 256 for CTA pairs)
   int tiles_m, tiles_n;
   int total_tiles;         // tiles that intersect the written part of C
@@ -564,6 +565,16 @@ __global__ void __launch_bounds__(THREADS, 1) tc_gemm_kernel(const __grid_consta
                 const float sj = p.erow ? ra * wscale[j] : ra;
                 dst[(size_t)j * p.ldc] = sj * __uint_as_float(v32[j]) + p.beta * old[j];
               }
+          } else if (p.epi == kTcEpiMod8) {
+            // the exact int32 sum reduced modulo p.modulus, one byte per element
+            uint8_t* dst = static_cast<uint8_t*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
+            const int md = p.modulus;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (mask >> j & 1u) {
+                const int t = (int)v32[j] % md;
+                dst[(size_t)j * p.ldc] = (uint8_t)(t < 0 ? t + md : t);
+              }
           } else {
             double* dst = static_cast<double*>(p.C) + (size_t)(n0 + c0) * p.ldc + r;
             const int er = p.erow[r] + p.shift;
@@ -671,6 +682,8 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
     return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: scaled epilogue needs int8 and exponents");
   if (g.epi == kTcEpiF32 && g.kind == kTcI8)
     return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: fp32 epilogue needs bf16 or fp16 operands");
+  if (g.epi == kTcEpiMod8 && (g.kind != kTcI8 || g.modulus < 2 || g.modulus > 256))
+    return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: modular epilogue needs int8 and a modulus <= 256");
   if (g.epi == kTcEpiF32 && (!g.erow) != (!g.ecol))
     return set_error(MOAO_ERR_BAD_ARG, "tc_gemm: row and column exponents go together");
   TcParams p;
@@ -710,6 +723,7 @@ moao_status tc_gemm(const TcGemm& g, cudaStream_t s, long long* launches) {
   p.erow = g.erow;
   p.ecol = g.ecol;
   p.shift = g.shift;
+  p.modulus = g.modulus;
   p.err = g.err;
   p.spin_limit = g.spin_limit > 0 ? g.spin_limit : kSpinLimit;
   // Pairs of CTAs (256-row tiles) when asked for and C has more than one

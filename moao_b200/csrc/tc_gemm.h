@@ -15,7 +15,8 @@ constexpr int kTcMaxSegs = 8;
 // erow/ecol the FP32 epilogue scales by 2^(erow[r] + ecol[c] + shift), so the
 // operands can be stored scaled per row into fp16's range.
 enum TcKind { kTcBf16 = 0, kTcI8 = 1, kTcF16 = 2 };
-enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1 };
+enum TcEpilogue { kTcEpiF32 = 0, kTcEpiF64Scaled = 1, kTcEpiMod8 = 2 };
+// kTcEpiMod8 (int8 operands): C (uint8, column-major) = acc mod modulus, in [0, modulus).
 
 // A K-major operand: rows x kcols elements, row stride in elements.
 struct TcTensor {
@@ -46,12 +47,14 @@ struct TcGemm {
   int a_row0 = 0, b_row0 = 0;  // rows of A / B that map to C row / column 0
   int lower = 0, diag_off = 0; // only C(r, c) with r + diag_off >= c
   float alpha = 1.f, beta = 0.f;
-  void* C = nullptr;           // float (kTcEpiF32) or double (kTcEpiF64Scaled), column-major
+  void* C = nullptr;           // float (kTcEpiF32), double (kTcEpiF64Scaled) or uint8
+                               // (kTcEpiMod8), column-major
   long ldc = 0;
   const int* erow = nullptr;   // kTcEpiF64Scaled: C += acc * 2^(erow[r] + ecol[c] + shift);
                                // kTcEpiF32 (optional): acc scaled the same way
   const int* ecol = nullptr;
   int shift = 0;
+  int modulus = 0;             // kTcEpiMod8: 2..256
   int* err = nullptr;          // device flag: nonzero after a bounded wait expired
   int max_ctas = 0;            // cap on the persistent grid (0: one CTA per SM)
   int pair = 0;                // 1: 256 x 256 tiles on clusters of two CTAs where M > 128
