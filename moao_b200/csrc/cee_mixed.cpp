@@ -10,7 +10,9 @@
 // with the Ozaki splitting (int8 slices scaled by powers of two per row, exact
 // int32 accumulation, FP64 sums):
 //   Cee  = sym(tril(Ctt)) - R Ctm^T          nts x nts x nmeas, ns slices each
-//   E    = Ctm - R sym(Cmm)                  nts x nmeas x nmeas, ns slices each
+//   E    = Ctm - R sym(Cmm)                  nts x nmeas x nmeas, ns-slice operands,
+//                                            exact CRT products (one int8 GEMM per
+//                                            modulus, as the refinement residual)
 //   Cee -= E R^T                             3 slices of E: E is a residual, a few
 //                                            1e-6 of Ctm, so its product needs only
 //                                            ~1e-6 relative accuracy
@@ -69,9 +71,16 @@ moao_status cee_cvv_mixed(moao_ctx* ctx, long nm, long nt, long nact, const doub
   for (int w = 0; w < nro; ++w)
     if (off.end[w] > nm)
       return set_error(MOAO_ERR_BAD_ARG, "mixed Cee_Cvv: an offset range ends beyond nmeas");
+  // E by exact CRT products (as the refinement residual) where the moduli cover it
+  const int nmod = (!use_state && ctx->residual_crt) ? crt_moduli_for(ns, nm) : 0;
   if (nt > 0 && nm > 0) {
     MOAO_TRY(ctx->mx_qa.ensure((size_t)ns * nt * ldq));
-    MOAO_TRY(ctx->mx_qb.ensure((size_t)ns * nm * ldq));
+    if (!use_state && !nmod) MOAO_TRY(ctx->mx_qb.ensure((size_t)ns * nm * ldq));
+    if (nmod) {
+      MOAO_TRY(ctx->mx_qr.ensure((size_t)nmod * nt * ldq));
+      MOAO_TRY(ctx->mx_qs.ensure((size_t)nmod * nm * ldq));
+      MOAO_TRY(ctx->mx_z.ensure((size_t)nmod * nt * nm));
+    }
     MOAO_TRY(ctx->cx_qc.ensure((size_t)std::max(ns, kErrSlices) * nt * ldq));
     MOAO_TRY(ctx->mx_ea.ensure(sizeof(int) * (size_t)nt));
     MOAO_TRY(ctx->cx_ec.ensure(2 * sizeof(int) * (size_t)nt));
@@ -104,17 +113,37 @@ moao_status cee_cvv_mixed(moao_ctx* ctx, long nm, long nt, long nact, const doub
       MOAO_TRY(make_tc_map(&taR[i], qa + (size_t)i * nt * ldq, kTcI8, nt, nm, ldq));
       MOAO_TRY(make_tc_map(&tbR[i], qa + (size_t)i * nt * ldq, kTcI8, nt, nm, ldq, 256));
       MOAO_TRY(make_tc_map(&tbC[i], qc + (size_t)i * nt * ldq, kTcI8, nt, nm, ldq, 256));
-      MOAO_TRY(make_tc_map(&tbS[i], qb + (size_t)i * nm * ldq, kTcI8, nm, nm, ldq, 256));
+      if (!use_state && !nmod)
+        MOAO_TRY(make_tc_map(&tbS[i], qb + (size_t)i * nm * ldq, kTcI8, nm, nm, ldq, 256));
     }
     for (int i = 0; i < kErrSlices; ++i)
       MOAO_TRY(make_tc_map(&taE[i], qc + (size_t)i * nt * ldq, kTcI8, nt, nm, ldq));
+    TcTensor tr[kCrtMaxModuli], ts[kCrtMaxModuli];
+    for (int i = 0; i < nmod; ++i) {
+      MOAO_TRY(make_tc_map(&tr[i], ctx->mx_qr.as<int8_t>() + (size_t)i * nt * ldq, kTcI8, nt, nm,
+                           ldq));
+      MOAO_TRY(make_tc_map(&ts[i], ctx->mx_qs.as<int8_t>() + (size_t)i * nm * ldq, kTcI8, nm, nm,
+                           ldq, 256));
+    }
     // slices of R's rows (or the refinement's R_k) and of Ctm's rows
     if (!use_state) MOAO_TRY(ozaki_split_rows(R, ldR, nt, nm, ns, ea, qa, ldq, s));
     MOAO_TRY(ozaki_split_rows(Cpm, ldCpm, nt, nm, ns, ec, qc, ldq, s));
     // Cee = sym(tril(Ctt)) - R Ctm^T
     MOAO_TRY(sym_from_lower(Cpp, ldCpp, Cee, ldCee, nt, s, &ctx->launches));
     MOAO_TRY(ozaki_gemm(ctx, taR, ns, tbC, ns, ns + 1, nt, nt, nm, -1.f, Cee, ldCee, ea, ec, err));
-    if (!use_state) {
+    if (!use_state && nmod) {
+      // E = Ctm - R sym(Cmm) by exact CRT products of the sliced operands
+      MOAO_TRY(crt_split_sym(Cmm, ldCmm, nm, ns, nmod, fb, ctx->mx_colmax.as<unsigned long long>(),
+                             ctx->mx_qs.as<int8_t>(), ldq, rid, off, s));
+      MOAO_TRY(crt_split_rows(R, ldR, nt, nm, ns, nmod, ea, ctx->mx_qr.as<int8_t>(), ldq, s));
+      MOAO_TRY(crt_gemm(ctx, tr, ts, nmod, nt, nm, nm, ctx->mx_z.as<uint8_t>(), err));
+      MOAO_TRY(crt_combine(ctx->mx_z.as<uint8_t>(), nt, nm, nmod, ns, ea, fb, Cpm, ldCpm, -1.0,
+                           E64, nt, s));
+      if (nro > 0) {  // the offsets' part of R Cmm
+        MOAO_TRY(range_sums(R, ldR, nt, off, RU, s));
+        MOAO_TRY(subtract_offset_products(E64, nt, nt, nm, RU, rid, off, s));
+      }
+    } else if (!use_state) {
       // E = Ctm - R sym(Cmm) (the refinement state holds it for R_k)
       MOAO_CUDA_TRY(cudaMemcpy2DAsync(E64, nt * sizeof(double), Cpm, ldCpm * sizeof(double),
                                       nt * sizeof(double), nm, cudaMemcpyDeviceToDevice, s));

@@ -222,6 +222,11 @@ moao_status factor_to_host(moao_ctx* ctx, const double* Cmm, long ldCmm, long n)
 moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTensor* tb, int nsb,
                        int dmax, long M, long N, long K, float alpha, double* C, long ldc,
                        const int* erow, const int* ecol, int* err);
+// Residues of A B^T (M x N over K < 2^17) modulo the first nmod CRT moduli from
+// the operands' residues (ta / tb, one per modulus): one exact int8 GEMM per
+// modulus into Z + i*M*N (uint8, column-major, ld M). Accounted as tc_int8.
+moao_status crt_gemm(moao_ctx* ctx, const TcTensor* ta, const TcTensor* tb, int nmod, long M,
+                     long N, long K, uint8_t* Z, int* err);
 // Cee and Cvv with the int8 tensor cores (cee_mixed.cpp); same arguments and
 // in-place contract as moao_cee_cvv except that Cpp is left as given. With
 // from_refinement and a matching refinement state on the context, Cee is

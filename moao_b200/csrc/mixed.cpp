@@ -341,9 +341,8 @@ moao_status ozaki_gemm(moao_ctx* ctx, const TcTensor* ta, int nsa, const TcTenso
   return MOAO_OK;
 }
 
-// Residues of the product A B^T (M x N over K) modulo the first nmod moduli:
-// one int8 GEMM per modulus on the operands' residues (exact int32 sums, K <
-// 2^17), reduced in the epilogue into Z + i*M*N (uint8, column-major, ld M).
+// One int8 GEMM per modulus (exact int32 sums, K < 2^17), reduced modulo it in
+// the epilogue.
 moao_status crt_gemm(moao_ctx* ctx, const TcTensor* ta, const TcTensor* tb, int nmod, long M,
                      long N, long K, uint8_t* Z, int* err) {
   if (nmod < 2 || nmod > kCrtMaxModuli || K >= (1L << 17))
