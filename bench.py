@@ -1155,8 +1155,8 @@ def main():
         refine = 1 if args.path == "mixed" else 0
         fp64_flop = (nm ** 3 / 3.0 + 2.0 * nts * nm * nm * (1 + 2 * refine)) * args.steps
         fp64_equiv = fp64_flop / (ms / 1000.0) / 1e12
-        return {"kernel": "tc_gemm_kernel (tcgen05 kind::f16 fp16-split products and kind::i8 Ozaki "
-                          "residual; TMA, TMEM)", "bound": "tensor",
+        return {"kernel": "tc_gemm_kernel (tcgen05 kind::f16 fp16-split products and kind::i8 exact "
+                          "CRT residual products; TMA, TMEM)", "bound": "tensor",
                 "achieved": round(achieved, 3), "peak": round(bf16, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / bf16, 4),
                 "peak_source": (f"bf16_tflops_sustained {peak_src} (the kernel runs inside a "
@@ -1165,7 +1165,8 @@ def main():
                 "frac_fp64_equivalent": round(fp64_equiv / bf16, 4),
                 "fp64_equivalent_note": ("algorithmic FP64 flop of the build over this kernel's time: "
                                          "the split products multiply the tensor work (3 fp16 products "
-                                         "per update, 15 int8 slice pairs per residual)"),
+                                         "per update, one int8 product per CRT modulus, 11 at nmeas "
+                                         "47,552, per residual)"),
                 "traffic": traffic,
                 "traffic_note": ("DRAM bytes per launch: each family's bytes per unit of work from its "
                                  "ncu capture in profiles/ (nmeas 15,936) times the work of this run's "
@@ -1190,7 +1191,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.path == "fp64" else
                  ("fp16x2 row-scaled split (fp32 accumulate) tensor-core updates + f64 diagonal blocks "
-                  "+ int8 Ozaki f64 residual"),
+                  "+ exact int8 CRT products for the f64 residual"),
         "data": "synthetic (seeded ELT-scale system; reference parameter-file format)",
         "config": {"workload": workload_name(args.config, nm, nts, atm.nLayer), "path": args.path,
                    "nmeas": nm, "nmeasts": nts, "layers": atm.nLayer, "panel_nb": nb_main,
