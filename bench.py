@@ -1148,7 +1148,7 @@ def main():
         bf16 = float(peaks.get("bf16_tflops_sustained", 1400.0))
         achieved = (a["work"] + 0.5 * b["work"]) / (ms / 1000.0) / 1e12
         ra = read_traffic_ratio("tc_gemm_f16_trailing_nmeas15936.txt")
-        rb = read_traffic_ratio("tc_gemm_int8_residual_nmeas15936.txt")
+        rb = read_traffic_ratio("tc_gemm_int8_crt_nmeas15936.txt")
         traffic = None
         if ra and rb:
             traffic = (ra * a["work"] + rb * b["work"]) / max(1, a["launches"] + b["launches"])
