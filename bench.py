@@ -1103,7 +1103,7 @@ def main():
             peak = bf16 * (2.0 if fam == "tc_int8" else 1.0)
             achieved = s["work"] / (s["ms"] / 1000.0) / 1e12
             what = "int8" if fam == "tc_int8" else "fp16/bf16 split"
-            ratio = read_traffic_ratio("tc_gemm_int8_residual_nmeas15936.txt" if fam == "tc_int8"
+            ratio = read_traffic_ratio("tc_gemm_int8_crt_nmeas15936.txt" if fam == "tc_int8"
                                        else "tc_gemm_f16_trailing_nmeas15936.txt")
             return {"kernel": f"tc_gemm_kernel ({what} tcgen05, TMA, TMEM)", "bound": "tensor",
                     "achieved": round(achieved, 3), "peak": round(peak, 3),
