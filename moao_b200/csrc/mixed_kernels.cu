@@ -466,6 +466,32 @@ __device__ __forceinline__ void crt_residues(double x, int nmod, int8_t* r) {
   crt_residue_from<1>(x, nmod, r);
 }
 
+// The residues of four integers x[0..3] (|x| <= 2^41) modulo the I-th modulus
+// and those after it, each packed into one word w[I] (byte q = residue of x[q]):
+// the low 32 bits of r + kMagic64 hold r in two's complement, and two levels of
+// byte permutes assemble the word.
+template <int I>
+__device__ __forceinline__ void crt_words_from(const double* x, int nmod, uint32_t* w) {
+  if constexpr (I < kCrtMaxModuli) {
+    if (I < nmod) {
+      int l[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if constexpr (I == 0) {
+          l[q] = __double2loint(x[q] + kMagic64);  // the low byte: x mod 256
+        } else {
+          constexpr int M = crt_mod(I);
+          constexpr double INV = 1.0 / M;
+          const double qt = fma(x[q], INV, kMagic64) - kMagic64;
+          l[q] = __double2loint(fma(-(double)M, qt, x[q]) + kMagic64);
+        }
+      }
+      w[I] = __byte_perm(__byte_perm(l[0], l[1], 0x0040), __byte_perm(l[2], l[3], 0x0040), 0x5410);
+    }
+    crt_words_from<I + 1>(x, nmod, w);
+  }
+}
+
 // Garner's step for modulus I: t <- (((t - v_0) m_0^-1 - v_1) m_1^-1 - ...) mod m_I,
 // centred, in FP32: every operand is an integer below 2^17 in magnitude (exact),
 // and y / M (error <= 2^-14) is at least 1 / 2M from a half-integer.
@@ -554,14 +580,13 @@ __global__ void crt_rows_kernel(const double* __restrict__ A, long lda, long m, 
 // (the K-major B operand), S(k, j) = A(max(k,j), min(k,j)) minus offsets,
 // whose exponent is f[j]. B is not symmetric (the scale is per column), but
 // B[j][k] and B[k][j] scale the same stored element: a block of 32 x 32 tiles
-// at or below the diagonal (kb >= jb) loads its stored elements once, and its
-// residues for both orientations are written, the mirrored ones staged through
-// shared memory so that both sets of stores are 32-bit and coalesced.
+// at or below the diagonal (kb >= jb) loads its stored elements once and
+// writes the residues of both orientations, each thread four consecutive
+// entries of a row per residue (one 32-bit coalesced store).
 __global__ void crt_sym_kernel(const double* __restrict__ A, long lda, long n,
                                const int* __restrict__ f, int sh, int nmod, int8_t* out,
                                long ldo, long stride, const int* rid, const OffsetValues ov) {
-  __shared__ double t[32][33];                       // t[jj][kk] = S(k0+kk, j0+jj)
-  __shared__ int8_t rs[kCrtMaxModuli][32][36];       // rs[i][kk][jj]: residue of S(j, k) at f[k]
+  __shared__ double t[32][33];  // t[jj][kk] = S(k0+kk, j0+jj)
   // tile (jb, kb) with kb >= jb from the linear index (kb rows of the lower triangle)
   const long tix = blockIdx.x;
   long kb = (long)((sqrt(8.0 * (double)tix + 1.0) - 1.0) * 0.5);
@@ -586,51 +611,44 @@ __global__ void crt_sym_kernel(const double* __restrict__ A, long lda, long n,
     }
   }
   __syncthreads();
-  // direct orientation: row j, 4 consecutive k per thread, one 32-bit store per residue
   const int tid = ty * 32 + tx;
-  const int jj = tid >> 3, kq = (tid & 7) * 4;
-  const long j = j0 + jj, k = k0 + kq;
-  const bool mirror = k0 > j0;
-  if (j < n && k < n) {
-    const double sc = pow2i(sh - f[j]);
-    uint32_t w[kCrtMaxModuli];
-#pragma unroll
-    for (int i = 0; i < kCrtMaxModuli; ++i) w[i] = 0;
-#pragma unroll
-    for (int q4 = 0; q4 < 4; ++q4) {
-      const double v = (k + q4 < n) ? t[jj][kq + q4] * sc : 0.0;
-      int8_t res[kCrtMaxModuli] = {};
-      crt_residues((v + kMagic64) - kMagic64, nmod, res);
-#pragma unroll
-      for (int i = 0; i < kCrtMaxModuli; ++i) w[i] |= (uint32_t)(uint8_t)res[i] << (8 * q4);
-    }
-#pragma unroll
-    for (int i = 0; i < kCrtMaxModuli; ++i)
-      if (i < nmod) *reinterpret_cast<uint32_t*>(out + i * stride + j * ldo + k) = w[i];
-  }
-  if (!mirror) return;  // a diagonal tile's mirror is itself
-  // mirrored orientation: row k (column k of S, exponent f[k]), entries j: the
-  // thread computes S(k0+kk, j0+jq..jq+3) at f[k0+kk] and stages them
+  const int a = tid >> 3, q4 = (tid & 7) * 4;
+  // direct orientation: row j0 + a, entries k0 + q4 .. + 3 at f[j]
   {
-    const int kk = tid >> 3, jq = (tid & 7) * 4;
-    const long kr = k0 + kk;
-    if (kr < n) {
-      const double sc = pow2i(sh - f[kr]);
+    const long j = j0 + a, k = k0 + q4;
+    if (j < n && k < n) {
+      const double sc = pow2i(sh - f[j]);
+      double x[4];
 #pragma unroll
-      for (int q4 = 0; q4 < 4; ++q4) {
-        const double v = (j0 + jq + q4 < n) ? t[jq + q4][kk] * sc : 0.0;
-        int8_t res[kCrtMaxModuli] = {};
-        crt_residues((v + kMagic64) - kMagic64, nmod, res);
-#pragma unroll
-        for (int i = 0; i < kCrtMaxModuli; ++i)
-          if (i < nmod) rs[i][kk][jq + q4] = res[i];
+      for (int q = 0; q < 4; ++q) {
+        const double v = (k + q < n) ? t[a][q4 + q] * sc : 0.0;
+        x[q] = (v + kMagic64) - kMagic64;
       }
-      // the thread's own 4 bytes per residue are contiguous: store them as one word
+      uint32_t w[kCrtMaxModuli];
+      crt_words_from<0>(x, nmod, w);
 #pragma unroll
       for (int i = 0; i < kCrtMaxModuli; ++i)
-        if (i < nmod && j0 + jq < n)
-          *reinterpret_cast<uint32_t*>(out + i * stride + kr * ldo + j0 + jq) =
-              *reinterpret_cast<const uint32_t*>(&rs[i][kk][jq]);
+        if (i < nmod) *reinterpret_cast<uint32_t*>(out + i * stride + j * ldo + k) = w[i];
+    }
+  }
+  if (k0 == j0) return;  // a diagonal tile's mirror is itself
+  // mirrored orientation: row k0 + a (column k of S, exponent f[k]), entries
+  // j0 + q4 .. + 3
+  {
+    const long k = k0 + a, j = j0 + q4;
+    if (k < n && j < n) {
+      const double sc = pow2i(sh - f[k]);
+      double x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double v = (j + q < n) ? t[q4 + q][a] * sc : 0.0;
+        x[q] = (v + kMagic64) - kMagic64;
+      }
+      uint32_t w[kCrtMaxModuli];
+      crt_words_from<0>(x, nmod, w);
+#pragma unroll
+      for (int i = 0; i < kCrtMaxModuli; ++i)
+        if (i < nmod) *reinterpret_cast<uint32_t*>(out + i * stride + k * ldo + j) = w[i];
     }
   }
 }
