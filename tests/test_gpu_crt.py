@@ -94,3 +94,32 @@ def test_reconstructor_with_either_residual(ctx, scheme):
     err = np.linalg.norm(got - want) / np.linalg.norm(want)
     assert err <= 1e-5, (scheme, err)
     assert rep["refine_steps"] >= 1 and rep["refine_resid"] < 1e-3
+
+
+@pytest.mark.parametrize("name", ["elt16", "elt24"])
+def test_crt_residual_with_declared_offsets(cuda, name):
+    """The model's LGS offsets declared (the residual's operands are then
+    sym(Cmm) minus the offsets, whose part of R Cmm comes from FP64 range sums):
+    R within 1e-5 of the oracle with either residual, and the CRT residual's R
+    at least as accurate as the slice products' (it drops no terms)."""
+    import oracle as O
+    import systems
+    sf, af = systems.files(name)
+    t = M.Tomo(sf, af)
+    g = O.Geometry.from_tomo(t)
+    nm, nts = g.nmeas, g.nmeasts
+    Cmm = O.matcov(g, nm, nm, 0, 0, 1, nthreads=16)
+    Ctm = O.matcov(g, nts, nm, 0, 0, 3, nthreads=16)
+    _, R_ref, _ = O.reconstructor(Cmm, Ctm)
+    errs = {}
+    for scheme in ("crt", "slices"):
+        c2 = M.Context(0)
+        c2.set_offsets_from_tomo(t)
+        c2.set_residual_scheme(scheme)
+        dC, dT = dev(Cmm), dev(Ctm)
+        M.reconstructor(nm, nts, dC, nm, dT, nts, 1, prec="mixed", ctx=c2)
+        c2.synchronize()
+        errs[scheme] = O.rel_fro(host(dT), R_ref)
+        c2.close()
+    assert errs["crt"] <= 1e-5 and errs["slices"] <= 1e-5, errs
+    assert errs["crt"] <= 1.05 * errs["slices"], errs
