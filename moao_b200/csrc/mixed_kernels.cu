@@ -746,25 +746,42 @@ __global__ void mul_small_left_kernel(const double* __restrict__ S, int k,
 }
 
 // 256 rows per block, 64 columns per block; ZU(i, :) stays in registers.
+// KMAX >= k bounds the unrolled range loops (registers for ZU's row).
+template <int KMAX>
 __global__ void woodbury_kernel(const float* __restrict__ Z, long ldz, long m, long n,
                                 const double* __restrict__ ZU, int k,
                                 const double* __restrict__ Y2, double* __restrict__ R, long ldr,
                                 int accumulate) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  // the block's 64 columns of Y2 (k values each) in shared memory, read as
+  // broadcasts; four columns' Z values in flight per thread
+  __shared__ double ys[64 * KMAX];
   const long j0 = (long)blockIdx.y * 64;
-  if (i >= m) return;
-  double zu[kMaxOffsetRanges];
-#pragma unroll
-  for (int w = 0; w < kMaxOffsetRanges; ++w) zu[w] = w < k ? ZU[(long)w * m + i] : 0.0;
   const long j1 = min(n, j0 + 64);
-  for (long j = j0; j < j1; ++j) {
-    double a = (double)Z[j * ldz + i];
-    const double* y = Y2 + j * k;
+  for (int t = threadIdx.x; t < (int)(j1 - j0) * k; t += blockDim.x) ys[t] = Y2[j0 * k + t];
+  __syncthreads();
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double zu[KMAX];
 #pragma unroll
-    for (int w = 0; w < kMaxOffsetRanges; ++w)
-      if (w < k) a = fma(-zu[w], y[w], a);
-    if (accumulate) R[j * ldr + i] += a;
-    else R[j * ldr + i] = a;
+  for (int w = 0; w < KMAX; ++w) zu[w] = w < k ? ZU[(long)w * m + i] : 0.0;
+  for (long j = j0; j < j1; j += 4) {
+    float zv[4];
+    double rv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      zv[q] = j + q < j1 ? Z[(j + q) * ldz + i] : 0.f;
+      rv[q] = (accumulate && j + q < j1) ? R[(j + q) * ldr + i] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (j + q >= j1) break;
+      const double* y = ys + (j + q - j0) * k;
+      double a = (double)zv[q];
+#pragma unroll
+      for (int w = 0; w < KMAX; ++w)
+        if (w < k) a = fma(-zu[w], y[w], a);
+      R[(j + q) * ldr + i] = rv[q] + a;
+    }
   }
 }
 
@@ -891,7 +908,11 @@ moao_status woodbury_apply(const float* Z, long ldz, long m, long n, const doubl
   if (m <= 0 || n <= 0) return MOAO_OK;
   if (k < 1 || k > kMaxOffsetRanges) return set_error(MOAO_ERR_BAD_ARG, "woodbury_apply: k");
   dim3 grid((unsigned)((m + 255) / 256), (unsigned)((n + 63) / 64));
-  woodbury_kernel<<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, accumulate ? 1 : 0);
+  const int acc = accumulate ? 1 : 0;
+  static_assert(kMaxOffsetRanges <= 32, "woodbury_kernel instantiations");
+  if (k <= 8) woodbury_kernel<8><<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, acc);
+  else if (k <= 16) woodbury_kernel<16><<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, acc);
+  else woodbury_kernel<32><<<grid, 256, 0, st>>>(Z, ldz, m, n, ZU, k, Y2, R, ldr, acc);
   ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
