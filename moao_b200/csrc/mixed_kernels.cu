@@ -222,46 +222,39 @@ __global__ void split_f16_kernel(const T* __restrict__ src, long lds, long m, lo
   }
 }
 
-// Row exponents and row-major fp16 slices of an FP32 column-major m x kb block in
-// one pass: a CTA stages 16 full rows (kb <= kSplitMaxCols) in shared memory,
-// takes their maxima, then writes each slice two columns per thread; columns
-// kb..kpad-1 of the slices get zeros (the tensor core reads K in steps of 64).
-// Same exponents and slices as row_exponent_kernel + split_f16_kernel.
-constexpr int kSplitRows = 16;
+// Row-major fp16 slices of an FP32 column-major m x kb block (kb <= kSplitMaxCols)
+// from its row exponents; columns kb..kpad-1 of the slices get zeros (the tensor
+// core reads K in steps of 64). Same exponents and slices as row_exponent_kernel +
+// split_f16_kernel.
 constexpr int kSplitMaxCols = 1024;
-__global__ void __launch_bounds__(256) split_rows_f16_kernel(const float* __restrict__ src, long lds,
-                                                             long m, int kb, int ns, BfSlices out,
-                                                             long ldx, int kpad,
-                                                             int* __restrict__ erow, int bias) {
-  extern __shared__ float srow[];  // kSplitRows x (kb + 1)
-  __shared__ float red[16][kSplitRows + 1];
-  __shared__ float sscale[kSplitRows];
-  const int tid = threadIdx.x, tr = tid % kSplitRows, tc = tid / kSplitRows;
-  const long r0 = (long)blockIdx.x * kSplitRows, r = r0 + tr;
-  const int ld = kb + 1;
-  float mx = 0.f;
-  if (r < m)
-    for (int c = tc; c < kb; c += 16) {
-      const float v = src[(long)c * lds + r];
-      srow[tr * ld + c] = v;
-      mx = fmaxf(mx, fabsf(v));
-    }
-  red[tc][tr] = mx;
-  __syncthreads();
-  if (tc == 0) {
-    for (int k = 1; k < 16; ++k) mx = fmaxf(mx, red[k][tr]);
-    const int e = exponent_of((double)mx) - bias;
-    if (r < m) erow[r] = e;
-    sscale[tr] = pow2f(-e);
+
+// A CTA takes a 32-row x 64-column tile, reads it column by column (coalesced
+// over the rows) into shared memory and writes each row's 64 entries as 32
+// half2 words per slice (coalesced over the columns); columns kb..kpad-1 are
+// written as zeros.
+__global__ void __launch_bounds__(256) split_rows_f16_t_kernel(const float* __restrict__ src,
+                                                               long lds, long m, int kb, int ns,
+                                                               BfSlices out, long ldx, int kpad,
+                                                               const int* __restrict__ erow) {
+  __shared__ float2 t[32][33];  // t[row][column pair]
+  const long r0 = (long)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 64;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  float* tf = reinterpret_cast<float*>(&t[0][0]);
+  for (int cc = ty; cc < 64; cc += 8) {
+    const long r = r0 + tx;
+    const int c = c0 + cc;
+    tf[tx * 66 + cc] = (r < m && c < kb) ? src[(long)c * lds + r] : 0.f;
   }
   __syncthreads();
-  const int half = kpad / 2;
-  for (int idx = tid; idx < kSplitRows * half; idx += blockDim.x) {
-    const int rr = idx / half, c = 2 * (idx % half);
+  const int c = c0 + 2 * tx;
+  if (c >= kpad) return;
+  for (int rr = ty; rr < 32; rr += 8) {
     const long row = r0 + rr;
     if (row >= m) continue;
-    float a = c < kb ? srow[rr * ld + c] * sscale[rr] : 0.f;
-    float b = c + 1 < kb ? srow[rr * ld + c + 1] * sscale[rr] : 0.f;
+    const float sc = pow2f(-erow[row]);
+    const float2 v = t[rr][tx];
+    float a = v.x * sc, b = v.y * sc;
     for (int k = 0; k < ns; ++k) {
       const __half ha = __float2half_rn(a), hb = __float2half_rn(b);
       a -= __half2float(ha);
@@ -1042,12 +1035,14 @@ moao_status split_rows_f16(const float* src, long lds, long m, long kb, int ns, 
   if (ns < 1 || ns > kMaxBfSlices) return set_error(MOAO_ERR_BAD_ARG, "split_rows_f16: slices");
   if (kb > kSplitMaxCols || kpad < kb || kpad > ldx || (kpad & 1) || (ldx & 1))
     return set_error(MOAO_ERR_BAD_ARG, "split_rows_f16: block shape");
-  static std::atomic<unsigned long long> configured{0};
-  const int smem = (int)(kSplitRows * (kSplitMaxCols + 1) * sizeof(float));
-  MOAO_CUDA_TRY(set_smem_limit(split_rows_f16_kernel, smem, configured));
-  const size_t dyn = (size_t)kSplitRows * (kb + 1) * sizeof(float);
-  split_rows_f16_kernel<<<(unsigned)((m + kSplitRows - 1) / kSplitRows), 256, dyn, st>>>(
-      src, lds, m, (int)kb, ns, out, ldx, (int)kpad, erow, bias);
+  // row exponents, then the split through 32 x 64 tiles (the block stays in L2
+  // between the two passes)
+  row_exponent_kernel<float><<<(unsigned)((m + 31) / 32), dim3(32, 8), 0, st>>>(src, lds, m, kb,
+                                                                              erow, bias);
+  ++tl_launches;
+  const dim3 grid((unsigned)((m + 31) / 32), (unsigned)((kpad + 63) / 64));
+  split_rows_f16_t_kernel<<<grid, dim3(32, 8), 0, st>>>(src, lds, m, (int)kb, ns, out, ldx,
+                                                        (int)kpad, erow);
   ++tl_launches;
   MOAO_CUDA_TRY(cudaGetLastError());
   return MOAO_OK;
