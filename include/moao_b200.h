@@ -190,7 +190,9 @@ moao_status moao_ctx_set_block(moao_ctx* ctx, int nb);
  * factor in the correction solves (1 to the format's slice count; 1 uses only
  * the leading slice products; 0, the default, picks 1 for MOAO_FACTOR_F16X2
  * and 2 for BF16X3: a correction needs ~1e-2 relative accuracy), int8
- * slices per operand of the refinement residual (2..6, default 5), refinement
+ * slices per operand of the refinement residual (2..6, default 5; with the CRT
+ * residual of moao_ctx_set_residual they set the operands' precision, 7 bits
+ * per slice less one, and the moduli count follows), refinement
  * corrections per target (0..8, default 1), residual tolerance that stops
  * refinement early (default 0) and whether to evaluate the residual again after
  * the last correction (so the report's refine_resid describes the returned R;
