@@ -36,6 +36,11 @@ moao_status moao_debug_residual(moao_ctx* ctx, int scheme, long m, long n, const
                                 long ldR, const double* Cmm, long ldCmm, const double* Ctm,
                                 long ldCtm, double* E, long ldE);
 
+/* Moduli the CRT residual uses for a product over K terms of two operands of
+ * ns-slice precision (0: none suffice, or K >= 131,072 breaks the exact int32
+ * sums, and the slice products run instead). Host only. */
+int moao_debug_crt_moduli(int ns, long K);
+
 #ifdef __cplusplus
 }
 #endif

@@ -164,6 +164,7 @@ SIGNATURES = {
     "moao_debug_tc_gemm": (i32, [vp, i32, i64, i64, i64, dp, i64, i32, dp, i64, i32, i32, dp, dp, dp,
                                  i64, C.c_float, C.c_float, dp, dp, i32, i32]),
     "moao_debug_residual": (i32, [vp, i32, i64, i64, dp, i64, dp, i64, dp, i64, dp, i64]),
+    "moao_debug_crt_moduli": (i32, [i32, i64]),
 }
 
 

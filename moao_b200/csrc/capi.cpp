@@ -8,6 +8,7 @@
 
 #include "context.h"
 #include "dense.h"
+#include "mixed.h"
 
 namespace moao {
 
@@ -592,6 +593,8 @@ moao_status moao_debug_residual(moao_ctx* c, int scheme, long m, long n, const d
   MOAO_CUDA_TRY(cudaSetDevice(c->device));
   return debug_residual(c, scheme, m, n, R, ldR, Cmm, ldCmm, Ctm, ldCtm, E, ldE);
 }
+
+int moao_debug_crt_moduli(int ns, long K) { return crt_moduli_for(ns, K); }
 
 moao_status moao_ctx_set_tc_pair(moao_ctx* c, int on) {
   if (!c) return set_error(MOAO_ERR_BAD_ARG, "ctx_set_tc_pair: null");

@@ -122,3 +122,12 @@ def test_floating_point_reductions_are_exact():
         t = yf - np.float32(m) * np.rint(yf * inv)   # every product and difference is exact
         wy = ((y + m // 2) % m) - m // 2
         assert np.array_equal(t.astype(np.int64), wy), m
+
+
+def test_library_moduli_count_matches(built):
+    """The library's own count (moao_debug_crt_moduli, host code) equals this
+    restatement's, the fallback to slice products included."""
+    from moao_b200._lib import lib
+    for ns in range(1, 7):
+        for K in (1, 2, 100, 4096, 47552, 100000, 131071, 131072, 10 ** 6):
+            assert lib().moao_debug_crt_moduli(ns, K) == moduli_for(ns, K), (ns, K)
