@@ -131,3 +131,43 @@ def test_library_moduli_count_matches(built):
     for ns in range(1, 7):
         for K in (1, 2, 100, 4096, 47552, 100000, 131071, 131072, 10 ** 6):
             assert lib().moao_debug_crt_moduli(ns, K) == moduli_for(ns, K), (ns, K)
+
+
+def test_kernel_reconstruction_path_in_floating_point():
+    """The reconstruction as crt_combine_kernel runs it, restated in numpy:
+    Garner digits by FP32 steps y = (t - v_j) m_j^-1, t = y - M round(y / M)
+    (round by the 1.5 * 2^23 constant), then P = L + W_7 H from two int64
+    Horner halves joined in FP64. Equal to the exact value within 2 ulp."""
+    rng = np.random.default_rng(7)
+    nmod = 11
+    M = math.prod(MODULI[:nmod])
+    # sums of K = 47552 products of 35-bit integers, spread over the whole range
+    exact = [int(rng.integers(-2 ** 62, 2 ** 62)) * int(rng.integers(1, 2 ** 21)) for _ in range(3000)]
+    exact += [0, 1, -1, 47552 * 2 ** 68, -47552 * 2 ** 68, M // 2 - 1, -(M // 2) + 1]
+    magic = np.float32(12582912.0)
+    z = np.array([[p % m for m in MODULI[:nmod]] for p in exact], dtype=np.float32)
+    v = np.zeros_like(z)
+    v[:, 0] = np.where(z[:, 0] >= 128, z[:, 0] - 256, z[:, 0])
+    for i in range(1, nmod):
+        m = MODULI[i]
+        inv_m = np.float32(1.0) / np.float32(m)
+        t = z[:, i].copy()
+        for j in range(i):
+            y = (t - v[:, j]) * np.float32(pow(MODULI[j] % m, -1, m))
+            q = (y * inv_m + magic) - magic
+            t = y - np.float32(m) * q
+        v[:, i] = t
+    vi = v.astype(np.int64)
+    L = np.zeros(len(exact), dtype=np.int64)
+    for i in reversed(range(7)):
+        L = L * MODULI[i] + vi[:, i]
+    H = np.zeros(len(exact), dtype=np.int64)
+    for i in reversed(range(7, nmod)):
+        H = H * MODULI[i] + vi[:, i]
+    w7 = float(math.prod(MODULI[:7]))
+    assert w7 == math.prod(MODULI[:7])  # exact in FP64
+    for p, l, h in zip(exact, L.tolist(), H.tolist()):
+        assert l + math.prod(MODULI[:7]) * h == p            # the digits are exact
+        got = float(h) * w7 + float(l)                       # two roundings (the kernel fuses one)
+        want = float(p)
+        assert abs(got - want) <= 2 * np.spacing(abs(want)) + 0.0, (p, got, want)
