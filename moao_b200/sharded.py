@@ -123,7 +123,14 @@ def generate(lay: Layout, A, B, ops, tomo) -> None:
 def factor_and_solve(lay: Layout, A, B, ops, dist=None, group=None) -> int:
     """Factors the distributed Cmm in A and turns the distributed Ctm columns in
     B into R's (in place). Returns 0, or the 1-based global column of the first
-    non-positive pivot (then every rank stops after that step)."""
+    non-positive pivot (then every rank stops after that step).
+
+    With several ranks the factorisation looks one panel ahead: at step k the
+    owner of panel k + 1 first applies panel k to that panel alone, factors it
+    and starts its broadcast (asynchronously), and only then applies panel k
+    to the rest of its panels, so that panel k + 1 travels while every rank
+    updates. The collectives are the same broadcasts in the same order on every
+    rank."""
     import torch
     n, m, nb, P, rank = lay.n, lay.m, lay.nb, lay.P, lay.rank
     dev, f64 = A.device, torch.float64
@@ -134,60 +141,104 @@ def factor_and_solve(lay: Layout, A, B, ops, dist=None, group=None) -> int:
         if P > 1:
             dist.broadcast(buf, src=src, group=group)
 
-    for k in range(lay.nt):
-        k0, kb, o = k * nb, lay.width(k), lay.owner(k)
+    def buffer(k):
+        k0, kb = k * nb, lay.width(k)
         rest = n - k0 - kb
-        buf = torch.empty(1 + (kb * rest + kb * m if P > 1 else 0), dtype=f64, device=dev)
-        if rank == o:
+        return torch.empty(1 + (kb * rest + kb * m if P > 1 else 0), dtype=f64, device=dev)
+
+    def factor_panel(k):
+        """On the owner of panel k: L_kk and its inverse, the panel's rows
+        below the diagonal block L_ik = A_ik L_kk^-T and X_k = B_k L_kk^-T;
+        returns the broadcast buffer [status, L(k0+kb : n, k), X_k]."""
+        k0, kb = k * nb, lay.width(k)
+        rest = n - k0 - kb
+        buf = buffer(k)
+        lc = lay.local_col(k)
+        Lk = torch.zeros((kb, kb), dtype=f64, device=dev)
+        info = ops.potrf_inv((A, lc, k0), kb, Lk)
+        linv[k] = Lk
+        if info == 0:
+            if rest:
+                W = torch.empty((kb, rest), dtype=f64, device=dev)
+                ops.gemm(True, False, rest, kb, kb, 1.0, (A, lc, k0 + kb), (Lk, 0, 0), 0.0,
+                         (W, 0, 0))
+                A[lc:lc + kb, k0 + kb:n] = W
+            if m:
+                W = torch.empty((kb, m), dtype=f64, device=dev)
+                ops.gemm(True, False, m, kb, kb, 1.0, (B, lc, 0), (Lk, 0, 0), 0.0, (W, 0, 0))
+                B[lc:lc + kb, :] = W
+        buf[0] = float(info + k0 if info else 0)
+        if P > 1:
+            if rest:
+                buf[1:1 + kb * rest].view(kb, rest).copy_(A[lc:lc + kb, k0 + kb:n])
+            if m:
+                buf[1 + kb * rest:].view(kb, m).copy_(B[lc:lc + kb, :])
+        return buf
+
+    def update(k, panels, buf):
+        """Apply panel k (its broadcast buffer) to this rank's panels `panels`
+        (consecutive in local storage, all after k)."""
+        if not panels:
+            return
+        k0, kb = k * nb, lay.width(k)
+        rest = n - k0 - kb
+        Lp = buf[1:1 + kb * rest].view(kb, rest)   # L(k0+kb : n, panel k), ld rest
+        Xk = buf[1 + kb * rest:].view(kb, m)       # X_k, ld m
+        for j in panels:  # A(j0:n, panel j) -= L(j0:n, k) L(j0:j0+jb, k)^T, lower on its diagonal block
+            j0, jb = j * nb, lay.width(j)
+            r = j0 - (k0 + kb)
+            ops.gemm(True, True, n - j0, jb, kb, -1.0, (Lp, 0, r), (Lp, 0, r), 1.0,
+                     (A, lay.local_col(j), j0))
+        if m:  # B(:, panels) -= X_k L(rows of the panels, k)^T in one product
+            rows = torch.cat([torch.arange(j * nb - (k0 + kb), j * nb - (k0 + kb) + lay.width(j),
+                                           device=dev) for j in panels])
+            G = Lp[:, rows].contiguous()
+            ops.gemm(True, False, m, int(rows.numel()), kb, -1.0, (Xk, 0, 0), (G, 0, 0), 1.0,
+                     (B, lay.local_col(panels[0]), 0))
+
+    if P == 1:
+        for k in range(lay.nt):
+            k0, kb = k * nb, lay.width(k)
+            rest = n - k0 - kb
+            info = int(factor_panel(k)[0].item())
+            if info:
+                return info
+            later = [j for j in owned if j > k]
+            if not later:
+                continue
+            # the later panels are the whole trailing matrix: one lower SYRK, L(k0+kb : n,
+            # panel k) and X_k read in place
             lc = lay.local_col(k)
-            Lk = torch.zeros((kb, kb), dtype=f64, device=dev)
-            info = ops.potrf_inv((A, lc, k0), kb, Lk)
-            linv[k] = Lk
-            if info == 0:
-                if rest:
-                    W = torch.empty((kb, rest), dtype=f64, device=dev)
-                    ops.gemm(True, False, rest, kb, kb, 1.0, (A, lc, k0 + kb), (Lk, 0, 0), 0.0,
-                             (W, 0, 0))
-                    A[lc:lc + kb, k0 + kb:n] = W
-                if m:
-                    W = torch.empty((kb, m), dtype=f64, device=dev)
-                    ops.gemm(True, False, m, kb, kb, 1.0, (B, lc, 0), (Lk, 0, 0), 0.0, (W, 0, 0))
-                    B[lc:lc + kb, :] = W
-            buf[0] = float(info + k0 if info else 0)
-            if P > 1:
-                if rest:
-                    buf[1:1 + kb * rest].view(kb, rest).copy_(A[lc:lc + kb, k0 + kb:n])
-                if m:
-                    buf[1 + kb * rest:].view(kb, m).copy_(B[lc:lc + kb, :])
-        bcast(buf, o)
-        info = int(buf[0].item())
-        if info:
-            return info
-        later = [j for j in owned if j > k]
-        if not later:
-            continue
-        if P == 1:  # the later panels are the whole trailing matrix: one lower SYRK
-            lc = lay.local_col(k)
-            Lv, Xv = (A, lc, k0 + kb), (B, lc, 0)  # L(k0+kb : n, panel k) and X_k in place
+            Lv, Xv = (A, lc, k0 + kb), (B, lc, 0)
             ops.gemm(True, True, rest, rest, kb, -1.0, Lv, Lv, 1.0,
                      (A, lay.local_col(later[0]), k0 + kb))
             if m:
                 ops.gemm(True, False, m, rest, kb, -1.0, Xv, Lv, 1.0,
                          (B, lay.local_col(later[0]), 0))
-            continue
-        Lp = buf[1:1 + kb * rest].view(kb, rest)   # L(k0+kb : n, panel k), ld rest
-        Xk = buf[1 + kb * rest:].view(kb, m)       # X_k, ld m
-        for j in later:  # A(j0:n, panel j) -= L(j0:n, k) L(j0:j0+jb, k)^T, lower on its diagonal block
-            j0, jb = j * nb, lay.width(j)
-            r = j0 - (k0 + kb)
-            ops.gemm(True, True, n - j0, jb, kb, -1.0, (Lp, 0, r), (Lp, 0, r), 1.0,
-                     (A, lay.local_col(j), j0))
-        if m:  # B(:, later panels) -= X_k L(rows of the later panels, k)^T in one product
-            rows = torch.cat([torch.arange(j * nb - (k0 + kb), j * nb - (k0 + kb) + lay.width(j),
-                                           device=dev) for j in later])
-            G = Lp[:, rows].contiguous()
-            ops.gemm(True, False, m, int(rows.numel()), kb, -1.0, (Xk, 0, 0), (G, 0, 0), 1.0,
-                     (B, lay.local_col(later[0]), 0))
+    else:
+        def post(k, buf):
+            return dist.broadcast(buf, src=lay.owner(k), group=group, async_op=True)
+
+        buf = factor_panel(0) if rank == lay.owner(0) else buffer(0)
+        work = post(0, buf)
+        for k in range(lay.nt):
+            work.wait()
+            info = int(buf[0].item())
+            if info:
+                return info  # nothing posted beyond panel k: every rank stops here
+            later = [j for j in owned if j > k]
+            nxt = None
+            if k + 1 < lay.nt:
+                if rank == lay.owner(k + 1):
+                    update(k, later[:1], buf)        # panel k + 1 is this rank's first later panel
+                    later = later[1:]
+                    nxt = factor_panel(k + 1)
+                else:
+                    nxt = buffer(k + 1)
+                work = post(k + 1, nxt)
+            update(k, later, buf)
+            if nxt is not None:
+                buf = nxt
     for c in reversed(range(lay.nt)):
         c0, cb, o = c * nb, lay.width(c), lay.owner(c)
         buf = torch.empty(cb * m, dtype=f64, device=dev)
