@@ -2,9 +2,11 @@
 distribution, the broadcast schedule and the per-rank updates, with the tile
 operations done in numpy (the GPU runs the same schedule with the library's
 kernels, tests/test_gpu_sharded.py). R gathered on rank 0 equals numpy's
-Ctm Cmm^-1 for 1, 2 and 3 ranks, ragged panel widths included; the Cmm panels
-come from the oracle's covariance model on a check system; an indefinite Cmm
-stops every rank at the same step with the same column."""
+Ctm Cmm^-1 for 1, 2 and 3 ranks, ragged panel widths included (with several
+ranks the factorisation looks one panel ahead: the next panel's broadcast is
+posted before the rest of the update); the Cmm panels come from the oracle's
+covariance model on a check system; an indefinite Cmm (its failed pivot found
+in a look-ahead step) stops every rank at the same step with the same column."""
 import os
 import socket
 
