@@ -239,23 +239,61 @@ def factor_and_solve(lay: Layout, A, B, ops, dist=None, group=None) -> int:
             update(k, later, buf)
             if nxt is not None:
                 buf = nxt
-    for c in reversed(range(lay.nt)):
-        c0, cb, o = c * nb, lay.width(c), lay.owner(c)
-        buf = torch.empty(cb * m, dtype=f64, device=dev)
-        if rank == o and m:
-            lc = lay.local_col(c)
-            W = torch.empty((cb, m), dtype=f64, device=dev)
-            ops.gemm(False, False, m, cb, cb, 1.0, (B, lc, 0), (linv[c], 0, 0), 0.0, (W, 0, 0))
-            B[lc:lc + cb, :] = W
+    # backward solve, c = nt-1 .. 0: R_c = B_c L_cc^-1 on the owner of panel c, then
+    # B(:, earlier panels) -= R_c L(c0 : c0+cb, earlier panels) on every rank
+    if not m:
+        return 0
+
+    def finish(c, buf=None):
+        """On the owner of panel c: R_c into B's columns (and into buf)."""
+        cb, lc = lay.width(c), lay.local_col(c)
+        W = torch.empty((cb, m), dtype=f64, device=dev)
+        ops.gemm(False, False, m, cb, cb, 1.0, (B, lc, 0), (linv[c], 0, 0), 0.0, (W, 0, 0))
+        B[lc:lc + cb, :] = W
+        if buf is not None:
             buf.view(cb, m).copy_(W)
-        if not m:
-            continue
-        bcast(buf, o)
-        Rc = buf.view(cb, m)
+        return buf
+
+    def back_update(c, Rc, col, ncols):
+        """B(:, local columns col .. col+ncols) -= R_c L(c0 : c0+cb, those columns)."""
+        if ncols:
+            ops.gemm(False, False, m, ncols, lay.width(c), -1.0, (Rc, 0, 0), (A, col, c * nb),
+                     1.0, (B, col, 0))
+
+    def rbuf(c):
+        return torch.empty(lay.width(c) * m, dtype=f64, device=dev)
+
+    if P == 1:
+        for c in reversed(range(lay.nt)):
+            Rc = finish(c, rbuf(c)).view(lay.width(c), m)
+            back_update(c, Rc, 0, lay.local_col(c))  # the earlier panels precede panel c
+        return 0
+    # several ranks: one panel ahead, as in the factorisation (the owner of panel
+    # c - 1 updates that panel's columns with R_c, finishes R_(c-1) and posts it
+    # before updating the rest of its earlier columns)
+    def post(c, buf):
+        return dist.broadcast(buf, src=lay.owner(c), group=group, async_op=True)
+
+    c = lay.nt - 1
+    buf = finish(c, rbuf(c)) if rank == lay.owner(c) else rbuf(c)
+    work = post(c, buf)
+    for c in reversed(range(lay.nt)):
+        work.wait()
+        Rc = buf.view(lay.width(c), m)
         earlier = [j for j in owned if j < c]
-        if earlier:  # B(:, earlier panels) -= R_c L(c0:c0+cb, earlier panels)
-            N = sum(lay.width(j) for j in earlier)
-            ops.gemm(False, False, m, N, cb, -1.0, (Rc, 0, 0), (A, 0, c0), 1.0, (B, 0, 0))
+        nxt = None
+        if c > 0:
+            if rank == lay.owner(c - 1):
+                lc1 = lay.local_col(c - 1)  # this rank's last earlier panel
+                back_update(c, Rc, lc1, lay.width(c - 1))
+                earlier = earlier[:-1]
+                nxt = finish(c - 1, rbuf(c - 1))
+            else:
+                nxt = rbuf(c - 1)
+            work = post(c - 1, nxt)
+        back_update(c, Rc, 0, sum(lay.width(j) for j in earlier))
+        if nxt is not None:
+            buf = nxt
     return 0
 
 
