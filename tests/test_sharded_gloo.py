@@ -75,6 +75,10 @@ def _problem(kind, n, m, seed):
         Cmm = np.eye(n)
         Cmm[n - 3, n - 3] = -1.0
         Ctm = rng.standard_normal((m, n))
+    elif kind == "indefinite_mid":  # the failed pivot in panel 2 of 64-wide panels
+        Cmm = np.eye(n)
+        Cmm[150, 150] = -1.0
+        Ctm = rng.standard_normal((m, n))
     else:  # the oracle's covariance model on a check system
         import oracle as O
         import systems
@@ -145,7 +149,7 @@ def _launch(world, kind, n, m, nb):
 
 
 @pytest.mark.parametrize("world,n,m,nb", [(1, 300, 40, 64), (2, 300, 40, 64), (3, 517, 61, 64),
-                                          (2, 200, 0, 64), (3, 130, 17, 128)])
+                                          (2, 200, 0, 64), (3, 130, 17, 128), (4, 700, 30, 64)])
 def test_sharded_schedule_builds_R(world, n, m, nb):
     res = _launch(world, "random", n, m, nb)
     Cmm, Ctm = _problem("random", n, m, 5)
@@ -170,3 +174,13 @@ def test_sharded_schedule_on_a_check_system():
 def test_sharded_failure_stops_every_rank_at_the_same_column():
     res = _launch(2, "indefinite", 300, 20, 64)
     assert [r["info"] for r in res] == [298, 298]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_failure_in_a_lookahead_step(world):
+    """A non-positive pivot in panel 2 is found by panel 2's owner while it looks
+    ahead during step 1; every rank reads it from that panel's broadcast at
+    step 2 and stops with the same column."""
+    res = _launch(world, "indefinite_mid", 300, 20, 64)
+    assert [r["info"] for r in res] == [151] * world
+
